@@ -1,0 +1,339 @@
+// collide.cu - collision broad phase, deterministic merges, compaction.
+//
+// Broad phase: replaces broad_phase_collision_kernel (engine/src/cuda/
+// collision_kernel.cu:16-64), which only compares each body with the next 31
+// in Morton order and so misses pairs, with a query of the octree: a body
+// descends into every cell whose box, grown by the largest radius inside it,
+// lies within its own radius; at leaves it applies the reference's exact
+// FP64 test |xi - xj|^2 < (ri + rj)^2 (collision_kernel.cu:40-52).  Each pair
+// is emitted once (by its lower row) as the key lo << 32 | hi and the keys
+// are radix-sorted, which is CollisionResolver::sort_pairs' order
+// (engine/src/physics/collision_resolver.cpp:8-18).
+//
+// Merge: the reference GPU kernel (resolve_merges_kernel.cu:43-194) resolves
+// pairs under try-locks, so which pairs merge depends on thread timing.
+// Pairs per step are few (the per-frame cap is 64), so the merge here runs
+// the CPU resolver's sequential semantics (collision_resolver.cpp:20-100,
+// 190-250) in pair order in one device thread: deterministic and identical
+// to the CPU reference.
+//
+// Compaction: replaces the ~35-launch scan/scatter of compact_kernel.cu:
+// 191-407 (with a host scan above 262,144 bodies) by one kernel: warp ballot
+// / popc ranks, decoupled look-back across 4096-row tiles, and a scatter of
+// every state field.  Mask is_active && mass > 0 (compact_kernel.cu:39);
+// row order is preserved.
+#include "collide.cuh"
+#include "sort.cuh"
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+namespace nb {
+
+constexpr int kCompThreads = 256;
+constexpr int kCompItems = 16;
+constexpr int kCompTile = kCompThreads * kCompItems;
+constexpr uint32_t kCFlagAgg = 1u << 30;
+constexpr uint32_t kCFlagPre = 2u << 30;
+constexpr uint32_t kCValMask = (1u << 30) - 1;
+
+int collide_alloc(CollideBufs& b, int capacity, const std::function<int(void**, size_t)>& alloc) {
+    b.capacity = capacity;
+    b.pair_cap = capacity / 4 > 4096 ? capacity / 4 : 4096;
+    int r;
+    if ((r = alloc((void**)&b.pair_keys, sizeof(uint64_t) * b.pair_cap))) return r;
+    if ((r = alloc((void**)&b.pair_vals, sizeof(uint32_t) * b.pair_cap))) return r;
+    if ((r = alloc((void**)&b.pair_keys_alt, sizeof(uint64_t) * b.pair_cap))) return r;
+    if ((r = alloc((void**)&b.pair_vals_alt, sizeof(uint32_t) * b.pair_cap))) return r;
+    if ((r = alloc((void**)&b.pair_sort_ws, sort_workspace_bytes(b.pair_cap)))) return r;
+    if ((r = alloc((void**)&b.merge_count, sizeof(int) * (size_t)capacity))) return r;
+    const size_t tiles = (size_t)ceil_div(capacity, kCompTile) + 1;
+    if ((r = alloc((void**)&b.look, sizeof(uint32_t) * tiles))) return r;
+    return alloc((void**)&b.tile_ctr, sizeof(uint32_t) * 4);
+}
+
+// ---- broad phase ----------------------------------------------------------
+
+__global__ void k_broad_phase(int n, State s, const double4* __restrict__ sbody,
+                              const float* __restrict__ srad, const uint64_t* __restrict__ skeys,
+                              const uint32_t* __restrict__ sidx, TreeBufs t,
+                              const double* __restrict__ cube, uint64_t* __restrict__ pairs,
+                              int cap, int* __restrict__ count, int* err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t row = sidx[k];
+    if (!s.collidable[row]) return;
+    const double xi = s.px[row], yi = s.py[row], zi = s.pz[row], ri = s.radius[row];
+    const double h = cube[3];
+    const double lo[3] = {cube[0] - h, cube[1] - h, cube[2] - h};
+    const double pad = 1e-9 * h;
+    int stack[176];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int node = stack[--sp];
+        const int4 lk = t.link[node];
+        const float4 q1 = t.q1[node];
+        // the node's cell box from its level and the key of its first body
+        const int L = t.level[node];
+        const uint64_t key = skeys[lk.z];
+        const double w = ldexp(2.0 * h, -L);
+        const uint32_t c[3] = {compact21(key >> 2) >> (21 - L), compact21(key >> 1) >> (21 - L),
+                               compact21(key) >> (21 - L)};
+        const double p[3] = {xi, yi, zi};
+        double d2 = 0.0;
+        for (int a = 0; a < 3; a++) {
+            const double b0 = lo[a] + c[a] * w - pad, b1 = lo[a] + (c[a] + 1) * w + pad;
+            const double e = p[a] < b0 ? b0 - p[a] : (p[a] > b1 ? p[a] - b1 : 0.0);
+            d2 += e * e;
+        }
+        const double reach = ri + (double)q1.z;
+        if (d2 > reach * reach * (1.0 + 1e-9)) continue;
+        if (lk.y == 0) {
+            for (int j = lk.z; j < lk.z + lk.w; j++) {
+                const uint32_t rj = sidx[j];
+                if (rj <= row || !s.collidable[rj]) continue;
+                const double dx = xi - s.px[rj], dy = yi - s.py[rj], dz = zi - s.pz[rj];
+                const double dd = dx * dx + dy * dy + dz * dz;
+                const double sr = ri + s.radius[rj];
+                if (dd < sr * sr) {
+                    const int slot = atomicAdd(count, 1);
+                    if (slot < cap) pairs[slot] = ((uint64_t)row << 32) | rj;
+                    else dev_flag(err, kErrCapacity);
+                }
+            }
+            continue;
+        }
+        for (int ch = lk.x + lk.y - 1; ch >= lk.x; ch--) {
+            if (sp < 176) stack[sp++] = ch;
+            else dev_flag(err, kErrOverflow);
+        }
+    }
+}
+
+__global__ void k_iota(int n, uint32_t* v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (uint32_t)i;
+}
+
+int broad_phase(cudaStream_t st, CollideBufs& b, CollideArgs& a, bool build_tree, int* np) {
+    *np = 0;
+    if (a.n <= 0) return NB_OK;
+    if (build_tree) {
+        launch_kick_drift_bbox(st, a.n, a.s, false, 0.0, a.bbox_ord, a.n_active_dev, a.err);
+        launch_cube(st, a.bbox_ord, nullptr, a.cube);
+    }
+    launch_keys_cube(st, a.n, a.s, a.cube, a.keys0, a.vals0, (uint32_t*)a.sort_ws);
+    sort_pairs(st, a.n, a.keys0, a.vals0, a.keys1, a.vals1, a.sort_ws, true, a.err, a.sms);
+    launch_gather(st, a.n_active, a.s, a.vals0, a.sbody, a.srad);
+    tree_build(st, a.tree, a.n_active, a.keys0, a.sbody, a.srad, a.cube, a.leaf_cap, a.err);
+    cudaMemsetAsync(a.n_pairs, 0, sizeof(int), st);
+    if (a.n_active > 0)
+        k_broad_phase<<<ceil_div(a.n_active, 128), 128, 0, st>>>(
+            a.n_active, a.s, a.sbody, a.srad, a.keys0, a.vals0, a.tree, a.cube, b.pair_keys,
+            b.pair_cap, a.n_pairs, a.err);
+    int cnt = 0;
+    if (cudaMemcpyAsync(&cnt, a.n_pairs, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return NB_ERR_CUDA;
+    const int w = cnt < b.pair_cap ? cnt : b.pair_cap;
+    if (w > 1) {
+        k_iota<<<ceil_div(w, 256), 256, 0, st>>>(w, b.pair_vals);
+        sort_pairs(st, w, b.pair_keys, b.pair_vals, b.pair_keys_alt, b.pair_vals_alt,
+                   b.pair_sort_ws, false, a.err, a.sms);
+    }
+    *np = cnt;
+    return NB_OK;
+}
+
+// ---- merge --------------------------------------------------------------
+
+__device__ double dm_density(double mass, double radius, double min_radius) {
+    const double r = (radius > min_radius) ? radius : min_radius;
+    const double volume = __dmul_rn(__dmul_rn(__dmul_rn((4.0 / 3.0) * M_PI, r), r), r);
+    if (volume < 1e-30) return 0.0;
+    return mass / volume;
+}
+
+__device__ double dm_radius(double mass, double density, double min_radius) {
+    if (density < 1e-30 || mass < 1e-30) return min_radius;
+    const double r = cbrt(__dmul_rn(3.0, mass) / __dmul_rn(4.0 * M_PI, density));
+    return (r > min_radius) ? r : min_radius;
+}
+
+__device__ __forceinline__ double wavg(double ma, double a, double mb, double b, double M) {
+    return __dadd_rn(__dmul_rn(ma, a), __dmul_rn(mb, b)) / M;
+}
+
+// CollisionResolver::resolve in Merge mode (collision_resolver.cpp:20-100)
+// with resolve_merge (:190-250) and DensityModel (density_model.cpp:10-22).
+__global__ void k_merge_sequential(State s, const uint64_t* __restrict__ pairs, int np,
+                                   int max_frame, int max_body, int density_merge,
+                                   double min_radius, int* __restrict__ counts,
+                                   int* __restrict__ n_merges) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int total = 0;
+    for (int k = 0; k < np; k++) {
+        const int a = (int)(pairs[k] >> 32), b = (int)(pairs[k] & 0xFFFFFFFFu);
+        if (!s.active[a] || !s.active[b]) continue;
+        if (total >= max_frame) continue;
+        if (counts[a] >= max_body || counts[b] >= max_body) continue;
+        const double ma = s.mass[a], mb = s.mass[b];
+        const double M = __dadd_rn(ma, mb);
+        if (!(M < 1e-30)) {
+            const double vx = wavg(ma, s.vx[a], mb, s.vx[b], M);
+            const double vy = wavg(ma, s.vy[a], mb, s.vy[b], M);
+            const double vz = wavg(ma, s.vz[a], mb, s.vz[b], M);
+            const double x = wavg(ma, s.px[a], mb, s.px[b], M);
+            const double y = wavg(ma, s.py[a], mb, s.py[b], M);
+            const double z = wavg(ma, s.pz[a], mb, s.pz[b], M);
+            const int sv = (ma >= mb) ? a : b;
+            const int vc = (ma >= mb) ? b : a;
+            double rm;
+            if (density_merge) {
+                double sd = s.density[sv];
+                if (sd < 1e-30) sd = dm_density(s.mass[sv], s.radius[sv], min_radius);
+                rm = dm_radius(M, sd, min_radius);
+            } else {
+                const double ra = s.radius[a], rb = s.radius[b];
+                rm = cbrt(__dadd_rn(__dmul_rn(__dmul_rn(ra, ra), ra), __dmul_rn(__dmul_rn(rb, rb), rb)));
+            }
+            s.px[sv] = x; s.py[sv] = y; s.pz[sv] = z;
+            s.vx[sv] = vx; s.vy[sv] = vy; s.vz[sv] = vz;
+            s.mass[sv] = M;
+            s.radius[sv] = rm;
+            s.density[sv] = dm_density(M, rm, min_radius);
+            s.active[vc] = 0;
+        }
+        const int surv = (s.mass[a] > 0 && s.active[a]) ? a : b;
+        counts[surv]++;
+        total++;
+    }
+    *n_merges = total;
+}
+
+// ---- compaction ---------------------------------------------------------
+
+template <bool SCATTER>
+__global__ void __launch_bounds__(kCompThreads)
+k_compact(int n, State s, State d, int32_t* __restrict__ dest, uint32_t* look,
+          uint32_t* tile_ctr, int* n_kept, int* err) {
+    __shared__ int s_tile;
+    __shared__ uint32_t s_wtot[kCompThreads / 32];
+    __shared__ uint32_t s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_tile = (int)atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    const int tile = s_tile;
+    const int seg = tile * kCompTile + warp * (32 * kCompItems);
+    unsigned ball[kCompItems];
+    uint32_t wcount = 0;
+#pragma unroll
+    for (int k = 0; k < kCompItems; k++) {
+        const int i = seg + k * 32 + lane;
+        const bool keep = i < n && s.active[i] && s.mass[i] > 0.0;
+        ball[k] = __ballot_sync(0xFFFFFFFFu, keep);
+        wcount += __popc(ball[k]);
+    }
+    if (lane == 0) s_wtot[warp] = wcount;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int w = 0; w < kCompThreads / 32; w++) tot += s_wtot[w];
+        uint32_t excl = 0;
+        if (tile == 0) {
+            atomicExch(&look[0], kCFlagPre | tot);
+        } else {
+            atomicExch(&look[tile], kCFlagAgg | tot);
+            int j = tile - 1;
+            uint32_t spins = 0;
+            while (j >= 0) {
+                const uint32_t v = *(volatile uint32_t*)&look[j];
+                if ((v & ~kCValMask) == 0) {
+                    if (++spins > kSpinLimit) {
+                        dev_flag(err, kErrTimeout);
+                        break;
+                    }
+                    continue;
+                }
+                excl += v & kCValMask;
+                if ((v & ~kCValMask) == kCFlagPre) break;
+                j--;
+            }
+            __threadfence();
+            atomicExch(&look[tile], kCFlagPre | (excl + tot));
+        }
+        s_base = excl;
+        if (tile == (int)gridDim.x - 1) *n_kept = (int)(excl + tot);
+    }
+    __syncthreads();
+    uint32_t off = s_base;
+    for (int w = 0; w < warp; w++) off += s_wtot[w];
+#pragma unroll
+    for (int k = 0; k < kCompItems; k++) {
+        const int i = seg + k * 32 + lane;
+        const bool keep = (ball[k] >> lane) & 1u;
+        const uint32_t pos = off + __popc(ball[k] & lanemask_lt());
+        off += __popc(ball[k]);
+        if (i >= n) continue;
+        if (!SCATTER) {
+            dest[i] = keep ? (int32_t)pos : -1;
+            continue;
+        }
+        if (!keep) continue;
+        d.px[pos] = s.px[i]; d.py[pos] = s.py[i]; d.pz[pos] = s.pz[i];
+        d.vx[pos] = s.vx[i]; d.vy[pos] = s.vy[i]; d.vz[pos] = s.vz[i];
+        d.ax[pos] = s.ax[i]; d.ay[pos] = s.ay[i]; d.az[pos] = s.az[i];
+        d.mass[pos] = s.mass[i]; d.radius[pos] = s.radius[i]; d.density[pos] = s.density[i];
+        d.active[pos] = s.active[i]; d.collidable[pos] = s.collidable[i];
+        d.ids[pos] = s.ids[i];
+    }
+}
+
+static void launch_compact(cudaStream_t st, CollideBufs& b, int n, const State& s, const State& d,
+                           int32_t* dest, bool scatter, int* n_kept, int* err) {
+    const int tiles = ceil_div(n, kCompTile);
+    cudaMemsetAsync(b.look, 0, sizeof(uint32_t) * (size_t)tiles, st);
+    cudaMemsetAsync(b.tile_ctr, 0, sizeof(uint32_t), st);
+    if (scatter) k_compact<true><<<tiles, kCompThreads, 0, st>>>(n, s, d, dest, b.look, b.tile_ctr, n_kept, err);
+    else k_compact<false><<<tiles, kCompThreads, 0, st>>>(n, s, d, dest, b.look, b.tile_ctr, n_kept, err);
+}
+
+int compact_indices(cudaStream_t st, CollideBufs& b, int n, const uint8_t* active,
+                    const double* mass, int32_t* dest, int* n_kept_dev, int* err) {
+    if (n <= 0) return NB_OK;
+    State s{};
+    s.active = (uint8_t*)active;
+    s.mass = (double*)mass;
+    launch_compact(st, b, n, s, s, dest, false, n_kept_dev, err);
+    return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int collide_step(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* npairs, int* nmerge,
+                 int* nkept) {
+    int np = 0;
+    int r = broad_phase(st, b, a, true, &np);
+    if (r) return r;
+    *npairs = np;
+    *nmerge = 0;
+    const int w = np < b.pair_cap ? np : b.pair_cap;
+    cudaMemsetAsync(a.n_merges, 0, sizeof(int), st);
+    if (w > 0) {
+        cudaMemsetAsync(b.merge_count, 0, sizeof(int) * (size_t)a.n, st);
+        k_merge_sequential<<<1, 32, 0, st>>>(a.s, b.pair_keys, w, a.max_frame, a.max_body,
+                                             a.density_merge, a.min_radius, b.merge_count,
+                                             a.n_merges);
+    }
+    launch_compact(st, b, a.n, a.s, a.s_alt, nullptr, true, a.n_kept, a.err);
+    int host[2] = {0, 0};
+    if (cudaMemcpyAsync(&host[0], a.n_kept, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(&host[1], a.n_merges, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return NB_ERR_CUDA;
+    *nkept = host[0];
+    *nmerge = host[1];
+    return NB_OK;
+}
+
+}  // namespace nb

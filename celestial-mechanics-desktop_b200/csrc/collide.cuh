@@ -1,0 +1,53 @@
+// collide.cuh - collision broad phase, merge and stream compaction.
+#pragma once
+#include <functional>
+
+#include "bodies.cuh"
+#include "tree.cuh"
+
+namespace nb {
+
+struct CollideBufs {
+    int pair_cap;
+    uint64_t* pair_keys;   // (lo << 32 | hi), sorted after broad_phase
+    uint32_t* pair_vals;
+    uint64_t* pair_keys_alt;
+    uint32_t* pair_vals_alt;
+    void* pair_sort_ws;
+    int* merge_count;      // per row, merges this step
+    uint32_t* look;        // compaction look-back words
+    uint32_t* tile_ctr;
+    int capacity;
+};
+
+struct CollideArgs {
+    int n, n_active;
+    State s, s_alt;
+    uint64_t *keys0, *keys1;
+    uint32_t *vals0, *vals1;
+    void* sort_ws;
+    TreeBufs tree;
+    double4* sbody;
+    float* srad;
+    double* cube;
+    int leaf_cap;
+    int max_frame, max_body, density_merge;
+    double min_radius;
+    int *n_pairs, *n_kept, *n_merges;
+    int* err;
+    int sms;
+    unsigned long long* bbox_ord;
+    int* n_active_dev;
+};
+
+int collide_alloc(CollideBufs& b, int capacity, const std::function<int(void**, size_t)>& alloc);
+// All overlapping pairs of active, collidable rows, sorted; *np on the host.
+int broad_phase(cudaStream_t st, CollideBufs& b, CollideArgs& a, bool build_tree, int* np);
+// Broad phase + merges + compaction of c.s into c.s_alt.
+int collide_step(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* npairs, int* nmerge,
+                 int* nkept);
+// Destination rows of the order-preserving compaction (mask active && mass > 0).
+int compact_indices(cudaStream_t st, CollideBufs& b, int n, const uint8_t* active,
+                    const double* mass, int32_t* dest, int* n_kept_dev, int* err);
+
+}  // namespace nb

@@ -1,0 +1,15 @@
+// diag.cuh - energy / momentum diagnostics and the sampled FP64 audit.
+#pragma once
+#include "bodies.cuh"
+
+namespace nb {
+
+size_t diag_partial_bytes(int capacity);
+// out12: KE, Px, Py, Pz, Lx, Ly, Lz, sum m x, sum m y, sum m z, M, PE.
+// pe_mode 0: exact pair sum; 1: 1/2 sum m_i phi_i from `phi` (by row).
+void diagnostics(cudaStream_t st, int n, const State& s, double eps, int pe_mode,
+                 const double* phi, double* rows, double* part, double* out12);
+void direct_targets(cudaStream_t st, int n, const State& s, double eps, int nt,
+                    const int32_t* targets, double* out3);
+
+}  // namespace nb

@@ -1,0 +1,16 @@
+// direct.cuh - softened O(n^2) direct sums.
+#pragma once
+#include "common.cuh"
+
+namespace nb {
+
+// FP64, rows in caller order, bit-identical to CpuParallelBackend.
+void direct_fp64(cudaStream_t st, int n, const double* px, const double* py, const double* pz,
+                 const double* m, const double* rad, const uint8_t* act, double eps, bool shell,
+                 double* ax, double* ay, double* az);
+// FP32 pair math over the n sorted (active) bodies; writes rows sidx[k].
+void direct_fp32(cudaStream_t st, int n, const double4* sbody, const float* srad,
+                 const uint32_t* sidx, double eps, bool shell, double* ax, double* ay,
+                 double* az, unsigned long long* counter);
+
+}  // namespace nb

@@ -1,0 +1,865 @@
+// engine.cu - the C ABI (include/nbody_b200.h): handle, device buffers and
+// the force / step pipelines.
+//
+// The handle replaces the reference's global Engine* behind its C ABI
+// (engine/src/interop/native_api.cpp:9,30-124) and the GpuPool buffers
+// (engine/src/memory/gpu_pool.cu:79-124): one CUDA stream and fixed-capacity
+// device arrays per handle, allocated once in nb_create, so no call allocates
+// device memory on the hot path.  Every entry point returns a status; no C++
+// exception leaves this file; there is no CPU fallback.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bodies.cuh"
+#include "collide.cuh"
+#include "diag.cuh"
+#include "direct.cuh"
+#include "sort.cuh"
+#include "tree.cuh"
+#include "walk.cuh"
+
+namespace {
+
+// Device scalars of a handle (one allocation).
+struct Scal {
+    unsigned long long bbox_ord[6];
+    int n_active;
+    unsigned group_ctr;
+    double cube[4];
+    double cube_in[4];
+    int err[nb::kErrCount];
+    unsigned long long counters[4];
+    double diag[16];
+    int n_pairs;
+    int n_kept;
+    int n_merges;
+    int pad;
+};
+
+}  // namespace
+
+struct nb_engine {
+    int device = 0;
+    int sms = 148;
+    int capacity = 0;
+    cudaStream_t st = nullptr;
+    char err_msg[512] = {0};
+    // parameters
+    double theta = 0.5;
+    int leaf_cap = 8;
+    int max_merges_frame = 64;
+    int max_merges_body = 2;
+    double min_radius = 1e-6;
+    int density_merge = 1;
+    int timing = 1;
+    double mac_budget = -3.0;
+    int group_bodies = 32;
+    // device-resident state
+    int n = 0;
+    int n_active = 0;
+    bool has_state = false;
+    nb::State s{};
+    nb::State s_alt{};  // compaction target
+    // work buffers
+    uint64_t *keys0 = nullptr, *keys1 = nullptr;
+    uint32_t *vals0 = nullptr, *vals1 = nullptr;
+    void* sort_ws = nullptr;
+    double4* sbody = nullptr;
+    float* srad = nullptr;
+    void* tree_mem = nullptr;
+    nb::TreeBufs tree{};
+    nb::WalkConfig wcfg{};
+    int* front = nullptr;
+    double* rows = nullptr;
+    double* part = nullptr;
+    double* phi = nullptr;
+    int32_t* targets = nullptr;
+    double* tgt_out = nullptr;
+    nb::CollideBufs col{};
+    Scal* scal = nullptr;
+    std::vector<void*> allocs;
+    // timing
+    cudaEvent_t ev[6] = {};
+    bool ev_valid = false;
+    bool ev_tree = false;
+    double timings[NB_T_COUNT] = {0};
+    int64_t counters[NB_C_COUNT] = {0};
+};
+
+namespace {
+
+int fail(nb_engine* h, int code, const char* fmt, ...) {
+    if (h) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(h->err_msg, sizeof(h->err_msg), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+#define NB_CUDA(h, call)                                                                \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail((h), NB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+int dalloc(nb_engine* h, T** p, size_t count) {
+    size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess)
+        return fail(h, NB_ERR_CUDA, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    h->allocs.push_back(q);
+    *p = (T*)q;
+    return NB_OK;
+}
+
+int alloc_state(nb_engine* h, nb::State& s, int cap) {
+    int r = NB_OK;
+    double** d[] = {&s.px, &s.py, &s.pz, &s.vx, &s.vy, &s.vz, &s.ax, &s.ay, &s.az,
+                    &s.mass, &s.radius, &s.density};
+    for (double** p : d)
+        if ((r = dalloc(h, p, cap))) return r;
+    if ((r = dalloc(h, &s.active, cap))) return r;
+    if ((r = dalloc(h, &s.collidable, cap))) return r;
+    return dalloc(h, &s.ids, cap);
+}
+
+// Collect the device error word and the last CUDA error after a sync.
+int check_device(nb_engine* h) {
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) return fail(h, NB_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, NB_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    int err[nb::kErrCount];
+    e = cudaMemcpy(err, h->scal->err, sizeof(err), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(h, NB_ERR_CUDA, "error word: %s", cudaGetErrorString(e));
+    cudaMemsetAsync(h->scal->err, 0, sizeof(err), h->st);
+    if (err[nb::kErrNonFinite]) return fail(h, NB_ERR_NONFINITE, "non-finite position or mass");
+    if (err[nb::kErrTimeout]) return fail(h, NB_ERR_TIMEOUT, "a bounded device wait expired");
+    if (err[nb::kErrOverflow])
+        return fail(h, NB_ERR_STACK_OVERFLOW, "tree-walk frontier overflow");
+    if (err[nb::kErrCapacity]) return fail(h, NB_ERR_CAPACITY, "device buffer capacity exceeded");
+    return NB_OK;
+}
+
+int upload(nb_engine* h, void* dst, const void* src, size_t bytes) {
+    if (!src || bytes == 0) return NB_OK;
+    NB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->st));
+    return NB_OK;
+}
+
+int download(nb_engine* h, void* dst, const void* src, size_t bytes) {
+    if (!dst || bytes == 0) return NB_OK;
+    NB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->st));
+    return NB_OK;
+}
+
+int check_n(nb_engine* h, int n) {
+    if (n < 0) return fail(h, NB_ERR_INVALID_ARG, "n = %d is negative", n);
+    if (n > h->capacity)
+        return fail(h, NB_ERR_CAPACITY, "n = %d exceeds the handle capacity %d", n, h->capacity);
+    return NB_OK;
+}
+
+void record(nb_engine* h, int k) {
+    if (h->timing) cudaEventRecord(h->ev[k], h->st);
+}
+
+// Forces for the current device rows.  kick: fuse the first half kick and
+// the drift of a Verlet step into the bounding-box pass.
+int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
+    const int mode = flags & NB_MODE_MASK;
+    const bool shell = (flags & NB_FLAG_SHELL_THEOREM) != 0;
+    const int n = h->n;
+    Scal* sc = h->scal;
+    record(h, 0);
+    nb::launch_kick_drift_bbox(h->st, n, h->s, kick, dt, sc->bbox_ord, &sc->n_active, sc->err);
+    cudaMemsetAsync(sc->counters, 0, sizeof(sc->counters), h->st);
+    h->ev_tree = false;
+    if (mode == NB_MODE_DIRECT_FP64) {
+        record(h, 1);
+        record(h, 2);
+        nb::direct_fp64(h->st, n, h->s.px, h->s.py, h->s.pz, h->s.mass, h->s.radius,
+                        h->s.active, eps, shell, h->s.ax, h->s.ay, h->s.az);
+        record(h, 3);
+        h->counters[NB_C_BODY_INTERACTIONS] = (int64_t)h->n_active * (h->n_active - 1);
+        h->counters[NB_C_CELL_INTERACTIONS] = 0;
+        h->ev_valid = h->timing != 0;
+        return NB_OK;
+    }
+    const int na = h->n_active;
+    nb::launch_zero_acc(h->st, n, h->s);
+    nb::launch_cube(h->st, sc->bbox_ord, nullptr, sc->cube);
+    nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws);
+    nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err,
+                   h->sms);
+    nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, shell ? h->srad : nullptr);
+    record(h, 1);
+    if (mode == NB_MODE_DIRECT) {
+        record(h, 2);
+        nb::direct_fp32(h->st, na, h->sbody, h->srad, h->vals0, eps, shell, h->s.ax, h->s.ay,
+                        h->s.az, &sc->counters[1]);
+    } else if (mode == NB_MODE_BARNES_HUT || mode == NB_MODE_BARNES_HUT_REF) {
+        const bool ref = mode == NB_MODE_BARNES_HUT_REF;
+        nb::tree_build(h->st, h->tree, na, h->keys0, h->sbody, shell ? h->srad : nullptr, sc->cube,
+                       ref ? 1 : h->leaf_cap, sc->err);
+        h->ev_tree = true;
+        record(h, 2);
+        nb::WalkArgs a{};
+        a.n = na;
+        a.sbody = h->sbody;
+        a.srad = h->srad;
+        a.skeys = h->keys0;
+        a.sidx = h->vals0;
+        a.t = h->tree;
+        a.eps2 = eps * eps;
+        a.ax = h->s.ax;
+        a.ay = h->s.ay;
+        a.az = h->s.az;
+        a.pot = nullptr;
+        a.front = h->front;
+        a.group_ctr = &sc->group_ctr;
+        a.counters = sc->counters;
+        a.err = sc->err;
+        if (ref) {
+            const double te = h->theta < 0.2 ? 0.2 : h->theta;  // barnes_hut_solver.cpp:16
+            a.theta2 = te * te;
+            nb::walk_reference(h->st, a, shell);
+        } else {
+            a.theta2 = h->theta * h->theta;
+            nb::walk_group(h->st, h->wcfg, a, (flags & NB_FLAG_NO_QUADRUPOLE) == 0, shell, false);
+        }
+    } else {
+        return fail(h, NB_ERR_INVALID_ARG, "unknown force mode %d", mode);
+    }
+    record(h, 3);
+    h->ev_valid = h->timing != 0;
+    return NB_OK;
+}
+
+void collect_counters(nb_engine* h) {
+    unsigned long long c[4];
+    if (cudaMemcpy(c, h->scal->counters, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) {
+        h->counters[NB_C_CELL_INTERACTIONS] = (int64_t)c[0];
+        h->counters[NB_C_BODY_INTERACTIONS] = (int64_t)c[1];
+    }
+    int nn = 0;
+    if (h->ev_tree && cudaMemcpy(&nn, h->tree.n_nodes, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess)
+        h->counters[NB_C_NODES] = nn;
+    h->counters[NB_C_ACTIVE] = h->n_active;
+}
+
+int count_active_host(const uint8_t* a, int n) {
+    int c = 0;
+    for (int i = 0; i < n; i++) c += a[i] != 0;
+    return c;
+}
+
+// Upload positions / masses / radii / active into the device rows (the
+// host-array entry points stage through the state arrays).
+int stage_bodies(nb_engine* h, int n, const double* px, const double* py, const double* pz,
+                 const double* mass, const double* radius, const uint8_t* active) {
+    int r;
+    if ((r = check_n(h, n))) return r;
+    if (n > 0 && (!px || !py || !pz || !active))
+        return fail(h, NB_ERR_INVALID_ARG, "null position or active array");
+    const size_t d = sizeof(double) * (size_t)n;
+    if ((r = upload(h, h->s.px, px, d)) || (r = upload(h, h->s.py, py, d)) ||
+        (r = upload(h, h->s.pz, pz, d)) || (r = upload(h, h->s.active, active, (size_t)n)))
+        return r;
+    if (mass) {
+        if ((r = upload(h, h->s.mass, mass, d))) return r;
+    } else {
+        NB_CUDA(h, cudaMemsetAsync(h->s.mass, 0, d, h->st));
+    }
+    if (radius) {
+        if ((r = upload(h, h->s.radius, radius, d))) return r;
+    } else {
+        NB_CUDA(h, cudaMemsetAsync(h->s.radius, 0, d, h->st));
+    }
+    h->n = n;
+    h->n_active = n > 0 ? count_active_host(active, n) : 0;
+    h->has_state = false;
+    return NB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+NB_API const char* nb_version(void) { return "nbody_b200 1.0 (sm_100a)"; }
+
+NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
+    if (!out) return NB_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (capacity <= 0) return NB_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return NB_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return NB_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return NB_ERR_NO_DEVICE;
+    if (prop.major != 10) return NB_ERR_NO_DEVICE;  // built for sm_100a only
+    nb_engine* h = new (std::nothrow) nb_engine();
+    if (!h) return NB_ERR_CAPACITY;
+    h->device = device;
+    h->sms = prop.multiProcessorCount;
+    h->capacity = capacity;
+    int r = NB_OK;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return NB_ERR_CUDA;
+    }
+    nb::sort_init();
+    nb::walk_init(h->sms, h->wcfg);
+    const size_t cap = (size_t)capacity;
+    do {
+        if ((r = alloc_state(h, h->s, capacity))) break;
+        if ((r = alloc_state(h, h->s_alt, capacity))) break;
+        if ((r = dalloc(h, &h->keys0, cap)) || (r = dalloc(h, &h->keys1, cap))) break;
+        if ((r = dalloc(h, &h->vals0, cap)) || (r = dalloc(h, &h->vals1, cap))) break;
+        if ((r = dalloc(h, (char**)&h->sort_ws, nb::sort_workspace_bytes(capacity)))) break;
+        if ((r = dalloc(h, &h->sbody, cap)) || (r = dalloc(h, &h->srad, cap))) break;
+        if ((r = dalloc(h, (char**)&h->tree_mem, nb::tree_bytes(capacity)))) break;
+        nb::tree_carve(h->tree, h->tree_mem, capacity);
+        if ((r = dalloc(h, (char**)&h->front, nb::walk_front_bytes(h->wcfg)))) break;
+        if ((r = dalloc(h, &h->rows, cap)) || (r = dalloc(h, &h->phi, cap))) break;
+        if ((r = dalloc(h, (char**)&h->part, nb::diag_partial_bytes(capacity)))) break;
+        if ((r = dalloc(h, &h->targets, cap)) || (r = dalloc(h, &h->tgt_out, 3 * cap))) break;
+        if ((r = nb::collide_alloc(h->col, capacity, [h](void** p, size_t b) {
+                 return dalloc(h, (char**)p, b);
+             })))
+            break;
+        if ((r = dalloc(h, &h->scal, 1))) break;
+        if (cudaMemset(h->scal, 0, sizeof(Scal)) != cudaSuccess) { r = NB_ERR_CUDA; break; }
+        for (auto& e : h->ev)
+            if (cudaEventCreate(&e) != cudaSuccess) { r = NB_ERR_CUDA; break; }
+    } while (0);
+    if (r != NB_OK) {
+        nb_destroy(h);
+        return r;
+    }
+    *out = h;
+    return NB_OK;
+}
+
+NB_API int32_t nb_destroy(nb_engine* h) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    if (h->st) cudaStreamSynchronize(h->st);
+    for (void* p : h->allocs) cudaFree(p);
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+    return NB_OK;
+}
+
+NB_API const char* nb_last_error(const nb_engine* h) { return h ? h->err_msg : "null handle"; }
+
+NB_API void* nb_stream(nb_engine* h) { return h ? (void*)h->st : nullptr; }
+
+NB_API int32_t nb_set_param_f64(nb_engine* h, int32_t p, double v) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    switch (p) {
+        case NB_PARAM_THETA:
+            if (!(v >= 0.0)) return fail(h, NB_ERR_INVALID_ARG, "theta must be >= 0");
+            h->theta = v;
+            return NB_OK;
+        case NB_PARAM_MIN_RADIUS: h->min_radius = v; return NB_OK;
+        case NB_PARAM_MAC_BUDGET: h->mac_budget = v; return NB_OK;
+        default: return fail(h, NB_ERR_INVALID_ARG, "unknown f64 parameter %d", p);
+    }
+}
+
+NB_API int32_t nb_set_param_i32(nb_engine* h, int32_t p, int32_t v) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    switch (p) {
+        case NB_PARAM_LEAF_CAPACITY:
+            if (v < 1 || v > 64) return fail(h, NB_ERR_INVALID_ARG, "leaf capacity must be 1..64");
+            h->leaf_cap = v;
+            return NB_OK;
+        case NB_PARAM_MAX_MERGES_FRAME: h->max_merges_frame = v; return NB_OK;
+        case NB_PARAM_MAX_MERGES_BODY: h->max_merges_body = v; return NB_OK;
+        case NB_PARAM_DENSITY_MERGE: h->density_merge = v; return NB_OK;
+        case NB_PARAM_TIMING: h->timing = v; return NB_OK;
+        case NB_PARAM_GROUP_BODIES:
+            if (v != 32) return fail(h, NB_ERR_INVALID_ARG, "group size must be 32");
+            h->group_bodies = v;
+            return NB_OK;
+        default: return fail(h, NB_ERR_INVALID_ARG, "unknown i32 parameter %d", p);
+    }
+}
+
+NB_API int32_t nb_get_timings(const nb_engine* hc, double* out, int32_t n) {
+    nb_engine* h = const_cast<nb_engine*>(hc);
+    if (!h || !out) return NB_ERR_INVALID_ARG;
+    if (h->ev_valid) {
+        float t[3] = {0, 0, 0};
+        cudaEventSynchronize(h->ev[3]);
+        cudaEventElapsedTime(&t[0], h->ev[0], h->ev[1]);
+        cudaEventElapsedTime(&t[1], h->ev[1], h->ev[2]);
+        cudaEventElapsedTime(&t[2], h->ev[2], h->ev[3]);
+        h->timings[NB_T_SORT] = t[0];
+        h->timings[NB_T_TREE] = t[1];
+        h->timings[NB_T_BUILD] = t[0] + t[1];
+        h->timings[NB_T_TRAVERSAL] = t[2];
+        h->timings[NB_T_TOTAL] = t[0] + t[1] + t[2];
+        h->ev_valid = false;
+    }
+    for (int i = 0; i < n && i < NB_T_COUNT; i++) out[i] = h->timings[i];
+    return NB_OK;
+}
+
+NB_API int32_t nb_get_counters(const nb_engine* h, int64_t* out, int32_t n) {
+    if (!h || !out) return NB_ERR_INVALID_ARG;
+    for (int i = 0; i < n && i < NB_C_COUNT; i++) out[i] = h->counters[i];
+    return NB_OK;
+}
+
+NB_API int32_t nb_compute_forces(nb_engine* h, int32_t n, const double* px, const double* py,
+                                 const double* pz, const double* mass, const double* radius,
+                                 const uint8_t* active, double softening, int32_t flags,
+                                 double* ax, double* ay, double* az) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, NB_ERR_CUDA, "cudaSetDevice");
+    if ((flags & NB_FLAG_SHELL_THEOREM) && !radius)
+        return fail(h, NB_ERR_INVALID_ARG, "shell theorem needs radii");
+    if (!mass && n > 0) return fail(h, NB_ERR_INVALID_ARG, "null mass array");
+    if (n > 0 && (!ax || !ay || !az)) return fail(h, NB_ERR_INVALID_ARG, "null output array");
+    int r;
+    if ((r = stage_bodies(h, n, px, py, pz, mass, radius, active))) return r;
+    if (n == 0) return NB_OK;
+    if ((r = force_pipeline(h, flags, softening, false, 0.0))) return r;
+    const size_t d = sizeof(double) * (size_t)n;
+    if ((r = download(h, ax, h->s.ax, d)) || (r = download(h, ay, h->s.ay, d)) ||
+        (r = download(h, az, h->s.az, d)))
+        return r;
+    if ((r = check_device(h))) return r;
+    collect_counters(h);
+    return NB_OK;
+}
+
+NB_API int32_t nb_set_state(nb_engine* h, int32_t n, const double* px, const double* py,
+                            const double* pz, const double* vx, const double* vy, const double* vz,
+                            const double* mass, const double* radius, const double* density,
+                            const uint8_t* active, const uint8_t* collidable,
+                            const double* oax, const double* oay, const double* oaz) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, NB_ERR_CUDA, "cudaSetDevice");
+    int r;
+    if (n > 0 && (!vx || !vy || !vz || !mass))
+        return fail(h, NB_ERR_INVALID_ARG, "null velocity or mass array");
+    if ((r = stage_bodies(h, n, px, py, pz, mass, radius, active))) return r;
+    const size_t d = sizeof(double) * (size_t)n;
+    if ((r = upload(h, h->s.vx, vx, d)) || (r = upload(h, h->s.vy, vy, d)) ||
+        (r = upload(h, h->s.vz, vz, d)))
+        return r;
+    double* acc[3] = {h->s.ax, h->s.ay, h->s.az};
+    const double* old[3] = {oax, oay, oaz};
+    for (int k = 0; k < 3; k++) {
+        if (old[k]) {
+            if ((r = upload(h, acc[k], old[k], d))) return r;
+        } else {
+            NB_CUDA(h, cudaMemsetAsync(acc[k], 0, d, h->st));
+        }
+    }
+    if (density) {
+        if ((r = upload(h, h->s.density, density, d))) return r;
+    } else {
+        NB_CUDA(h, cudaMemsetAsync(h->s.density, 0, d, h->st));
+    }
+    if (collidable) {
+        if ((r = upload(h, h->s.collidable, collidable, (size_t)n))) return r;
+    } else {
+        NB_CUDA(h, cudaMemsetAsync(h->s.collidable, 1, (size_t)n, h->st));
+    }
+    std::vector<int32_t> ids((size_t)n);
+    for (int i = 0; i < n; i++) ids[i] = i;
+    if ((r = upload(h, h->s.ids, ids.data(), sizeof(int32_t) * (size_t)n))) return r;
+    if ((r = check_device(h))) return r;
+    h->has_state = true;
+    return NB_OK;
+}
+
+NB_API int32_t nb_get_state(nb_engine* h, int32_t* n_out, double* px, double* py, double* pz,
+                            double* vx, double* vy, double* vz, double* ax, double* ay,
+                            double* az, double* mass, double* radius, uint8_t* active,
+                            int32_t* ids) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NB_ERR_STATE, "no device-resident state");
+    cudaSetDevice(h->device);
+    const int n = h->n;
+    if (n_out) *n_out = n;
+    const size_t d = sizeof(double) * (size_t)n;
+    int r;
+    if ((r = download(h, px, h->s.px, d)) || (r = download(h, py, h->s.py, d)) ||
+        (r = download(h, pz, h->s.pz, d)) || (r = download(h, vx, h->s.vx, d)) ||
+        (r = download(h, vy, h->s.vy, d)) || (r = download(h, vz, h->s.vz, d)) ||
+        (r = download(h, ax, h->s.ax, d)) || (r = download(h, ay, h->s.ay, d)) ||
+        (r = download(h, az, h->s.az, d)) || (r = download(h, mass, h->s.mass, d)) ||
+        (r = download(h, radius, h->s.radius, d)) ||
+        (r = download(h, active, h->s.active, (size_t)n)) ||
+        (r = download(h, ids, h->s.ids, sizeof(int32_t) * (size_t)n)))
+        return r;
+    return check_device(h);
+}
+
+NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softening, int32_t flags) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NB_ERR_STATE, "nb_step before nb_set_state");
+    if (n_steps < 0) return fail(h, NB_ERR_INVALID_ARG, "negative step count");
+    cudaSetDevice(h->device);
+    const bool collide = (flags & NB_FLAG_COLLISIONS) != 0;
+    int r;
+    for (int k = 0; k < n_steps; k++) {
+        if ((r = force_pipeline(h, flags, softening, true, dt))) return r;
+        nb::launch_kick(h->st, h->n, h->s, dt);
+        if (collide) {
+            nb::CollideArgs c{};
+            c.n = h->n;
+            c.n_active = h->n_active;
+            c.s = h->s;
+            c.s_alt = h->s_alt;
+            c.keys0 = h->keys0; c.keys1 = h->keys1; c.vals0 = h->vals0; c.vals1 = h->vals1;
+            c.sort_ws = h->sort_ws;
+            c.tree = h->tree;
+            c.sbody = h->sbody;
+            c.srad = h->srad;
+            c.cube = h->scal->cube;
+            c.leaf_cap = h->leaf_cap;
+            c.max_frame = h->max_merges_frame;
+            c.max_body = h->max_merges_body;
+            c.density_merge = h->density_merge;
+            c.min_radius = h->min_radius;
+            c.n_pairs = &h->scal->n_pairs;
+            c.n_kept = &h->scal->n_kept;
+            c.n_merges = &h->scal->n_merges;
+            c.err = h->scal->err;
+            c.sms = h->sms;
+            c.bbox_ord = h->scal->bbox_ord;
+            c.n_active_dev = &h->scal->n_active;
+            int npairs = 0, nmerge = 0, nkept = 0;
+            if ((r = nb::collide_step(h->st, h->col, c, &npairs, &nmerge, &nkept)))
+                return fail(h, r, "collision step failed");
+            std::swap(h->s, h->s_alt);
+            h->n = nkept;
+            h->n_active = nkept;
+            h->counters[NB_C_PAIRS] = npairs;
+            h->counters[NB_C_MERGES] = nmerge;
+            if ((r = check_device(h))) return r;
+        }
+    }
+    if ((r = check_device(h))) return r;
+    collect_counters(h);
+    return NB_OK;
+}
+
+NB_API int32_t nb_diagnostics(nb_engine* h, double softening, int32_t pe_mode, double* out13) {
+    if (!h || !out13) return NB_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NB_ERR_STATE, "no device-resident state");
+    cudaSetDevice(h->device);
+    int r;
+    if (pe_mode == 1) {
+        // tree potential: a walk with the potential accumulated
+        const int n = h->n;
+        Scal* sc = h->scal;
+        nb::launch_kick_drift_bbox(h->st, n, h->s, false, 0.0, sc->bbox_ord, &sc->n_active, sc->err);
+        nb::launch_cube(h->st, sc->bbox_ord, nullptr, sc->cube);
+        nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws);
+        nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err, h->sms);
+        nb::launch_gather(h->st, h->n_active, h->s, h->vals0, h->sbody, nullptr);
+        nb::tree_build(h->st, h->tree, h->n_active, h->keys0, h->sbody, nullptr, sc->cube,
+                       h->leaf_cap, sc->err);
+        NB_CUDA(h, cudaMemsetAsync(h->phi, 0, sizeof(double) * (size_t)n, h->st));
+        // the walk writes acc too: keep the state's acc in the alt buffers
+        nb::WalkArgs a{};
+        a.n = h->n_active;
+        a.sbody = h->sbody;
+        a.sidx = h->vals0;
+        a.skeys = h->keys0;
+        a.t = h->tree;
+        a.theta2 = h->theta * h->theta;
+        a.eps2 = softening * softening;
+        a.ax = h->s_alt.ax;
+        a.ay = h->s_alt.ay;
+        a.az = h->s_alt.az;
+        a.pot = h->phi;
+        a.front = h->front;
+        a.group_ctr = &sc->group_ctr;
+        a.counters = nullptr;
+        a.err = sc->err;
+        nb::walk_group(h->st, h->wcfg, a, true, false, true);
+    }
+    double out[12];
+    nb::diagnostics(h->st, h->n, h->s, softening, pe_mode, h->phi, h->rows, h->part, h->scal->diag);
+    if ((r = download(h, out, h->scal->diag, sizeof(out)))) return r;
+    if ((r = check_device(h))) return r;
+    const double M = out[10];
+    out13[0] = out[0];
+    out13[1] = out[11];
+    out13[2] = out[0] + out[11];
+    for (int k = 0; k < 6; k++) out13[3 + k] = out[1 + k];
+    for (int k = 0; k < 3; k++) out13[9 + k] = M > 0 ? out[7 + k] / M : 0.0;
+    out13[12] = M;
+    return NB_OK;
+}
+
+NB_API int32_t nb_force_error(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
+                              int32_t flags, double* out3) {
+    (void)flags;
+    if (!h || !out3) return NB_ERR_INVALID_ARG;
+    if (!h->has_state && h->n == 0) return fail(h, NB_ERR_STATE, "no bodies on the device");
+    cudaSetDevice(h->device);
+    const int n = h->n;
+    std::vector<uint8_t> act((size_t)n);
+    int r;
+    if ((r = download(h, act.data(), h->s.active, (size_t)n))) return r;
+    if ((r = check_device(h))) return r;
+    std::vector<int32_t> cand;
+    for (int i = 0; i < n; i++)
+        if (act[i]) cand.push_back(i);
+    // SplitMix64-driven partial Fisher-Yates: uniform sample without replacement
+    uint64_t x = seed;
+    auto next = [&x]() {
+        uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    int ns = (n_samples <= 0 || n_samples >= (int)cand.size()) ? (int)cand.size() : n_samples;
+    if (ns < (int)cand.size())
+        for (int k = 0; k < ns; k++) {
+            uint64_t j = k + next() % (uint64_t)(cand.size() - k);
+            std::swap(cand[k], cand[j]);
+        }
+    cand.resize(ns);
+    if ((r = upload(h, h->targets, cand.data(), sizeof(int32_t) * (size_t)ns))) return r;
+    nb::direct_targets(h->st, n, h->s, softening, ns, h->targets, h->tgt_out);
+    std::vector<double> ref((size_t)ns * 3), ax((size_t)n), ay((size_t)n), az((size_t)n);
+    if ((r = download(h, ref.data(), h->tgt_out, sizeof(double) * 3 * (size_t)ns))) return r;
+    if ((r = download(h, ax.data(), h->s.ax, sizeof(double) * (size_t)n)) ||
+        (r = download(h, ay.data(), h->s.ay, sizeof(double) * (size_t)n)) ||
+        (r = download(h, az.data(), h->s.az, sizeof(double) * (size_t)n)))
+        return r;
+    if ((r = check_device(h))) return r;
+    // ForceErrorAnalyzer.CompareForces statistics (ForceErrorAnalyzer.cs:100-134)
+    double se = 0, se2 = 0, mx = 0;
+    int c = 0;
+    for (int k = 0; k < ns; k++) {
+        const int i = cand[k];
+        const double ex = ref[3 * k], ey = ref[3 * k + 1], ez = ref[3 * k + 2];
+        const double em = sqrt(ex * ex + ey * ey + ez * ez);
+        if (em < 1e-30) continue;
+        const double dx = ax[i] - ex, dy = ay[i] - ey, dz = az[i] - ez;
+        const double e = sqrt(dx * dx + dy * dy + dz * dz) / em;
+        se += e;
+        se2 += e * e;
+        if (e > mx) mx = e;
+        c++;
+    }
+    out3[0] = c ? se / c : 0;
+    out3[1] = mx;
+    out3[2] = c ? sqrt(se2 / c) : 0;
+    return NB_OK;
+}
+
+NB_API int32_t nb_morton_keys(nb_engine* h, int32_t n, const double* px, const double* py,
+                              const double* pz, const uint8_t* active, int32_t mode,
+                              const double* cube4, uint64_t* keys, int32_t* idx,
+                              double* cube4_out) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    if (mode != 0 && mode != 1) return fail(h, NB_ERR_INVALID_ARG, "mode must be 0 or 1");
+    cudaSetDevice(h->device);
+    int r;
+    if ((r = stage_bodies(h, n, px, py, pz, nullptr, nullptr, active))) return r;
+    if (n == 0) return NB_OK;
+    Scal* sc = h->scal;
+    nb::launch_kick_drift_bbox(h->st, n, h->s, false, 0.0, sc->bbox_ord, &sc->n_active, sc->err);
+    if (mode == 0) {
+        nb::launch_keys_aabb(h->st, n, h->s, sc->bbox_ord, h->keys0, h->vals0);
+    } else {
+        if (cube4 && (r = upload(h, sc->cube_in, cube4, sizeof(double) * 4))) return r;
+        nb::launch_cube(h->st, sc->bbox_ord, cube4 ? sc->cube_in : nullptr, sc->cube);
+        nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws);
+        if ((r = download(h, cube4_out, sc->cube, sizeof(double) * 4))) return r;
+    }
+    if ((r = download(h, keys, h->keys0, sizeof(uint64_t) * (size_t)n)) ||
+        (r = download(h, idx, h->vals0, sizeof(int32_t) * (size_t)n)))
+        return r;
+    return check_device(h);
+}
+
+NB_API int32_t nb_sort_pairs(nb_engine* h, int32_t n, uint64_t* keys, int32_t* values) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    int r;
+    if ((r = check_n(h, n))) return r;
+    if (n <= 1) return NB_OK;
+    if ((r = upload(h, h->keys0, keys, sizeof(uint64_t) * (size_t)n)) ||
+        (r = upload(h, h->vals0, values, sizeof(int32_t) * (size_t)n)))
+        return r;
+    nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, false,
+                   h->scal->err, h->sms);
+    if ((r = download(h, keys, h->keys0, sizeof(uint64_t) * (size_t)n)) ||
+        (r = download(h, values, h->vals0, sizeof(int32_t) * (size_t)n)))
+        return r;
+    h->has_state = false;
+    return check_device(h);
+}
+
+NB_API int32_t nb_build_octree(nb_engine* h, int32_t n, const double* px, const double* py,
+                               const double* pz, const double* mass, const uint8_t* active,
+                               const double* cube4, int32_t leaf_capacity, int32_t max_nodes,
+                               int32_t* n_nodes, int32_t* level, int32_t* first_child,
+                               int32_t* n_children, int32_t* body_first, int32_t* body_count,
+                               double* node_mass, double* com3, float* quad6,
+                               int32_t* sorted_idx, uint64_t* sorted_keys) {
+    if (!h || !n_nodes) return NB_ERR_INVALID_ARG;
+    if (leaf_capacity < 1 || leaf_capacity > 64)
+        return fail(h, NB_ERR_INVALID_ARG, "leaf capacity must be 1..64");
+    cudaSetDevice(h->device);
+    int r;
+    if ((r = stage_bodies(h, n, px, py, pz, mass, nullptr, active))) return r;
+    *n_nodes = 0;
+    if (n == 0) return NB_OK;
+    Scal* sc = h->scal;
+    nb::launch_kick_drift_bbox(h->st, n, h->s, false, 0.0, sc->bbox_ord, &sc->n_active, sc->err);
+    if (cube4 && (r = upload(h, sc->cube_in, cube4, sizeof(double) * 4))) return r;
+    nb::launch_cube(h->st, sc->bbox_ord, cube4 ? sc->cube_in : nullptr, sc->cube);
+    nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws);
+    nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err,
+                   h->sms);
+    const int na = h->n_active;
+    nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, nullptr);
+    nb::tree_build(h->st, h->tree, na, h->keys0, h->sbody, nullptr, sc->cube, leaf_capacity,
+                   sc->err);
+    int nn = 0;
+    if ((r = download(h, &nn, h->tree.n_nodes, sizeof(int)))) return r;
+    if ((r = check_device(h))) return r;
+    *n_nodes = nn;
+    if (nn > max_nodes) return fail(h, NB_ERR_CAPACITY, "%d nodes > max_nodes %d", nn, max_nodes);
+    std::vector<int4> link((size_t)nn);
+    std::vector<double4> com((size_t)nn);
+    std::vector<float4> q0((size_t)nn), q1((size_t)nn);
+    std::vector<int> lev((size_t)nn);
+    if ((r = download(h, link.data(), h->tree.link, sizeof(int4) * (size_t)nn)) ||
+        (r = download(h, com.data(), h->tree.com, sizeof(double4) * (size_t)nn)) ||
+        (r = download(h, q0.data(), h->tree.q0, sizeof(float4) * (size_t)nn)) ||
+        (r = download(h, q1.data(), h->tree.q1, sizeof(float4) * (size_t)nn)) ||
+        (r = download(h, lev.data(), h->tree.level, sizeof(int) * (size_t)nn)) ||
+        (r = download(h, sorted_idx, h->vals0, sizeof(int32_t) * (size_t)n)) ||
+        (r = download(h, sorted_keys, h->keys0, sizeof(uint64_t) * (size_t)n)))
+        return r;
+    if ((r = check_device(h))) return r;
+    for (int k = 0; k < nn; k++) {
+        if (level) level[k] = lev[k];
+        if (first_child) first_child[k] = link[k].x;
+        if (n_children) n_children[k] = link[k].y;
+        if (body_first) body_first[k] = link[k].z;
+        if (body_count) body_count[k] = link[k].w;
+        if (node_mass) node_mass[k] = com[k].w;
+        if (com3) {
+            com3[3 * k] = com[k].x;
+            com3[3 * k + 1] = com[k].y;
+            com3[3 * k + 2] = com[k].z;
+        }
+        if (quad6) {
+            const float qxx = q0[k].x, qyy = q0[k].y;
+            const float v[6] = {qxx, qyy, -(qxx + qyy), q0[k].z, q0[k].w, q1[k].x};
+            for (int j = 0; j < 6; j++) quad6[6 * k + j] = v[j];
+        }
+    }
+    h->ev_tree = true;
+    return NB_OK;
+}
+
+NB_API int32_t nb_compact_indices(nb_engine* h, int32_t n, const uint8_t* active,
+                                  const double* mass, int32_t* dest, int32_t* n_kept) {
+    if (!h || !n_kept) return NB_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    int r;
+    if ((r = check_n(h, n))) return r;
+    *n_kept = 0;
+    if (n == 0) return NB_OK;
+    if ((r = upload(h, h->s.active, active, (size_t)n)) ||
+        (r = upload(h, h->s.mass, mass, sizeof(double) * (size_t)n)))
+        return r;
+    int kept = 0;
+    if ((r = nb::compact_indices(h->st, h->col, n, h->s.active, h->s.mass, (int32_t*)h->vals1,
+                                 &h->scal->n_kept, h->scal->err)))
+        return fail(h, r, "compaction failed");
+    if ((r = download(h, dest, h->vals1, sizeof(int32_t) * (size_t)n)) ||
+        (r = download(h, &kept, &h->scal->n_kept, sizeof(int))))
+        return r;
+    if ((r = check_device(h))) return r;
+    *n_kept = kept;
+    h->has_state = false;
+    return NB_OK;
+}
+
+NB_API int32_t nb_broad_phase(nb_engine* h, int32_t n, const double* px, const double* py,
+                              const double* pz, const double* radius, const uint8_t* active,
+                              const uint8_t* collidable, int32_t max_pairs, int32_t* pair_lo,
+                              int32_t* pair_hi, int32_t* n_pairs) {
+    if (!h || !n_pairs || !radius) return NB_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    int r;
+    if ((r = stage_bodies(h, n, px, py, pz, nullptr, radius, active))) return r;
+    *n_pairs = 0;
+    if (n == 0) return NB_OK;
+    if (collidable) {
+        if ((r = upload(h, h->s.collidable, collidable, (size_t)n))) return r;
+    } else {
+        NB_CUDA(h, cudaMemsetAsync(h->s.collidable, 1, (size_t)n, h->st));
+    }
+    // the broad phase reads masses only through the tree: give every body
+    // unit mass so no cell is skipped as empty
+    std::vector<double> ones((size_t)n, 1.0);
+    if ((r = upload(h, h->s.mass, ones.data(), sizeof(double) * (size_t)n))) return r;
+    Scal* sc = h->scal;
+    nb::CollideArgs c{};
+    c.n = n;
+    c.n_active = h->n_active;
+    c.s = h->s;
+    c.s_alt = h->s_alt;
+    c.keys0 = h->keys0; c.keys1 = h->keys1; c.vals0 = h->vals0; c.vals1 = h->vals1;
+    c.sort_ws = h->sort_ws;
+    c.tree = h->tree;
+    c.sbody = h->sbody;
+    c.srad = h->srad;
+    c.cube = sc->cube;
+    c.leaf_cap = h->leaf_cap;
+    c.n_pairs = &sc->n_pairs;
+    c.err = sc->err;
+    c.sms = h->sms;
+    c.bbox_ord = sc->bbox_ord;
+    c.n_active_dev = &sc->n_active;
+    int np = 0;
+    if ((r = nb::broad_phase(h->st, h->col, c, true, &np)))
+        return fail(h, r, "broad phase failed");
+    if ((r = check_device(h))) return r;
+    *n_pairs = np;
+    const int w = np < max_pairs ? np : max_pairs;
+    if (w > 0) {
+        std::vector<uint64_t> pk((size_t)w);
+        if ((r = download(h, pk.data(), h->col.pair_keys, sizeof(uint64_t) * (size_t)w))) return r;
+        if ((r = check_device(h))) return r;
+        for (int k = 0; k < w; k++) {
+            if (pair_lo) pair_lo[k] = (int32_t)(pk[k] >> 32);
+            if (pair_hi) pair_hi[k] = (int32_t)(pk[k] & 0xFFFFFFFFu);
+        }
+    }
+    h->has_state = false;
+    if (np > max_pairs) return fail(h, NB_ERR_CAPACITY, "%d pairs > max_pairs %d", np, max_pairs);
+    return NB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,226 @@
+// sort.cu - stable LSD radix sort of (uint64 key, uint32 value) pairs.
+//
+// Replaces the reference's launch_radix_sort (engine/src/cuda/morton_kernel.cu:
+// 87-230: 16 passes of 4 bits, a <<<1,16>>> serial prefix over all blocks and
+// an unstable shared-memory atomicAdd scatter) with a one-sweep design:
+//   * one histogram kernel computes the digit counts of all 8 passes at once
+//     (fused into the Morton kernel on the tree path);
+//   * each 8-bit pass is a single kernel: tiles of 4096 keys are ranked
+//     stably in shared memory with warp match/ballot, the per-digit tile
+//     offsets are chained across tiles by decoupled look-back, and keys are
+//     written out digit-run by digit-run from a shared-memory staging copy.
+// Every look-back spin is bounded (kSpinLimit); on expiry the kernel records
+// NB_ERR_TIMEOUT in the device error word and the result is discarded.
+#include "sort.cuh"
+
+namespace nb {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPre = 2u << 30;
+constexpr uint32_t kValMask = (1u << 30) - 1;
+
+constexpr int kSortDynSmem = kSortTile * 12;
+const void* k_sort_pass_ptr();
+
+void sort_init() {
+    cudaFuncSetAttribute(k_sort_pass_ptr(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kSortDynSmem);
+}
+
+size_t sort_workspace_bytes(int capacity) {
+    size_t tiles = (size_t)ceil_div(capacity > 0 ? capacity : 1, kSortTile);
+    return sizeof(uint32_t) * (8 * 256 + 8 + 8 * tiles * 256);
+}
+
+// Digit histograms of all 8 passes (used when the keys were not produced by a
+// kernel that already counted them).
+__global__ void k_sort_histogram(int n, const uint64_t* __restrict__ keys,
+                                 uint32_t* __restrict__ hist) {
+    __shared__ uint32_t sh[8][256];
+    for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) (&sh[0][0])[t] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint64_t k = keys[i];
+#pragma unroll
+        for (int p = 0; p < 8; p++) atomicAdd(&sh[p][(k >> (8 * p)) & 0xFF], 1u);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) {
+        uint32_t v = (&sh[0][0])[t];
+        if (v) atomicAdd(&hist[t], v);
+    }
+}
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
+    return *(const volatile uint32_t*)p;
+}
+
+// One stable 8-bit pass.  hist: the 256 global counts of this digit;
+// look: tiles x 256 look-back words (zeroed); tile_ctr: dynamic tile index.
+__global__ void __launch_bounds__(kSortThreads)
+k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+            uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+            const uint32_t* __restrict__ hist, uint32_t* look, uint32_t* tile_ctr, int* err) {
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    uint64_t* s_keys = (uint64_t*)s_dyn;                 // kSortTile keys
+    uint32_t* s_vals = (uint32_t*)(s_dyn + 8 * kSortTile);  // kSortTile values
+    __shared__ uint16_t s_wcnt[kSortWarps][256];  // per-warp digit counts, then offsets
+    __shared__ uint32_t s_tile_excl[256];          // exclusive scan of tile counts over digits
+    __shared__ uint32_t s_glob[256];               // global write base of each digit
+    __shared__ uint32_t s_scan[256];
+    __shared__ int s_tile;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = (int)atomicAdd(tile_ctr, 1u);
+    for (int t = tid; t < kSortWarps * 256; t += kSortThreads) (&s_wcnt[0][0])[t] = 0;
+    __syncthreads();
+    const int tile = s_tile;
+    const int base = tile * kSortTile;
+    const int valid = min(kSortTile, n - base);
+
+    // Load: warp w owns the contiguous segment [base + 512w, base + 512w + 512),
+    // item k of lane l is element 32k + l of it, so (warp, k, lane) order is
+    // index order and the ranking below is stable.
+    uint64_t key[kSortItems];
+    uint32_t val[kSortItems];
+    uint32_t rank[kSortItems];
+    const int seg = base + warp * (32 * kSortItems);
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        int i = seg + k * 32 + lane;
+        key[k] = (i < n) ? kin[i] : ~0ull;
+        val[k] = (i < n) ? vin[i] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        uint32_t d = (uint32_t)(key[k] >> shift) & 0xFF;
+        unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+        uint32_t before = s_wcnt[warp][d];
+        rank[k] = before + __popc(peers & lanemask_lt());
+        __syncwarp();
+        if ((peers & lanemask_lt()) == 0) s_wcnt[warp][d] = (uint16_t)(before + __popc(peers));
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Thread t owns digit t: warp prefix, tile count.
+    const int d = tid;
+    uint32_t tile_cnt = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) {
+        uint32_t c = s_wcnt[w][d];
+        s_wcnt[w][d] = (uint16_t)tile_cnt;
+        tile_cnt += c;
+    }
+    // Out-of-range sentinels were ranked last within digit 255 of the last
+    // tile; they are never written and never counted in the look-back.
+    uint32_t tail = (uint32_t)(kSortTile - valid);
+    uint32_t real_cnt = (d == 255) ? tile_cnt - tail : tile_cnt;
+
+    // Publish the aggregate, then look back for the exclusive prefix.
+    uint32_t* my = look + (size_t)tile * 256;
+    if (tile == 0) {
+        atomicExch(&my[d], kFlagPre | real_cnt);
+    } else {
+        atomicExch(&my[d], kFlagAgg | real_cnt);
+    }
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int j = tile - 1;
+        uint32_t spins = 0;
+        while (j >= 0) {
+            uint32_t v = ld_volatile(look + (size_t)j * 256 + d);
+            if ((v & ~kValMask) == 0) {
+                if (++spins > kSpinLimit) {
+                    dev_flag(err, kErrTimeout);
+                    break;
+                }
+                continue;
+            }
+            excl += v & kValMask;
+            if ((v & ~kValMask) == kFlagPre) break;
+            j--;
+        }
+        __threadfence();
+        atomicExch(&my[d], kFlagPre | (excl + real_cnt));
+    }
+
+    // Global digit bases: exclusive scan of the global histogram; tile digit
+    // starts: exclusive scan of this tile's counts.
+    uint32_t gh = hist[d];
+    s_scan[d] = gh;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+        uint32_t t = (d >= o) ? s_scan[d - o] : 0;
+        __syncthreads();
+        s_scan[d] += t;
+        __syncthreads();
+    }
+    s_glob[d] = s_scan[d] - gh + excl;
+    __syncthreads();
+    s_scan[d] = tile_cnt;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+        uint32_t t = (d >= o) ? s_scan[d - o] : 0;
+        __syncthreads();
+        s_scan[d] += t;
+        __syncthreads();
+    }
+    s_tile_excl[d] = s_scan[d] - tile_cnt;
+    __syncthreads();
+
+    // Stage in shared memory in tile-sorted order.
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        uint32_t dg = (uint32_t)(key[k] >> shift) & 0xFF;
+        uint32_t pos = s_tile_excl[dg] + s_wcnt[warp][dg] + rank[k];
+        s_keys[pos] = key[k];
+        s_vals[pos] = val[k];
+    }
+    __syncthreads();
+    // Write out: consecutive s with the same digit go to consecutive addresses.
+    for (int s = tid; s < valid; s += kSortThreads) {
+        uint64_t k = s_keys[s];
+        uint32_t dg = (uint32_t)(k >> shift) & 0xFF;
+        uint32_t g = s_glob[dg] + (uint32_t)s - s_tile_excl[dg];
+        kout[g] = k;
+        vout[g] = s_vals[s];
+    }
+}
+
+const void* k_sort_pass_ptr() { return (const void*)k_sort_pass; }
+
+// Sort n pairs.  Data starts in (k0, v0); the result ends in (k0, v0) (8
+// passes, even count).  ws: sort_workspace_bytes(capacity) bytes.  When
+// `hist_ready` the 8x256 histograms at the head of ws are already filled (by
+// the fused Morton kernel); otherwise they are computed here.
+void sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1,
+                void* ws, bool hist_ready, int* err, int sms) {
+    if (n <= 1) return;
+    uint32_t* hist = (uint32_t*)ws;
+    uint32_t* ctr = hist + 8 * 256;
+    uint32_t* look = ctr + 8;
+    const int tiles = ceil_div(n, kSortTile);
+    if (!hist_ready) {
+        cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, st);
+        int grid = min(ceil_div(n, 256 * 8), sms * 8);
+        k_sort_histogram<<<grid, 256, 0, st>>>(n, k0, hist);
+    }
+    cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * (8 + (size_t)8 * tiles * 256), st);
+    uint64_t* ks = k0;
+    uint32_t* vs = v0;
+    uint64_t* kd = k1;
+    uint32_t* vd = v1;
+    for (int p = 0; p < 8; p++) {
+        k_sort_pass<<<tiles, kSortThreads, kSortDynSmem, st>>>(n, 8 * p, ks, vs, kd, vd, hist + 256 * p,
+                                                   look + (size_t)p * tiles * 256, ctr + p, err);
+        uint64_t* tk = ks; ks = kd; kd = tk;
+        uint32_t* tv = vs; vs = vd; vd = tv;
+    }
+}
+
+}  // namespace nb

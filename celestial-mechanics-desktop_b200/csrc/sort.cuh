@@ -1,0 +1,12 @@
+// sort.cuh - stable one-sweep LSD radix sort of (uint64, uint32) pairs.
+#pragma once
+#include "common.cuh"
+
+namespace nb {
+
+void sort_init();
+size_t sort_workspace_bytes(int capacity);
+void sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1,
+                void* ws, bool hist_ready, int* err, int sms);
+
+}  // namespace nb

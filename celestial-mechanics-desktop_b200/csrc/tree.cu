@@ -1,0 +1,384 @@
+// tree.cu - parallel octree build from sorted Morton keys, and multipoles.
+//
+// Replaces tree_build_kernel<<<1,1>>> (engine/src/cuda/gpu_tree.cu:269-464,
+// one thread inserting every body) with a fully parallel construction:
+//   1. k_radix_tree: Karras' binary radix tree over the sorted 63-bit keys
+//      (Karras 2012, "Maximizing parallelism in the construction of BVHs,
+//      octrees and k-d trees"), one thread per internal node; equal keys are
+//      split by index so the tree is always binary.
+//   2. k_octree_mark: a binary node X is an octree node iff floor(d_X/3) >
+//      floor(d_parent/3) (d = common prefix length): its body range is then
+//      exactly an octree cell, the deepest one being level floor(d_X/3).
+//      Single-child chains of the point-region octree collapse into it.  A
+//      node is emitted when its octree parent holds more than leaf_cap
+//      bodies; it is walk-internal when it also holds more than leaf_cap
+//      bodies and is above level 21.  Its walk children are the exits of
+//      its <= 3-deep binary subtree inside the same cell, in key order.
+//   3. block scan of the child counts gives every walk-internal node a
+//      contiguous child slot range; k_octree_emit writes the nodes.
+//   4. k_multipole: bottom-up, the last child to arrive at a parent computes
+//      the parent (arrival counters), so each node is reduced exactly once
+//      from its children in child order: deterministic.
+// With leaf_cap = 1 the walk tree is the reference's point-region octree
+// (OctreeBuilder::insert_body, engine/src/physics/octree_builder.cpp:50-105)
+// down to level 21, with chains collapsed.
+#include "tree.cuh"
+
+namespace nb {
+
+constexpr int kMarkThreads = 256;
+constexpr int kMarkItems = 4;
+constexpr int kMarkTile = kMarkThreads * kMarkItems;  // internal nodes per block
+
+size_t tree_bytes(int cap) {
+    size_t c = (size_t)(cap > 1 ? cap : 2);
+    size_t b = 0;
+    b += 2 * c * 4 + c * 4 + c * 4 + c + c * 4 + c + c * 4 + c * 4;  // binary tree
+    b += (c / kMarkTile + 2) * 4;                                      // block sums
+    b += 256;                                                          // align slack
+    size_t w = 2 * c;
+    b += w * 16 + w * 4 + w * 4 + w * 32 + w * 16 + w * 16 + w * 4 + 16;
+    return b + 16 * 64;
+}
+
+template <typename T>
+static T* carve(char*& p, size_t count, size_t align = 16) {
+    uintptr_t a = ((uintptr_t)p + align - 1) & ~(uintptr_t)(align - 1);
+    p = (char*)(a + count * sizeof(T));
+    return (T*)a;
+}
+
+void tree_carve(TreeBufs& t, void* base, int cap) {
+    size_t c = (size_t)(cap > 1 ? cap : 2);
+    size_t w = 2 * c;
+    char* p = (char*)base;
+    t.com = carve<double4>(p, w, 32);
+    t.link = carve<int4>(p, w);
+    t.q0 = carve<float4>(p, w);
+    t.q1 = carve<float4>(p, w);
+    t.level = carve<int>(p, w);
+    t.parent_bin = carve<int>(p, w);
+    t.counter = carve<int>(p, w);
+    t.n_nodes = carve<int>(p, 4);
+    t.bchild = carve<int>(p, 2 * c);
+    t.bfirst = carve<int>(p, c);
+    t.blast = carve<int>(p, c);
+    t.bparent = carve<int>(p, c);
+    t.child_base = carve<int>(p, c);
+    t.walk_index = carve<int>(p, c);
+    t.block_sums = carve<int>(p, c / kMarkTile + 2);
+    t.bdelta = carve<uint8_t>(p, c);
+    t.bnchild = carve<uint8_t>(p, c);
+    t.capacity = cap;
+}
+
+// Common prefix length of sorted keys i and j in the 63-bit key space;
+// equal keys continue with the index bits (>= 63); -1 out of range.
+__device__ __forceinline__ int prefix_len(const uint64_t* __restrict__ k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint64_t a = k[i], b = k[j];
+    if (a != b) return __clzll((long long)(a ^ b)) - 1;
+    return 63 + __clz(i ^ j);
+}
+
+__global__ void k_radix_tree(int n, const uint64_t* __restrict__ keys, TreeBufs t) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int dl = prefix_len(keys, n, i, i - 1);
+    int dr = prefix_len(keys, n, i, i + 1);
+    int d = (dr > dl) ? 1 : -1;
+    int dmin = min(dl, dr);
+    int lmax = 2;
+    while (prefix_len(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int s = lmax >> 1; s >= 1; s >>= 1)
+        if (prefix_len(keys, n, i, i + (l + s) * d) > dmin) l += s;
+    int j = i + l * d;
+    int dnode = prefix_len(keys, n, i, j);
+    int s = 0, step = l;
+    do {
+        step = (step + 1) >> 1;
+        if (prefix_len(keys, n, i, i + (s + step) * d) > dnode) s += step;
+    } while (step > 1);
+    int gamma = i + s * d + min(d, 0);
+    int first = min(i, j), last = max(i, j);
+    int left = (first == gamma) ? ~gamma : gamma;
+    int right = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    t.bchild[2 * i] = left;
+    t.bchild[2 * i + 1] = right;
+    t.bfirst[i] = first;
+    t.blast[i] = last;
+    t.bdelta[i] = (uint8_t)min(dnode, 63);
+    if (left >= 0) t.bparent[left] = i;
+    if (right >= 0) t.bparent[right] = i;
+    if (i == 0) t.bparent[0] = -1;
+}
+
+__device__ __forceinline__ int lvl(const TreeBufs& t, int x) { return t.bdelta[x] / 3; }
+
+// Walk-tree children (exits of the binary subtree inside node i's cell),
+// visited in key order; calls f(child_code) for each.
+template <typename F>
+__device__ __forceinline__ void for_each_exit(const TreeBufs& t, int i, F f) {
+    const int li = lvl(t, i);
+    int stack[8];  // the subtree is at most 3 binary levels deep: <= 5 entries
+    int sp = 0;
+    stack[sp++] = t.bchild[2 * i + 1];
+    stack[sp++] = t.bchild[2 * i];
+    while (sp > 0) {
+        int c = stack[--sp];
+        if (c < 0 || lvl(t, c) > li) {
+            f(c);
+        } else {  // same cell: expand, right pushed first so left comes out first
+            stack[sp++] = t.bchild[2 * c + 1];
+            stack[sp++] = t.bchild[2 * c];
+        }
+    }
+}
+
+// Counting pass; the visiting order does not matter here.
+__device__ int count_exits(const TreeBufs& t, int i) {
+    int c = 0;
+    for_each_exit(t, i, [&](int) { c++; });
+    return c;
+}
+
+__device__ __forceinline__ bool walk_internal(const TreeBufs& t, int x, int leaf_cap) {
+    return (t.blast[x] - t.bfirst[x] + 1) > leaf_cap && lvl(t, x) < 21;
+}
+
+__global__ void __launch_bounds__(kMarkThreads)
+k_octree_mark(int n, TreeBufs t, int leaf_cap) {
+    __shared__ int s_red[kMarkThreads / 32];
+    const int m = n - 1;  // internal nodes
+    int local = 0;
+    for (int k = 0; k < kMarkItems; k++) {
+        int i = blockIdx.x * kMarkTile + k * kMarkThreads + threadIdx.x;
+        if (i >= m) break;
+        int P = t.bparent[i];
+        int li = lvl(t, i);
+        bool exists;
+        if (P < 0) {
+            exists = true;
+        } else if (li <= lvl(t, P)) {
+            exists = false;  // inside its parent's cell
+        } else {
+            int Y = P;  // climb to the octree node holding P
+            while (t.bparent[Y] >= 0 && lvl(t, t.bparent[Y]) == lvl(t, Y)) Y = t.bparent[Y];
+            exists = walk_internal(t, Y, leaf_cap);
+        }
+        int nc = (exists && walk_internal(t, i, leaf_cap)) ? count_exits(t, i) : 0;
+        t.bnchild[i] = (uint8_t)nc;
+        t.walk_index[i] = -1;
+        local += nc;
+    }
+    local = warp_sum(local);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int w = 0; w < kMarkThreads / 32; w++) s += s_red[w];
+        t.block_sums[blockIdx.x] = s;
+    }
+}
+
+// Exclusive scan of the block sums in one block; writes the node count.
+__global__ void k_scan_block_sums(int nblocks, TreeBufs t, int n) {
+    __shared__ int s[1024];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nblocks; base += 1024) {
+        int i = base + threadIdx.x;
+        int v = (i < nblocks) ? t.block_sums[i] : 0;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            int x = (threadIdx.x >= (unsigned)o) ? s[threadIdx.x - o] : 0;
+            __syncthreads();
+            s[threadIdx.x] += x;
+            __syncthreads();
+        }
+        if (i < nblocks) t.block_sums[i] = carry + s[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += s[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *t.n_nodes = (n >= 2) ? 1 + carry : (n == 1 ? 1 : 0);
+}
+
+// Child slot of every walk-internal node: 1 + exclusive scan of bnchild.
+__global__ void __launch_bounds__(kMarkThreads) k_octree_base(int n, TreeBufs t) {
+    __shared__ int s_w[kMarkThreads / 32];
+    const int m = n - 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int off = 1 + t.block_sums[blockIdx.x];
+    for (int k = 0; k < kMarkItems; k++) {
+        int i = blockIdx.x * kMarkTile + k * kMarkThreads + threadIdx.x;
+        int v = (i < m) ? t.bnchild[i] : 0;
+        int inc = warp_incl_scan(v);
+        if (lane == 31) s_w[warp] = inc;
+        __syncthreads();
+        int wpre = 0, tot = 0;
+        for (int w = 0; w < kMarkThreads / 32; w++) {
+            int x = s_w[w];
+            if (w < warp) wpre += x;
+            tot += x;
+        }
+        if (i < m) t.child_base[i] = off + wpre + inc - v;
+        off += tot;
+        __syncthreads();
+    }
+}
+
+__global__ void k_octree_emit(int n, TreeBufs t, int leaf_cap) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n == 1) {
+        if (i == 0) {
+            t.link[0] = make_int4(-1, 0, 0, 1);
+            t.level[0] = 0;
+            t.parent_bin[0] = -1;
+        }
+        return;
+    }
+    if (i >= n - 1) return;
+    if (i == 0) {
+        bool wi = walk_internal(t, 0, leaf_cap);
+        t.link[0] = make_int4(wi ? t.child_base[0] : -1, t.bnchild[0], 0, n);
+        t.level[0] = lvl(t, 0);
+        t.parent_bin[0] = -1;
+        t.walk_index[0] = 0;
+    }
+    int nc = t.bnchild[i];
+    if (nc == 0) return;
+    const int li = lvl(t, i);
+    int w = t.child_base[i];
+    for_each_exit(t, i, [&](int c) {
+        if (c < 0) {
+            t.link[w] = make_int4(-1, 0, ~c, 1);
+            t.level[w] = li + 1;
+        } else {
+            bool wi = walk_internal(t, c, leaf_cap);
+            int cnt = t.blast[c] - t.bfirst[c] + 1;
+            t.link[w] = make_int4(wi ? t.child_base[c] : -1, wi ? (int)t.bnchild[c] : 0,
+                                  t.bfirst[c], cnt);
+            t.level[w] = lvl(t, c);
+            t.walk_index[c] = w;
+        }
+        t.parent_bin[w] = i;
+        w++;
+    });
+}
+
+__device__ __forceinline__ void quad_add(double q[6], double m, double dx, double dy, double dz) {
+    double r2 = dx * dx + dy * dy + dz * dz;
+    q[0] += m * (3.0 * dx * dx - r2);
+    q[1] += m * (3.0 * dy * dy - r2);
+    q[2] += m * (3.0 * dx * dy);
+    q[3] += m * (3.0 * dx * dz);
+    q[4] += m * (3.0 * dy * dz);
+}
+
+__global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody,
+                           const float* __restrict__ srad, const double* __restrict__ cube) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    int nn = *t.n_nodes;
+    if (w >= nn) return;
+    int4 lk = t.link[w];
+    if (lk.y != 0) return;  // internal nodes are reduced by their last child
+    const double root_half = cube[3];
+    {
+        // leaf: moments straight from its bodies
+        double M = 0, sx = 0, sy = 0, sz = 0;
+        float rmax = 0.f;
+        for (int b = lk.z; b < lk.z + lk.w; b++) {
+            double4 p = sbody[b];
+            M += p.w;
+            sx += p.w * p.x;
+            sy += p.w * p.y;
+            sz += p.w * p.z;
+            if (srad) rmax = fmaxf(rmax, srad[b]);
+        }
+        double cx, cy, cz;
+        if (M > 0) {
+            cx = sx / M; cy = sy / M; cz = sz / M;
+        } else {
+            double4 p = sbody[lk.z];
+            cx = p.x; cy = p.y; cz = p.z;
+        }
+        double q[6] = {0, 0, 0, 0, 0, 0};
+        if (lk.w > 1)
+            for (int b = lk.z; b < lk.z + lk.w; b++) {
+                double4 p = sbody[b];
+                quad_add(q, p.w, p.x - cx, p.y - cy, p.z - cz);
+            }
+        t.com[w] = make_double4(cx, cy, cz, M);
+        t.q0[w] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+        t.q1[w] = make_float4((float)q[4], (float)ldexp(root_half, -t.level[w]), rmax, 0.f);
+    }
+    // climb: the last child to arrive reduces the parent
+    int pb = t.parent_bin[w];
+    while (pb >= 0) {
+        int p = __ldcg(&t.walk_index[pb]);
+        __threadfence();
+        int4 pl = __ldcg(&t.link[p]);
+        if (atomicAdd(&t.counter[p], 1) != pl.y - 1) return;
+        __threadfence();
+        double M = 0, sx = 0, sy = 0, sz = 0;
+        float rmax = 0.f;
+        for (int c = pl.x; c < pl.x + pl.y; c++) {
+            double2 a = __ldcg((const double2*)&t.com[c]);
+            double2 b = __ldcg((const double2*)&t.com[c] + 1);
+            M += b.y;
+            sx += b.y * a.x;
+            sy += b.y * a.y;
+            sz += b.y * b.x;
+            rmax = fmaxf(rmax, __ldcg(&t.q1[c]).z);
+        }
+        double cx, cy, cz;
+        if (M > 0) {
+            cx = sx / M; cy = sy / M; cz = sz / M;
+        } else {
+            double2 a = __ldcg((const double2*)&t.com[pl.x]);
+            double2 b = __ldcg((const double2*)&t.com[pl.x] + 1);
+            cx = a.x; cy = a.y; cz = b.x;
+        }
+        double q[6] = {0, 0, 0, 0, 0, 0};
+        for (int c = pl.x; c < pl.x + pl.y; c++) {
+            double2 a = __ldcg((const double2*)&t.com[c]);
+            double2 b = __ldcg((const double2*)&t.com[c] + 1);
+            float4 c0 = __ldcg(&t.q0[c]);
+            float4 c1 = __ldcg(&t.q1[c]);
+            q[0] += c0.x; q[1] += c0.y; q[2] += c0.z; q[3] += c0.w; q[4] += c1.x;
+            quad_add(q, b.y, a.x - cx, a.y - cy, b.x - cz);
+        }
+        t.com[p] = make_double4(cx, cy, cz, M);
+        t.q0[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+        t.q1[p] = make_float4((float)q[4], (float)ldexp(root_half, -__ldcg(&t.level[p])), rmax,
+                              0.f);
+        pb = __ldcg(&t.parent_bin[p]);
+    }
+}
+
+void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys,
+                const double4* sbody, const float* srad, const double* cube, int leaf_cap,
+                int* err) {
+    (void)err;
+    if (n <= 0) {
+        cudaMemsetAsync(t.n_nodes, 0, sizeof(int), st);
+        return;
+    }
+    const int m = n - 1;
+    const int nblk = ceil_div(m > 0 ? m : 1, kMarkTile);
+    if (m > 0) {
+        k_radix_tree<<<ceil_div(m, 256), 256, 0, st>>>(n, skeys, t);
+        k_octree_mark<<<nblk, kMarkThreads, 0, st>>>(n, t, leaf_cap);
+    }
+    k_scan_block_sums<<<1, 1024, 0, st>>>(m > 0 ? nblk : 0, t, n);
+    if (m > 0) k_octree_base<<<nblk, kMarkThreads, 0, st>>>(n, t);
+    k_octree_emit<<<ceil_div(m > 0 ? m : 1, 256), 256, 0, st>>>(n, t, leaf_cap);
+    cudaMemsetAsync(t.counter, 0, sizeof(int) * 2 * (size_t)n, st);
+    k_multipole<<<ceil_div(2 * n, 256), 256, 0, st>>>(n, t, sbody, srad, cube);
+}
+
+}  // namespace nb

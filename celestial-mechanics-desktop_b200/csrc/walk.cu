@@ -1,0 +1,410 @@
+// walk.cu - Barnes-Hut force walks over the walk tree.
+//
+// k_walk_group replaces tree_traverse_kernel (engine/src/cuda/gpu_tree.cu:
+// 508-597: one thread per body, FP64, a 128-entry local stack that silently
+// drops children on overflow) with a warp-cooperative walk in the style of
+// Bedorf, Gaburov & Portegies Zwart 2012 (Bonsai):
+//   * a warp owns a group of 32 consecutive Morton-sorted bodies and walks
+//     the tree once for all of them, breadth first, 32 candidate nodes per
+//     step (one per lane);
+//   * the opening test is the reference's geometric MAC, 4h^2 < theta^2 d^2
+//     (gpu_tree.cu:567-569), with d the distance from the cell's centre of
+//     mass to the group's bounding box, so it is at least as strict as the
+//     per-body test for every body of the group;
+//   * accepted cells and the bodies of opened leaves are appended (ballot /
+//     warp scan) to shared-memory interaction lists that the 32 lanes then
+//     evaluate against their own body: broadcast reads, FP32 FMA chains;
+//   * coordinates are differenced in FP64 against the group centre once per
+//     list entry and per body, then the pair math is FP32 with monopole +
+//     traceless quadrupole; every list flush is summed in FP32 and folded
+//     into a compensated (Kahan) accumulator;
+//   * frontier overflow is reported (NB_ERR_STACK_OVERFLOW), never dropped
+//     silently.
+#include "walk.cuh"
+
+namespace nb {
+
+constexpr int kWalkWarps = 8;
+constexpr int kWalkThreads = kWalkWarps * 32;
+constexpr int kCellCap = 128;
+constexpr int kPartCap = 128;
+// per-warp shared memory, in floats
+constexpr int kWarpFloats = kCellCap * 9 + kPartCap * 4 + kPartCap * 2 + kPartCap;
+constexpr int kWalkSmem = kWalkWarps * kWarpFloats * 4;
+
+__device__ __forceinline__ void kahan(float& s, float& c, float x) {
+    float y = x - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+template <bool QUAD, bool SHELL, bool POT>
+__global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
+    extern __shared__ __align__(16) float s_walk[];
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* base = s_walk + warp * kWarpFloats;
+    float4* c0 = (float4*)base;                      // rel com xyz, mass
+    float4* c1 = c0 + kCellCap;                      // Qxx, Qyy, Qxy, Qxz
+    float* c2 = (float*)(c1 + kCellCap);             // Qyz
+    float4* p0 = (float4*)(c2 + kCellCap);           // rel xyz, mass
+    float2* p1 = (float2*)(p0 + kPartCap);           // R^2, m / (R^2 + eps^2)^1.5
+    int* p2 = (int*)(p1 + kPartCap);                 // sorted index
+    int* fa = a.front + (size_t)(blockIdx.x * kWalkWarps + warp) * 2 * a.front_cap;
+    int* fb = fa + a.front_cap;
+    const float eps2 = (float)a.eps2;
+    const float theta2 = (float)a.theta2;
+    const int ngroups = (a.n + 31) >> 5;
+    unsigned long long cnt_cell = 0, cnt_body = 0;
+
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = (int)atomicAdd(a.group_ctr, 1u);
+        g = __shfl_sync(FULL, g, 0);
+        if (g >= ngroups) break;
+        const int s = g * 32 + lane;
+        const bool valid = s < a.n;
+        const double4 b = a.sbody[valid ? s : a.n - 1];
+        const int nvalid = min(32, a.n - g * 32);
+        const double mnx = warp_min(b.x), mny = warp_min(b.y), mnz = warp_min(b.z);
+        const double mxx = warp_max(b.x), mxy = warp_max(b.y), mxz = warp_max(b.z);
+        const double gcx = 0.5 * (mnx + mxx), gcy = 0.5 * (mny + mxy), gcz = 0.5 * (mnz + mxz);
+        // half extents, rounded outwards so the FP32 box contains every body
+        const float ghx = (float)(0.5 * (mxx - mnx)) * 1.000001f + 1e-30f;
+        const float ghy = (float)(0.5 * (mxy - mny)) * 1.000001f + 1e-30f;
+        const float ghz = (float)(0.5 * (mxz - mnz)) * 1.000001f + 1e-30f;
+        const float bx = (float)(b.x - gcx), by = (float)(b.y - gcy), bz = (float)(b.z - gcz);
+
+        float sax = 0.f, say = 0.f, saz = 0.f, cax = 0.f, cay = 0.f, caz = 0.f;
+        float spot = 0.f, cpot = 0.f;
+        int nc = 0, np = 0;
+
+        auto flush_cells = [&]() {
+            float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
+#pragma unroll 4
+            for (int j = 0; j < nc; j++) {
+                const float4 A = c0[j];
+                const float dx = bx - A.x, dy = by - A.y, dz = bz - A.z;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+                const float inv = rsqrtf(r2);
+                const float inv2 = inv * inv;
+                const float inv3 = inv * inv2;
+                if (QUAD) {
+                    const float4 B = c1[j];
+                    const float C = c2[j];
+                    const float qzz = -(B.x + B.y);
+                    const float qx = fmaf(B.x, dx, fmaf(B.z, dy, B.w * dz));
+                    const float qy = fmaf(B.z, dx, fmaf(B.y, dy, C * dz));
+                    const float qz = fmaf(B.w, dx, fmaf(C, dy, qzz * dz));
+                    const float rqr = fmaf(dx, qx, fmaf(dy, qy, dz * qz));
+                    const float inv5 = inv3 * inv2;
+                    // a = -M r / r^3 + Q r / r^5 - (5/2) (r.Q.r) r / r^7
+                    const float f = fmaf(-2.5f * rqr, inv5 * inv2, -A.w * inv3);
+                    tx = fmaf(f, dx, fmaf(qx, inv5, tx));
+                    ty = fmaf(f, dy, fmaf(qy, inv5, ty));
+                    tz = fmaf(f, dz, fmaf(qz, inv5, tz));
+                    if (POT) tp = fmaf(-0.5f * rqr, inv5, fmaf(-A.w, inv, tp));
+                } else {
+                    const float f = -A.w * inv3;
+                    tx = fmaf(f, dx, tx);
+                    ty = fmaf(f, dy, ty);
+                    tz = fmaf(f, dz, tz);
+                    if (POT) tp = fmaf(-A.w, inv, tp);
+                }
+            }
+            kahan(sax, cax, tx);
+            kahan(say, cay, ty);
+            kahan(saz, caz, tz);
+            if (POT) kahan(spot, cpot, tp);
+            cnt_cell += (unsigned long long)nc * nvalid;
+            nc = 0;
+            __syncwarp();
+        };
+        auto flush_parts = [&]() {
+            float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
+#pragma unroll 4
+            for (int j = 0; j < np; j++) {
+                const float4 P = p0[j];
+                const float dx = bx - P.x, dy = by - P.y, dz = bz - P.z;
+                const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const float r2 = raw + eps2;
+                const float inv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+                float f = P.w * (inv * inv * inv);
+                if (SHELL) {
+                    const float2 S = p1[j];
+                    if (raw < S.x) f = S.y;
+                }
+                tx = fmaf(-f, dx, tx);
+                ty = fmaf(-f, dy, ty);
+                tz = fmaf(-f, dz, tz);
+                if (POT) {
+                    if (p2[j] != s) tp = fmaf(-P.w, inv, tp);
+                }
+            }
+            kahan(sax, cax, tx);
+            kahan(say, cay, ty);
+            kahan(saz, caz, tz);
+            if (POT) kahan(spot, cpot, tp);
+            cnt_body += (unsigned long long)np * nvalid;
+            np = 0;
+            __syncwarp();
+        };
+
+        int* cur = fa;
+        int* nxt = fb;
+        int ncur = 1;
+        if (lane == 0) cur[0] = 0;
+        __syncwarp();
+        while (ncur > 0) {
+            int nnext = 0;
+            for (int off = 0; off < ncur; off += 32) {
+                const int node = (off + lane < ncur) ? cur[off + lane] : -1;
+                bool take_cell = false, is_leaf = false, open = false;
+                int4 lk = make_int4(0, 0, 0, 0);
+                float rx = 0.f, ry = 0.f, rz = 0.f, mass = 0.f;
+                if (node >= 0) {
+                    lk = a.t.link[node];
+                    const double4 cm = a.t.com[node];
+                    if (cm.w > 0.0) {
+                        const float half = a.t.q1[node].y;
+                        rx = (float)(cm.x - gcx);
+                        ry = (float)(cm.y - gcy);
+                        rz = (float)(cm.z - gcz);
+                        mass = (float)cm.w;
+                        const float dx = fmaxf(fabsf(rx) - ghx, 0.f);
+                        const float dy = fmaxf(fabsf(ry) - ghy, 0.f);
+                        const float dz = fmaxf(fabsf(rz) - ghz, 0.f);
+                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        take_cell = d2 > 0.f && 4.f * half * half < theta2 * d2;
+                        if (!take_cell) {
+                            if (lk.y == 0) is_leaf = true;
+                            else open = true;
+                        }
+                    }
+                }
+                // 1. accepted cells -> cell list
+                const unsigned mcell = __ballot_sync(FULL, take_cell);
+                if (mcell) {
+                    const int k = __popc(mcell);
+                    if (nc + k > kCellCap) flush_cells();
+                    if (take_cell) {
+                        const int slot = nc + __popc(mcell & lanemask_lt());
+                        c0[slot] = make_float4(rx, ry, rz, mass);
+                        if (QUAD) {
+                            c1[slot] = a.t.q0[node];
+                            c2[slot] = a.t.q1[node].x;
+                        }
+                    }
+                    nc += k;
+                    __syncwarp();
+                }
+                // 2. children of opened nodes -> next frontier
+                const int nch = open ? lk.y : 0;
+                const int inc = warp_incl_scan(nch);
+                const int tot = __shfl_sync(FULL, inc, 31);
+                if (tot > 0) {
+                    if (nnext + tot > a.front_cap) {
+                        if (lane == 0) dev_flag(a.err, kErrOverflow);
+                    } else {
+                        for (int k = 0; k < nch; k++) nxt[nnext + inc - nch + k] = lk.x + k;
+                        nnext += tot;
+                    }
+                }
+                // 3. bodies of leaves that were not accepted -> particle list
+                const int cb = is_leaf ? lk.w : 0;
+                const int incl = warp_incl_scan(cb);
+                const int T = __shfl_sync(FULL, incl, 31);
+                for (int t0 = 0; t0 < T; t0 += 32) {
+                    if (np + 32 > kPartCap) flush_parts();
+                    const int t = t0 + lane;
+                    int pos = 0;  // first lane whose inclusive count exceeds t
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const int v = __shfl_sync(FULL, incl, pos + step - 1);
+                        if (v <= t) pos += step;
+                    }
+                    const int ofirst = __shfl_sync(FULL, lk.z, pos);
+                    const int oexcl = __shfl_sync(FULL, incl - cb, pos);
+                    const int take = min(32, T - t0);
+                    if (lane < take) {
+                        const int bi = ofirst + (t - oexcl);
+                        const double4 q = a.sbody[bi];
+                        p0[np + lane] = make_float4((float)(q.x - gcx), (float)(q.y - gcy),
+                                                    (float)(q.z - gcz), (float)q.w);
+                        if (SHELL) {
+                            const float R = a.srad[bi];
+                            const float R2 = R * R;
+                            const float id = rsqrtf(R2 + eps2);
+                            p1[np + lane] = make_float2(R > 0.f ? R2 : 0.f, (float)q.w * id * id * id);
+                        }
+                        if (POT) p2[np + lane] = bi;
+                    }
+                    np += take;
+                    __syncwarp();
+                }
+            }
+            int* tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+            ncur = nnext;
+            __syncwarp();
+        }
+        if (nc) flush_cells();
+        if (np) flush_parts();
+        if (valid) {
+            const uint32_t row = a.sidx[s];
+            a.ax[row] = (double)sax - (double)cax;
+            a.ay[row] = (double)say - (double)cay;
+            a.az[row] = (double)saz - (double)caz;
+            if (POT) a.pot[row] = (double)spot - (double)cpot;
+        }
+    }
+    if (lane == 0 && a.counters) {
+        atomicAdd(&a.counters[0], cnt_cell);
+        atomicAdd(&a.counters[1], cnt_body);
+    }
+}
+
+// Per-body FP64 walk with the reference's semantics: MAC 4h^2 < theta^2 d^2
+// with d to the cell's centre of mass (barnes_hut_solver.cpp:269-283),
+// monopole only, leaves direct, self skipped, mass-0 nodes skipped, children
+// visited in the reference's octant order x + 2y + 4z (octree_node.hpp:53-59).
+// Arithmetic order follows compute_force_on_body (barnes_hut_solver.cpp:
+// 230-286) without FMA contraction; leaves use GravityKernel's shell theorem
+// when `shell` (BarnesHutBackend.cs:410-424).
+__device__ __forceinline__ double mono_factor(double m, double d2, double eps2) {
+    double inv = 1.0 / sqrt(__dadd_rn(d2, eps2));
+    double inv3 = __dmul_rn(__dmul_rn(inv, inv), inv);
+    return __dmul_rn(m, inv3);
+}
+
+template <bool SHELL>
+__global__ void k_walk_reference(WalkArgs a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.n) return;
+    const double4 b = a.sbody[s];
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    int stack[176];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int k = stack[--sp];
+        const double4 cm = a.t.com[k];
+        if (cm.w == 0.0) continue;
+        const int4 lk = a.t.link[k];
+        const double dx = __dsub_rn(b.x, cm.x), dy = __dsub_rn(b.y, cm.y), dz = __dsub_rn(b.z, cm.z);
+        const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        if (lk.y == 0) {
+            for (int j = lk.z; j < lk.z + lk.w; j++) {
+                if (j == s) continue;
+                double ex = dx, ey = dy, ez = dz, e2 = d2, m = cm.w;
+                if (lk.w > 1) {  // a level-21 bucket of coincident keys: body by body
+                    const double4 q = a.sbody[j];
+                    ex = __dsub_rn(b.x, q.x); ey = __dsub_rn(b.y, q.y); ez = __dsub_rn(b.z, q.z);
+                    e2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+                    m = q.w;
+                }
+                double f;
+                if (SHELL) {
+                    const double R = (double)a.srad[j];
+                    if (R > 0.0 && sqrt(e2) < R) {
+                        const double den = __dadd_rn(__dmul_rn(R, R), a.eps2);
+                        const double ids = 1.0 / sqrt(den);
+                        f = __dmul_rn(m, ids) / den;
+                    } else {
+                        const double inv = 1.0 / sqrt(__dadd_rn(e2, a.eps2));
+                        f = __dmul_rn(__dmul_rn(__dmul_rn(m, inv), inv), inv);
+                    }
+                } else {
+                    f = mono_factor(m, e2, a.eps2);
+                }
+                ax = __dsub_rn(ax, __dmul_rn(f, ex));
+                ay = __dsub_rn(ay, __dmul_rn(f, ey));
+                az = __dsub_rn(az, __dmul_rn(f, ez));
+            }
+            continue;
+        }
+        const double h = (double)a.t.q1[k].y;
+        const double s2 = __dmul_rn(__dmul_rn(4.0, h), h);
+        if (d2 > 0.0 && s2 < __dmul_rn(a.theta2, d2)) {
+            const double f = mono_factor(cm.w, d2, a.eps2);
+            ax = __dsub_rn(ax, __dmul_rn(f, dx));
+            ay = __dsub_rn(ay, __dmul_rn(f, dy));
+            az = __dsub_rn(az, __dmul_rn(f, dz));
+            continue;
+        }
+        // children: push in decreasing reference octant so octant 0 pops first
+        const int lev = a.t.level[k] + 1;  // subdivision level of this cell
+        const int shift = 63 - 3 * lev;
+        int oct_child[8];
+#pragma unroll
+        for (int o = 0; o < 8; o++) oct_child[o] = -1;
+        for (int c = lk.x; c < lk.x + lk.y; c++) {
+            const uint64_t key = a.skeys[a.t.link[c].z];
+            const int dg = (int)((key >> shift) & 7);  // Morton digit x<<2 | y<<1 | z
+            const int oct = ((dg >> 2) & 1) | (dg & 2) | ((dg & 1) << 2);
+            oct_child[oct] = c;
+        }
+        for (int o = 7; o >= 0; o--) {
+            if (oct_child[o] < 0) continue;
+            if (sp < 176) stack[sp++] = oct_child[o];
+            else dev_flag(a.err, kErrOverflow);
+        }
+    }
+    const uint32_t row = a.sidx[s];
+    a.ax[row] = ax;
+    a.ay[row] = ay;
+    a.az[row] = az;
+}
+
+void walk_init(int sms, WalkConfig& cfg) {
+    cudaFuncSetAttribute((const void*)k_walk_group<true, false, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    cudaFuncSetAttribute((const void*)k_walk_group<false, false, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    cudaFuncSetAttribute((const void*)k_walk_group<true, true, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    cudaFuncSetAttribute((const void*)k_walk_group<false, true, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    cudaFuncSetAttribute((const void*)k_walk_group<true, false, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    cudaFuncSetAttribute((const void*)k_walk_group<false, false, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_group<true, false, false>,
+                                                  kWalkThreads, kWalkSmem);
+    if (per_sm < 1) per_sm = 1;
+    cfg.blocks = sms * per_sm;
+    cfg.front_cap = 4096;
+}
+
+size_t walk_front_bytes(const WalkConfig& cfg) {
+    return (size_t)cfg.blocks * kWalkWarps * 2 * cfg.front_cap * sizeof(int);
+}
+
+void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,
+                bool pot) {
+    if (a.n <= 0) return;
+    a.front_cap = cfg.front_cap;
+    cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
+    const dim3 g(cfg.blocks), b(kWalkThreads);
+    if (pot) {
+        if (quad) k_walk_group<true, false, true><<<g, b, kWalkSmem, st>>>(a);
+        else k_walk_group<false, false, true><<<g, b, kWalkSmem, st>>>(a);
+    } else if (shell) {
+        if (quad) k_walk_group<true, true, false><<<g, b, kWalkSmem, st>>>(a);
+        else k_walk_group<false, true, false><<<g, b, kWalkSmem, st>>>(a);
+    } else {
+        if (quad) k_walk_group<true, false, false><<<g, b, kWalkSmem, st>>>(a);
+        else k_walk_group<false, false, false><<<g, b, kWalkSmem, st>>>(a);
+    }
+}
+
+void walk_reference(cudaStream_t st, WalkArgs a, bool shell) {
+    if (a.n <= 0) return;
+    if (shell) k_walk_reference<true><<<ceil_div(a.n, 128), 128, 0, st>>>(a);
+    else k_walk_reference<false><<<ceil_div(a.n, 128), 128, 0, st>>>(a);
+}
+
+}  // namespace nb

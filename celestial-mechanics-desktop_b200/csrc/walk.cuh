@@ -1,0 +1,40 @@
+// walk.cuh - Barnes-Hut tree walks.
+#pragma once
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace nb {
+
+struct WalkArgs {
+    int n;                      // active bodies, sorted positions [0, n)
+    const double4* sbody;       // sorted x, y, z, m
+    const float* srad;          // sorted radius (shell theorem), may be null
+    const uint64_t* skeys;      // sorted keys (reference-order walk)
+    const uint32_t* sidx;       // sorted position -> body row
+    TreeBufs t;
+    double theta2, eps2;
+    double* ax;                 // outputs by body row
+    double* ay;
+    double* az;
+    double* pot;                // potential by body row (may be null)
+    int* front;                 // per-warp frontier buffers, 2 x front_cap ints
+    int front_cap;
+    unsigned* group_ctr;        // dynamic group counter (zeroed)
+    unsigned long long* counters;  // [0] body-cell, [1] body-body interactions
+    int* err;
+};
+
+struct WalkConfig {
+    int blocks;        // persistent grid size
+    int front_cap;
+};
+
+void walk_init(int sms, WalkConfig& cfg);
+size_t walk_front_bytes(const WalkConfig& cfg);
+// Group walk, FP32 monopole(+quadrupole) on FP64-differenced coordinates.
+void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,
+                bool pot);
+// Per-body FP64 walk with the reference's MAC, monopole, child order.
+void walk_reference(cudaStream_t st, WalkArgs a, bool shell);
+
+}  // namespace nb

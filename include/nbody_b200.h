@@ -1,0 +1,225 @@
+/*
+ * nbody_b200.h - C ABI of the B200 (sm_100a) N-body force engine.
+ *
+ * The engine sits behind the desktop app's force-backend seam
+ *   IPhysicsComputeBackend.ComputeForces(BodySoA bodies, double softening)
+ *   (src/CelestialMechanics.Physics/Solvers/IPhysicsComputeBackend.cs:21-34)
+ * and is reached from C# through P/Invoke.  Every entry point is plain C:
+ * opaque handle, raw pointers, explicit sizes, int32 status.  No C++
+ * exception crosses this boundary and there is no CPU fallback: when the
+ * GPU path cannot run, the call returns a negative status and
+ * nb_last_error() says why.
+ *
+ * Conventions shared by all entry points
+ *   - G = 1 (AU, solar mass, time unit of the reference engine,
+ *     engine/include/celestial/core/constants.hpp:26,29).
+ *   - Host arrays are borrowed for the duration of the call only.
+ *   - `active` is one byte per body (C# bool[] passed as byte*).
+ *   - A handle owns one CUDA stream and its device buffers; it is not
+ *     thread-safe, separate handles are independent.
+ *   - Calls that take host arrays are synchronous: results are in the
+ *     host arrays when the call returns.
+ */
+#ifndef NBODY_B200_H
+#define NBODY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define NB_API __declspec(dllexport)
+#else
+#define NB_API __attribute__((visibility("default")))
+#endif
+
+typedef struct nb_engine nb_engine;
+
+/* Status codes.  Precedent: the reference ABI returns int32 0 / negative
+ * ErrorCode (engine/src/interop/native_api.cpp:30-55). */
+enum nb_status {
+    NB_OK = 0,
+    NB_ERR_INVALID_ARG = -1,
+    NB_ERR_CAPACITY = -2,       /* n above the handle's capacity            */
+    NB_ERR_CUDA = -3,           /* a CUDA runtime call failed               */
+    NB_ERR_TIMEOUT = -4,        /* a bounded device wait ran out            */
+    NB_ERR_STACK_OVERFLOW = -5, /* tree-walk frontier overflow (the reference
+                                   drops children silently, gpu_tree.cu:588) */
+    NB_ERR_NO_DEVICE = -6,      /* no CUDA device / not an sm_100 device    */
+    NB_ERR_NONFINITE = -7,      /* NaN/Inf in an input position or mass     */
+    NB_ERR_STATE = -8           /* call out of order (e.g. no state set)    */
+};
+
+/* Force modes (low 4 bits of `flags`). */
+enum nb_mode {
+    NB_MODE_DIRECT = 0,          /* tiled O(n^2), FP32 pair math on FP64-differenced coords */
+    NB_MODE_DIRECT_FP64 = 1,     /* tiled O(n^2), FP64 arithmetic of CpuParallelBackend     */
+    NB_MODE_BARNES_HUT = 2,      /* warp-group tree walk, monopole+quadrupole, FP32 pairs   */
+    NB_MODE_BARNES_HUT_REF = 3   /* per-body walk with the reference's MAC and monopole     */
+};
+#define NB_MODE_MASK 0xF
+#define NB_FLAG_SHELL_THEOREM 0x10  /* IGravityModelAwareBackend.EnableShellTheorem          */
+#define NB_FLAG_NO_QUADRUPOLE 0x20  /* monopole only in NB_MODE_BARNES_HUT                   */
+#define NB_FLAG_COLLISIONS 0x40     /* nb_step: broad phase + merge + compaction per step    */
+#define NB_FLAG_LEARNED_MAC 0x80    /* NB_MODE_BARNES_HUT: MLP opening criterion              */
+
+/* Parameter ids for nb_set_param_f64 / nb_set_param_i32. */
+enum nb_param {
+    NB_PARAM_THETA = 1,            /* f64, opening angle, default 0.5                         */
+    NB_PARAM_LEAF_CAPACITY = 2,    /* i32, bodies per leaf bucket of the walk tree, default 8  */
+    NB_PARAM_MAX_MERGES_FRAME = 3, /* i32, default 64 (simulation_config.hpp:57)               */
+    NB_PARAM_MAX_MERGES_BODY = 4,  /* i32, default 2  (simulation_config.hpp:58)               */
+    NB_PARAM_MIN_RADIUS = 5,       /* f64, density-model floor for merged radii, default 1e-10 */
+    NB_PARAM_DENSITY_MERGE = 6,    /* i32, 1 = density-preserving merge radius (default 1)     */
+    NB_PARAM_TIMING = 7,           /* i32, 1 = record per-stage CUDA events (default 1)        */
+    NB_PARAM_MAC_BUDGET = 8,       /* f64, learned MAC: max predicted log10 rel. error         */
+    NB_PARAM_GROUP_BODIES = 9      /* i32, bodies per walk group: 32 or 64 (default 32)        */
+};
+
+/* Indices into nb_get_timings() output (milliseconds, CUDA events).
+ * Mirrors BarnesHutBackend.LastBuildTimeMs/LastTraversalTimeMs/LastTotalTimeMs
+ * (src/CelestialMechanics.Physics/Solvers/BarnesHutBackend.cs:101-107). */
+enum nb_timing {
+    NB_T_BUILD = 0,     /* bbox + keys + sort + tree + multipoles */
+    NB_T_TRAVERSAL = 1, /* walk or direct sum                     */
+    NB_T_TOTAL = 2,     /* whole last force evaluation            */
+    NB_T_SORT = 3,      /* keys + radix sort                      */
+    NB_T_TREE = 4,      /* radix tree + octree + multipoles       */
+    NB_T_COUNT = 5
+};
+
+/* Indices into nb_get_counters() output. */
+enum nb_counter {
+    NB_C_CELL_INTERACTIONS = 0,     /* body-cell (multipole) interactions, last evaluation */
+    NB_C_BODY_INTERACTIONS = 1,     /* body-body interactions, last evaluation              */
+    NB_C_NODES = 2,                 /* walk-tree nodes                                      */
+    NB_C_ACTIVE = 3,                /* active bodies in the last evaluation                 */
+    NB_C_PAIRS = 4,                 /* collision pairs found, last step                     */
+    NB_C_MERGES = 5,                /* merges performed, last step                          */
+    NB_C_OVERFLOWS = 6,             /* walk frontier overflows (non-zero means an error)    */
+    NB_C_COUNT = 7
+};
+
+/* ---- lifetime -------------------------------------------------------- */
+
+/* Create a handle on CUDA device `device` able to hold `capacity` bodies.
+ * Replaces construction of a backend in NBodySolver.SelectBackend
+ * (src/CelestialMechanics.Physics/Solvers/NBodySolver.cs:451-484). */
+NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out);
+NB_API int32_t nb_destroy(nb_engine* h);
+/* Message of the last failed call on this handle (static storage per handle).
+ * Precedent: celestial_get_last_error_message (native_api.h:292-294). */
+NB_API const char* nb_last_error(const nb_engine* h);
+NB_API int32_t nb_set_param_f64(nb_engine* h, int32_t param, double value);
+NB_API int32_t nb_set_param_i32(nb_engine* h, int32_t param, int32_t value);
+NB_API int32_t nb_get_timings(const nb_engine* h, double* out, int32_t n);
+NB_API int32_t nb_get_counters(const nb_engine* h, int64_t* out, int32_t n);
+/* cudaStream_t of the handle, for callers that time with CUDA events. */
+NB_API void* nb_stream(nb_engine* h);
+NB_API const char* nb_version(void);
+
+/* ---- the seam --------------------------------------------------------- */
+
+/* IPhysicsComputeBackend.ComputeForces(BodySoA, softening)
+ * (IPhysicsComputeBackend.cs:33; arithmetic of CpuParallelBackend.cs:99-142
+ * and GravityKernel.cs:9-33).  Writes acc for all i in [0,n): active i get
+ * the sum over active j != i, inactive i get 0.  radius may be NULL unless
+ * NB_FLAG_SHELL_THEOREM is set. */
+NB_API int32_t nb_compute_forces(nb_engine* h, int32_t n,
+                                 const double* px, const double* py, const double* pz,
+                                 const double* mass, const double* radius,
+                                 const uint8_t* active, double softening, int32_t flags,
+                                 double* ax, double* ay, double* az);
+
+/* ---- device-resident state (ISoAIntegrator path) ---------------------- */
+
+/* Upload a BodySoA (BodySoA.cs:39-175).  old_ax/ay/az, radius, density and
+ * collidable may be NULL (zeros / 0 / 0 / all collidable). */
+NB_API int32_t nb_set_state(nb_engine* h, int32_t n,
+                            const double* px, const double* py, const double* pz,
+                            const double* vx, const double* vy, const double* vz,
+                            const double* mass, const double* radius, const double* density,
+                            const uint8_t* active, const uint8_t* collidable,
+                            const double* old_ax, const double* old_ay, const double* old_az);
+/* Download state; any pointer may be NULL.  `ids` receives each row's
+ * original body index (rows move when compaction removes merged bodies). */
+NB_API int32_t nb_get_state(nb_engine* h, int32_t* n_out,
+                            double* px, double* py, double* pz,
+                            double* vx, double* vy, double* vz,
+                            double* ax, double* ay, double* az,
+                            double* mass, double* radius, uint8_t* active, int32_t* ids);
+/* n_steps of SoAVerletIntegrator.Step (SoAVerletIntegrator.cs:48-116) on
+ * device-resident state: half kick, drift, forces, half kick.  With
+ * NB_FLAG_COLLISIONS each step then runs broad phase, merge
+ * (collision_resolver.cpp:20-100 semantics) and order-preserving compaction
+ * (compact_kernel.cu:39 mask). */
+NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softening,
+                       int32_t flags);
+/* Energy/momentum diagnostics of the device state, FP64
+ * (EnergyCalculator.cs:16-78, NewtonianGravity.cs:68-77, energy_tracker.cpp:194-240).
+ * out[0..12]: KE, PE, E, Px, Py, Pz, Lx, Ly, Lz, COMx, COMy, COMz, M.
+ * PE is the exact pairwise sum when pe_mode == 0, the tree potential
+ * 1/2 sum m_i phi_i when pe_mode == 1. */
+NB_API int32_t nb_diagnostics(nb_engine* h, double softening, int32_t pe_mode, double* out13);
+/* ForceErrorAnalyzer.CompareForces metric (ForceErrorAnalyzer.cs:67-134)
+ * of the device acc against an FP64 direct sum over all active sources,
+ * for `n_samples` bodies drawn uniformly with `seed` (all bodies if
+ * n_samples <= 0 or >= n).  out3: mean, max, rms relative error. */
+NB_API int32_t nb_force_error(nb_engine* h, int32_t n_samples, uint64_t seed,
+                              double softening, int32_t flags, double* out3);
+
+/* ---- single stages on host arrays (integer-stage parity) -------------- */
+
+/* Morton keys.  mode 0: per-axis AABB normalisation and the (2^21-1)
+ * scale of morton_code_kernel (morton_kernel.cu:11-45, morton.hpp:13-35);
+ * idx[i] = i, inactive keys = ~0.  mode 1: octree-aligned keys in the cube
+ * (cx,cy,cz,half) = cube4, or the bounding cube of the active bodies
+ * (gpu_tree.cu:163-167) when cube4 == NULL; cube4_out (may be NULL)
+ * receives the cube used. */
+NB_API int32_t nb_morton_keys(nb_engine* h, int32_t n,
+                              const double* px, const double* py, const double* pz,
+                              const uint8_t* active, int32_t mode, const double* cube4,
+                              uint64_t* keys, int32_t* idx, double* cube4_out);
+/* Stable sort of (key, value) pairs by key, in place; replaces
+ * launch_radix_sort (morton_kernel.cu:185-230) with a stable sort. */
+NB_API int32_t nb_sort_pairs(nb_engine* h, int32_t n, uint64_t* keys, int32_t* values);
+/* Build the octree of the active bodies in cube4 (NULL: bounding cube) and
+ * export it, replacing tree_build_kernel (gpu_tree.cu:269-464) and
+ * OctreeBuilder::build (octree_builder.cpp:8-135).  Nodes are in walk order
+ * (children contiguous).  Per node: level, first_child (-1 for leaves),
+ * n_children, body_first, body_count (in sorted order), mass, com[3],
+ * quad[6] (Qxx,Qyy,Qzz,Qxy,Qxz,Qyz).  sorted_idx receives the body index
+ * of each sorted position.  Any output pointer may be NULL.  *n_nodes is
+ * set to the node count; when it exceeds max_nodes nothing else is written
+ * and NB_ERR_CAPACITY is returned. */
+NB_API int32_t nb_build_octree(nb_engine* h, int32_t n,
+                               const double* px, const double* py, const double* pz,
+                               const double* mass, const uint8_t* active,
+                               const double* cube4, int32_t leaf_capacity, int32_t max_nodes,
+                               int32_t* n_nodes, int32_t* level, int32_t* first_child,
+                               int32_t* n_children, int32_t* body_first, int32_t* body_count,
+                               double* node_mass, double* com3, float* quad6,
+                               int32_t* sorted_idx, uint64_t* sorted_keys);
+/* Order-preserving compaction indices: dest[i] = destination row of body i
+ * or -1 when it is removed (mask is_active && mass > 0, compact_kernel.cu:39);
+ * *n_kept = survivors. */
+NB_API int32_t nb_compact_indices(nb_engine* h, int32_t n, const uint8_t* active,
+                                  const double* mass, int32_t* dest, int32_t* n_kept);
+/* Collision broad phase: all pairs of active, collidable bodies with
+ * |xi-xj|^2 < (ri+rj)^2, as (lo, hi) sorted lexicographically
+ * (collision_kernel.cu:16-64 test, CollisionResolver::sort_pairs order).
+ * *n_pairs is the true count even when it exceeds max_pairs (then only
+ * max_pairs are written and NB_ERR_CAPACITY is returned). */
+NB_API int32_t nb_broad_phase(nb_engine* h, int32_t n,
+                              const double* px, const double* py, const double* pz,
+                              const double* radius, const uint8_t* active,
+                              const uint8_t* collidable, int32_t max_pairs,
+                              int32_t* pair_lo, int32_t* pair_hi, int32_t* n_pairs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NBODY_B200_H */

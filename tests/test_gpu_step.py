@@ -1,0 +1,112 @@
+"""Device-resident stepping, diagnostics, collisions and compaction on the
+GPU against the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import bodies_dict
+from nbody_b200 import (FLAG_COLLISIONS, FLAG_SHELL_THEOREM, MODE_BARNES_HUT, MODE_DIRECT_FP64,
+                        NBodyError, scenarios)
+from nbody_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+
+def test_verlet_fp64_trajectory_bit_exact(engine, oracle):
+    """K Verlet steps with the FP64 direct sum on the device reproduce the
+    CPU SoAVerletIntegrator + CpuParallelBackend trajectory bit for bit."""
+    b = scenarios.plummer(300, seed=0)
+    b.active[::17] = 0
+    engine.set_state(b)
+    engine.step(50, 1e-3, 1e-4, MODE_DIRECT_FP64)
+    got, ids = engine.get_state()
+    want = oracle.verlet_direct(bodies_dict(b), 1e-4, 1e-3, 50)
+    np.testing.assert_array_equal(ids, np.arange(300))
+    for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az"):
+        np.testing.assert_array_equal(getattr(got, k), want[k], err_msg=k)
+
+
+def test_energy_drift_10k_steps_plummer_1000(engine, oracle):
+    """The FP64 direct-sum workload (N=1000 Plummer, seed 0, eps 1e-4,
+    dt 1e-3, 10k steps): the device run reproduces the CPU trajectory, so
+    the energy drift is the CPU drift."""
+    b = scenarios.plummer(1000, seed=0)
+    engine.set_state(b, old_acc=False)
+    e0 = engine.diagnostics(1e-4)["e"]
+    engine.step(10_000, 1e-3, 1e-4, MODE_DIRECT_FP64)
+    e1 = engine.diagnostics(1e-4)["e"]
+    drift_gpu = (e1 - e0) / abs(e0)
+    got, _ = engine.get_state()
+    want = oracle.verlet_direct(bodies_dict(b), 1e-4, 1e-3, 10_000)
+    want["active"] = b.active
+    drift_cpu = (oracle.energy(want, 1e-4)["e"] - oracle.energy(bodies_dict(b), 1e-4)["e"]) / abs(e0)
+    np.testing.assert_array_equal(got.px, want["px"])
+    assert drift_gpu == pytest.approx(drift_cpu, rel=1e-6, abs=1e-12)
+
+
+def test_diagnostics_match_oracle(engine, oracle):
+    b = scenarios.plummer(5000, seed=4)
+    b.active[::9] = 0
+    engine.set_state(b)
+    d = engine.diagnostics(1e-4, pe_mode=0)
+    w = oracle.energy(bodies_dict(b), 1e-4)
+    for k in ("ke", "pe", "e", "px", "py", "pz", "lx", "ly", "lz", "comx", "comy", "comz", "m"):
+        assert d[k] == pytest.approx(w[k], rel=1e-11, abs=1e-14), k
+    # tree potential (pe_mode 1) approximates the exact pair sum
+    dt = engine.diagnostics(1e-4, pe_mode=1)
+    assert dt["pe"] == pytest.approx(w["pe"], rel=1e-3)
+
+
+def test_force_error_audit_matches_oracle(engine, oracle):
+    b = scenarios.plummer(40_000, seed=6)
+    engine.set_param(N.PARAM_THETA, 0.5)
+    engine.set_state(b, old_acc=False)
+    engine.step(1, 0.0, 1e-4, MODE_BARNES_HUT)  # dt = 0: forces at the initial positions
+    mean, mx, rms = engine.force_error(0, 0, 1e-4)
+    got, _ = engine.get_state()
+    want = oracle.direct_forces(b.px, b.py, b.pz, b.mass, b.active, 1e-4)
+    wm, wx, wr = oracle.force_error((got.ax, got.ay, got.az), want, b.active)
+    assert mean == pytest.approx(wm, rel=1e-9) and rms == pytest.approx(wr, rel=1e-9)
+    assert mx == pytest.approx(wx, rel=1e-9)
+    assert rms < 1e-3
+
+
+def test_merge_and_compaction_step_bit_exact(engine, oracle):
+    """dt = 0 step with collisions: pairs, merges (sequential CPU-resolver
+    semantics) and compaction equal the oracle's."""
+    d = scenarios.collisional_disk(4000, seed=12, radius_scale=2500.0)
+    engine.set_state(d, old_acc=False)
+    engine.step(1, 0.0, 1e-4, MODE_BARNES_HUT | FLAG_SHELL_THEOREM | FLAG_COLLISIONS)
+    c = engine.counters()
+    got, ids = engine.get_state()
+    lo, hi = oracle.broad_phase(d.px, d.py, d.pz, d.radius, d.active, d.collidable)
+    out, nm = oracle.resolve_merges(bodies_dict(d), lo, hi)
+    assert c[N.C_PAIRS] == len(lo) and c[N.C_MERGES] == nm and nm > 0
+    dest, kept = oracle.compact_indices(out["active"], out["mass"])
+    assert len(ids) == kept
+    keep = np.nonzero(dest >= 0)[0]
+    np.testing.assert_array_equal(ids, keep)
+    for k in ("px", "py", "pz", "vx", "vy", "vz", "mass"):
+        np.testing.assert_array_equal(getattr(got, k), out[k][keep], err_msg=k)
+    np.testing.assert_allclose(got.radius, out["radius"][keep], rtol=4e-16)
+
+
+def test_collisional_steps_conserve_mass_and_momentum(engine):
+    d = scenarios.collisional_disk(20_000, seed=2, radius_scale=1500.0)
+    engine.set_state(d, old_acc=False)
+    p0 = engine.diagnostics(1e-4)
+    engine.step(5, 1e-3, 1e-4, MODE_BARNES_HUT | FLAG_SHELL_THEOREM | FLAG_COLLISIONS)
+    p1 = engine.diagnostics(1e-4)
+    assert p1["m"] == pytest.approx(p0["m"], rel=1e-13)
+    got, ids = engine.get_state()
+    assert len(ids) <= 20_001 and np.all(np.diff(ids) > 0)
+
+
+def test_step_before_state_is_an_error():
+    from nbody_b200 import Engine
+
+    with Engine(1024) as e:
+        with pytest.raises(NBodyError) as err:
+            e.step(1, 1e-3, 1e-4, MODE_BARNES_HUT)
+        assert err.value.status == N.NB_ERR_STATE
