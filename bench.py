@@ -38,6 +38,10 @@ THETA, EPS, DT, SEED = 0.5, 1e-4, 1e-4, 1
 FLOPS_BODY, FLOPS_CELL_QUAD = 20, 51
 
 
+def workload_name(n: int) -> str:
+    return "bh_plummer_1m" if n == N_BODIES else f"bh_plummer_n{n}"
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -163,7 +167,7 @@ def run_reference(args, ws, rank):
         return
     from nbody_b200 import scenarios
 
-    b = scenarios.plummer(N_BODIES, 1.0, 1.0, seed=SEED)
+    b = scenarios.plummer(args.n, 1.0, 1.0, seed=SEED)
     threads = os.cpu_count() or 1
     warm = min(args.warmup, 1)
     steps = max(1, min(args.steps, 3))
@@ -182,7 +186,7 @@ def run_reference(args, ws, rank):
         "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * total / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Plummer sphere)",
-        "config": {"workload": "bh_plummer_1m", "n": N_BODIES, "theta": THETA, "eps": EPS,
+        "config": {"workload": workload_name(args.n), "n": args.n, "theta": THETA, "eps": EPS,
                    "multipole": "monopole (reference)", "mac": "geometric"},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": kind,
                          "sample": sample},
@@ -199,8 +203,8 @@ def run_b200(args, ws, rank, local):
 
     dev = local
     torch.cuda.set_device(dev)
-    b = scenarios.plummer(N_BODIES, 1.0, 1.0, seed=SEED)
-    eng = Engine(N_BODIES, device=dev)
+    b = scenarios.plummer(args.n, 1.0, 1.0, seed=SEED)
+    eng = Engine(args.n, device=dev)
     eng.set_param(N.PARAM_THETA, THETA)
     flags = MODE_BARNES_HUT
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
@@ -278,7 +282,7 @@ def run_b200(args, ws, rank, local):
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Plummer sphere, numpy PCG64)",
-            "config": {"workload": "bh_plummer_1m", "n": N_BODIES, "theta": THETA, "eps": EPS,
+            "config": {"workload": workload_name(args.n), "n": args.n, "theta": THETA, "eps": EPS,
                        "dt": DT, "seed": SEED, "multipole": "monopole+quadrupole",
                        "mac": "geometric", "state": "f64", "pair_forces": "f32",
                        "parallelism": f"replicas x{ws}",
@@ -321,6 +325,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n", type=int, default=N_BODIES,
+                    help="bodies (default the 1,048,576-body workload; smaller for profiling)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     try:

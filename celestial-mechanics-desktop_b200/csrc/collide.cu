@@ -71,7 +71,12 @@ __global__ void k_broad_phase(int n, State s, const double4* __restrict__ sbody,
     int stack[176];
     int sp = 0;
     stack[sp++] = 0;
+    int visits = 0;  // every node is visited at most once per body
     while (sp > 0) {
+        if (++visits > 2 * n + 64) {
+            dev_flag(err, kErrOverflow);
+            break;
+        }
         const int node = stack[--sp];
         const int4 lk = t.link[node];
         const float4 q1 = t.q1[node];

@@ -88,8 +88,10 @@ __device__ __forceinline__ void kahan32(float& s, float& c, float x) {
 }
 
 // Targets and sources are the n sorted bodies (all active).  Block b handles
-// targets [b*512, b*512+512); its reference point is its first body.
-template <bool SHELL>
+// targets [b*512, b*512+512); its reference point is its first body.  The
+// self pair has dx = dy = dz = 0 and contributes 0 when eps > 0; GUARD (used
+// when eps == 0) zeroes 1/r at r = 0 instead of evaluating 0 * inf.
+template <bool SHELL, bool GUARD>
 __global__ void __launch_bounds__(kD32Threads)
 k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict__ srad,
               const uint32_t* __restrict__ sidx, float eps2, double* __restrict__ ax,
@@ -140,10 +142,9 @@ k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict_
                 const float dx = bx[u] - q.x, dy = by[u] - q.y, dz = bz[u] - q.z;
                 const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 const float r2 = raw + eps2;
-                const float inv = rsqrtf(r2);
+                const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrtf(r2);
                 float f = q.w * (inv * inv * inv);
                 if (SHELL && raw < sh.x) f = sh.y;
-                // self pair: dx = dy = dz = 0 contributes 0 (eps > 0 required)
                 tx[u] = fmaf(-f, dx, tx[u]);
                 ty[u] = fmaf(-f, dy, ty[u]);
                 tz[u] = fmaf(-f, dz, tz[u]);
@@ -189,8 +190,13 @@ void direct_fp32(cudaStream_t st, int n, const double4* sbody, const float* srad
     if (n <= 0) return;
     const float eps2 = (float)(eps * eps);
     const int g = ceil_div(n, kD32Threads * kD32Per);
-    if (shell) k_direct_fp32<true><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
-    else k_direct_fp32<false><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
+    if (eps2 > 0.f) {
+        if (shell) k_direct_fp32<true, false><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
+        else k_direct_fp32<false, false><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
+    } else {
+        if (shell) k_direct_fp32<true, true><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
+        else k_direct_fp32<false, true><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
+    }
 }
 
 }  // namespace nb

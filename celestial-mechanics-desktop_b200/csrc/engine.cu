@@ -29,6 +29,7 @@ struct Scal {
     unsigned long long bbox_ord[6];
     int n_active;
     unsigned group_ctr;
+    int n_groups;
     double cube[4];
     double cube_in[4];
     int err[nb::kErrCount];
@@ -78,6 +79,7 @@ struct nb_engine {
     double* part = nullptr;
     double* phi = nullptr;
     int32_t* targets = nullptr;
+    int2* groups = nullptr;
     double* tgt_out = nullptr;
     nb::CollideBufs col{};
     Scal* scal = nullptr;
@@ -227,6 +229,8 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
         a.pot = nullptr;
         a.front = h->front;
         a.group_ctr = &sc->group_ctr;
+        a.groups = h->groups;
+        a.n_groups = &sc->n_groups;
         a.counters = sc->counters;
         a.err = sc->err;
         if (ref) {
@@ -333,6 +337,7 @@ NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
         if ((r = dalloc(h, &h->rows, cap)) || (r = dalloc(h, &h->phi, cap))) break;
         if ((r = dalloc(h, (char**)&h->part, nb::diag_partial_bytes(capacity)))) break;
         if ((r = dalloc(h, &h->targets, cap)) || (r = dalloc(h, &h->tgt_out, 3 * cap))) break;
+        if ((r = dalloc(h, &h->groups, cap))) break;
         if ((r = nb::collide_alloc(h->col, capacity, [h](void** p, size_t b) {
                  return dalloc(h, (char**)p, b);
              })))
@@ -594,6 +599,8 @@ NB_API int32_t nb_diagnostics(nb_engine* h, double softening, int32_t pe_mode, d
         a.pot = h->phi;
         a.front = h->front;
         a.group_ctr = &sc->group_ctr;
+        a.groups = h->groups;
+        a.n_groups = &sc->n_groups;
         a.counters = nullptr;
         a.err = sc->err;
         nb::walk_group(h->st, h->wcfg, a, true, false, true);

@@ -318,7 +318,7 @@ __global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody
     }
     // climb: the last child to arrive reduces the parent
     int pb = t.parent_bin[w];
-    while (pb >= 0) {
+    for (int guard = 0; pb >= 0 && guard < 64; guard++) {  // <= 22 levels up
         int p = __ldcg(&t.walk_index[pb]);
         __threadfence();
         int4 pl = __ldcg(&t.link[p]);

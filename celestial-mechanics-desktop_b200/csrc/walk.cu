@@ -5,8 +5,8 @@
 // drops children on overflow) with a warp-cooperative walk in the style of
 // Bedorf, Gaburov & Portegies Zwart 2012 (Bonsai):
 //   * a warp owns a group of 32 consecutive Morton-sorted bodies and walks
-//     the tree once for all of them, breadth first, 32 candidate nodes per
-//     step (one per lane);
+//     the tree once for all of them with a warp-shared stack, testing 32
+//     candidate nodes per round (one per lane);
 //   * the opening test is the reference's geometric MAC, 4h^2 < theta^2 d^2
 //     (gpu_tree.cu:567-569), with d the distance from the cell's centre of
 //     mass to the group's bounding box, so it is at least as strict as the
@@ -18,7 +18,7 @@
 //     list entry and per body, then the pair math is FP32 with monopole +
 //     traceless quadrupole; every list flush is summed in FP32 and folded
 //     into a compensated (Kahan) accumulator;
-//   * frontier overflow is reported (NB_ERR_STACK_OVERFLOW), never dropped
+//   * stack overflow is reported (NB_ERR_STACK_OVERFLOW), never dropped
 //     silently.
 #include "walk.cuh"
 
@@ -31,6 +31,7 @@ constexpr int kPartCap = 128;
 // per-warp shared memory, in floats
 constexpr int kWarpFloats = kCellCap * 9 + kPartCap * 4 + kPartCap * 2 + kPartCap;
 constexpr int kWalkSmem = kWalkWarps * kWarpFloats * 4;
+constexpr int kMaxWalkRounds = 1 << 22;
 
 __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     float y = x - c;
@@ -51,11 +52,10 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
     float4* p0 = (float4*)(c2 + kCellCap);           // rel xyz, mass
     float2* p1 = (float2*)(p0 + kPartCap);           // R^2, m / (R^2 + eps^2)^1.5
     int* p2 = (int*)(p1 + kPartCap);                 // sorted index
-    int* fa = a.front + (size_t)(blockIdx.x * kWalkWarps + warp) * 2 * a.front_cap;
-    int* fb = fa + a.front_cap;
+    int* fa = a.front + (size_t)(blockIdx.x * kWalkWarps + warp) * a.front_cap;
     const float eps2 = (float)a.eps2;
     const float theta2 = (float)a.theta2;
-    const int ngroups = (a.n + 31) >> 5;
+    const int ngroups = *a.n_groups;
     unsigned long long cnt_cell = 0, cnt_body = 0;
 
     for (;;) {
@@ -63,10 +63,11 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
         if (lane == 0) g = (int)atomicAdd(a.group_ctr, 1u);
         g = __shfl_sync(FULL, g, 0);
         if (g >= ngroups) break;
-        const int s = g * 32 + lane;
-        const bool valid = s < a.n;
-        const double4 b = a.sbody[valid ? s : a.n - 1];
-        const int nvalid = min(32, a.n - g * 32);
+        const int2 grp = a.groups[g];  // body_first, body_count (<= 32)
+        const int s = grp.x + lane;
+        const bool valid = lane < grp.y;
+        const double4 b = a.sbody[valid ? s : grp.x];
+        const int nvalid = grp.y;
         const double mnx = warp_min(b.x), mny = warp_min(b.y), mnz = warp_min(b.z);
         const double mxx = warp_max(b.x), mxy = warp_max(b.y), mxz = warp_max(b.z);
         const double gcx = 0.5 * (mnx + mxx), gcy = 0.5 * (mny + mxy), gcz = 0.5 * (mnz + mxz);
@@ -151,15 +152,23 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
             __syncwarp();
         };
 
-        int* cur = fa;
-        int* nxt = fb;
-        int ncur = 1;
-        if (lane == 0) cur[0] = 0;
+        // Warp-shared LIFO stack of nodes still to test: 32 are popped per
+        // round (one per lane), children of opened nodes are pushed on top.
+        int* stk = fa;
+        int sp = 1;
+        if (lane == 0) stk[0] = 0;
         __syncwarp();
-        while (ncur > 0) {
-            int nnext = 0;
-            for (int off = 0; off < ncur; off += 32) {
-                const int node = (off + lane < ncur) ? cur[off + lane] : -1;
+        int rounds = 0;
+        while (sp > 0) {
+            if (++rounds > kMaxWalkRounds) {
+                if (lane == 0) dev_flag(a.err, kErrOverflow);
+                break;
+            }
+            {
+                const int take = min(32, sp);
+                const int node = (lane < take) ? stk[sp - take + lane] : -1;
+                sp -= take;
+                __syncwarp();  // every lane holds its node before the pushes below
                 bool take_cell = false, is_leaf = false, open = false;
                 int4 lk = make_int4(0, 0, 0, 0);
                 float rx = 0.f, ry = 0.f, rz = 0.f, mass = 0.f;
@@ -199,17 +208,18 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
                     nc += k;
                     __syncwarp();
                 }
-                // 2. children of opened nodes -> next frontier
+                // 2. children of opened nodes -> pushed on the stack
                 const int nch = open ? lk.y : 0;
                 const int inc = warp_incl_scan(nch);
                 const int tot = __shfl_sync(FULL, inc, 31);
                 if (tot > 0) {
-                    if (nnext + tot > a.front_cap) {
+                    if (sp + tot > a.front_cap) {
                         if (lane == 0) dev_flag(a.err, kErrOverflow);
                     } else {
-                        for (int k = 0; k < nch; k++) nxt[nnext + inc - nch + k] = lk.x + k;
-                        nnext += tot;
+                        for (int k = 0; k < nch; k++) stk[sp + inc - nch + k] = lk.x + k;
+                        sp += tot;
                     }
+                    __syncwarp();
                 }
                 // 3. bodies of leaves that were not accepted -> particle list
                 const int cb = is_leaf ? lk.w : 0;
@@ -244,11 +254,6 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
                     __syncwarp();
                 }
             }
-            int* tmp = cur;
-            cur = nxt;
-            nxt = tmp;
-            ncur = nnext;
-            __syncwarp();
         }
         if (nc) flush_cells();
         if (np) flush_parts();
@@ -288,7 +293,12 @@ __global__ void k_walk_reference(WalkArgs a) {
     int stack[176];
     int sp = 0;
     stack[sp++] = 0;
+    int visits = 0;  // every node is visited at most once per body
     while (sp > 0) {
+        if (++visits > 2 * a.n + 64) {
+            dev_flag(a.err, kErrOverflow);
+            break;
+        }
         const int k = stack[--sp];
         const double4 cm = a.t.com[k];
         if (cm.w == 0.0) continue;
@@ -358,6 +368,28 @@ __global__ void k_walk_reference(WalkArgs a) {
     a.az[row] = az;
 }
 
+// Group order in the list does not matter: every group's walk and sums are
+// independent of the others, so results are deterministic.
+__global__ void k_find_groups(TreeBufs t, int2* __restrict__ groups, int* __restrict__ n_groups) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= *t.n_nodes) return;
+    const int4 lk = t.link[w];
+    const int pb = t.parent_bin[w];
+    const int pcnt = pb < 0 ? 0x7FFFFFFF : t.blast[pb] - t.bfirst[pb] + 1;
+    if (pcnt <= 32) return;  // an ancestor already forms the group
+    if (lk.w <= 32) {
+        groups[atomicAdd(n_groups, 1)] = make_int2(lk.z, lk.w);
+    } else if (lk.y == 0) {  // a level-21 bucket of more than 32 equal keys
+        for (int off = 0; off < lk.w; off += 32)
+            groups[atomicAdd(n_groups, 1)] = make_int2(lk.z + off, min(32, lk.w - off));
+    }
+}
+
+void find_groups(cudaStream_t st, const TreeBufs& t, int n, int2* groups, int* n_groups) {
+    cudaMemsetAsync(n_groups, 0, sizeof(int), st);
+    if (n > 0) k_find_groups<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, groups, n_groups);
+}
+
 void walk_init(int sms, WalkConfig& cfg) {
     cudaFuncSetAttribute((const void*)k_walk_group<true, false, false>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
@@ -376,17 +408,18 @@ void walk_init(int sms, WalkConfig& cfg) {
                                                   kWalkThreads, kWalkSmem);
     if (per_sm < 1) per_sm = 1;
     cfg.blocks = sms * per_sm;
-    cfg.front_cap = 4096;
+    cfg.front_cap = 16384;
 }
 
 size_t walk_front_bytes(const WalkConfig& cfg) {
-    return (size_t)cfg.blocks * kWalkWarps * 2 * cfg.front_cap * sizeof(int);
+    return (size_t)cfg.blocks * kWalkWarps * cfg.front_cap * sizeof(int);
 }
 
 void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,
                 bool pot) {
     if (a.n <= 0) return;
     a.front_cap = cfg.front_cap;
+    find_groups(st, a.t, a.n, a.groups, a.n_groups);
     cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
     const dim3 g(cfg.blocks), b(kWalkThreads);
     if (pot) {

@@ -17,8 +17,10 @@ struct WalkArgs {
     double* ay;
     double* az;
     double* pot;                // potential by body row (may be null)
-    int* front;                 // per-warp frontier buffers, 2 x front_cap ints
+    int* front;                 // per-warp node stacks, front_cap ints each
     int front_cap;
+    int2* groups;               // walk groups: body_first, body_count (<= 32)
+    int* n_groups;
     unsigned* group_ctr;        // dynamic group counter (zeroed)
     unsigned long long* counters;  // [0] body-cell, [1] body-body interactions
     int* err;
@@ -30,6 +32,10 @@ struct WalkConfig {
 };
 
 void walk_init(int sms, WalkConfig& cfg);
+// Walk groups: the octree nodes holding <= 32 bodies whose parent holds
+// more (spatially compact sets of consecutive sorted bodies), plus 32-body
+// slices of level-21 buckets that hold more than 32.  groups: >= n entries.
+void find_groups(cudaStream_t st, const TreeBufs& t, int n, int2* groups, int* n_groups);
 size_t walk_front_bytes(const WalkConfig& cfg);
 // Group walk, FP32 monopole(+quadrupole) on FP64-differenced coordinates.
 void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,

@@ -143,7 +143,7 @@ def test_walk_tree_invariants_and_multipoles(engine, cap):
         q = np.einsum("i,ij,ik->jk", m, 3 * d, d) - np.eye(3) * (m * r2).sum()
         want = np.array([q[0, 0], q[1, 1], q[2, 2], q[0, 1], q[0, 2], q[1, 2]])
         scale = (m * r2).sum() + 1e-300
-        np.testing.assert_allclose(t["quad"][k], want, rtol=0, atol=2e-5 * scale)
+        np.testing.assert_allclose(t["quad"][k], want, rtol=0, atol=2e-5 * scale + 1e-30)
 
 
 @pytest.mark.parametrize("n", [0, 1, 4096, 4097, 300_001])
