@@ -59,6 +59,7 @@ struct nb_engine {
     int timing = 1;
     double mac_budget = -3.0;
     int group_bodies = 32;
+    double group_pack = 2.0;
     // device-resident state
     int n = 0;
     int n_active = 0;
@@ -231,6 +232,7 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
         a.group_ctr = &sc->group_ctr;
         a.groups = h->groups;
         a.n_groups = &sc->n_groups;
+        a.pack = h->group_pack;
         a.counters = sc->counters;
         a.err = sc->err;
         if (ref) {
@@ -254,10 +256,14 @@ void collect_counters(nb_engine* h) {
     if (cudaMemcpy(c, h->scal->counters, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) {
         h->counters[NB_C_CELL_INTERACTIONS] = (int64_t)c[0];
         h->counters[NB_C_BODY_INTERACTIONS] = (int64_t)c[1];
+        h->counters[NB_C_MAX_GROUP_WORK] = (int64_t)c[2];
     }
     int nn = 0;
     if (h->ev_tree && cudaMemcpy(&nn, h->tree.n_nodes, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess)
         h->counters[NB_C_NODES] = nn;
+    int ng = 0;
+    if (h->ev_tree && cudaMemcpy(&ng, &h->scal->n_groups, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess)
+        h->counters[NB_C_GROUPS] = ng;
     h->counters[NB_C_ACTIVE] = h->n_active;
 }
 
@@ -380,6 +386,10 @@ NB_API int32_t nb_set_param_f64(nb_engine* h, int32_t p, double v) {
             return NB_OK;
         case NB_PARAM_MIN_RADIUS: h->min_radius = v; return NB_OK;
         case NB_PARAM_MAC_BUDGET: h->mac_budget = v; return NB_OK;
+        case NB_PARAM_GROUP_PACK:
+            if (!(v >= 0.0 && v <= 64.0)) return fail(h, NB_ERR_INVALID_ARG, "group packing must be 0..64");
+            h->group_pack = v;
+            return NB_OK;
         default: return fail(h, NB_ERR_INVALID_ARG, "unknown f64 parameter %d", p);
     }
 }
@@ -601,6 +611,7 @@ NB_API int32_t nb_diagnostics(nb_engine* h, double softening, int32_t pe_mode, d
         a.group_ctr = &sc->group_ctr;
         a.groups = h->groups;
         a.n_groups = &sc->n_groups;
+        a.pack = h->group_pack;
         a.counters = nullptr;
         a.err = sc->err;
         nb::walk_group(h->st, h->wcfg, a, true, false, true);

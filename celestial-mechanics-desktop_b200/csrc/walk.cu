@@ -80,6 +80,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
         float sax = 0.f, say = 0.f, saz = 0.f, cax = 0.f, cay = 0.f, caz = 0.f;
         float spot = 0.f, cpot = 0.f;
         int nc = 0, np = 0;
+        unsigned long long grp_entries = 0;  // list entries of this group (load-balance record)
 
         auto flush_cells = [&]() {
             float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
@@ -119,6 +120,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
             kahan(saz, caz, tz);
             if (POT) kahan(spot, cpot, tp);
             cnt_cell += (unsigned long long)nc * nvalid;
+            grp_entries += nc;
             nc = 0;
             __syncwarp();
         };
@@ -148,6 +150,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
             kahan(saz, caz, tz);
             if (POT) kahan(spot, cpot, tp);
             cnt_body += (unsigned long long)np * nvalid;
+            grp_entries += np;
             np = 0;
             __syncwarp();
         };
@@ -257,6 +260,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
         }
         if (nc) flush_cells();
         if (np) flush_parts();
+        if (lane == 0 && a.counters) atomicMax(&a.counters[2], grp_entries);
         if (valid) {
             const uint32_t row = a.sidx[s];
             a.ax[row] = (double)sax - (double)cax;
@@ -370,24 +374,84 @@ __global__ void k_walk_reference(WalkArgs a) {
 
 // Group order in the list does not matter: every group's walk and sums are
 // independent of the others, so results are deterministic.
-__global__ void k_find_groups(TreeBufs t, int2* __restrict__ groups, int* __restrict__ n_groups) {
+// One thread per node holding more than 32 bodies: its children with at
+// most 32 bodies are consecutive in body order, and runs of them are packed
+// greedily into groups of at most 32 bodies (siblings share the parent's
+// cell, so a packed group stays compact); a level-21 bucket of more than 32
+// equal keys is cut into slices of 32.  pack = 0 keeps one child per group.
+struct Box {
+    double lo[3], hi[3];
+    __device__ void empty() {
+        for (int a = 0; a < 3; a++) { lo[a] = 1e300; hi[a] = -1e300; }
+    }
+    __device__ void add(const Box& b) {
+        for (int a = 0; a < 3; a++) { lo[a] = fmin(lo[a], b.lo[a]); hi[a] = fmax(hi[a], b.hi[a]); }
+    }
+    __device__ double ext() const {  // largest half extent
+        return 0.5 * fmax(fmax(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]);
+    }
+};
+
+// Sibling runs are packed only while the packed box stays within `pack`
+// times the larger part's box: siblings that sit far apart in a sparse cell
+// would make one group whose opening test walks most of the tree.
+__global__ void k_find_groups(TreeBufs t, const double4* __restrict__ sbody,
+                              int2* __restrict__ groups, int* __restrict__ n_groups, double pack) {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= *t.n_nodes) return;
     const int4 lk = t.link[w];
-    const int pb = t.parent_bin[w];
-    const int pcnt = pb < 0 ? 0x7FFFFFFF : t.blast[pb] - t.bfirst[pb] + 1;
-    if (pcnt <= 32) return;  // an ancestor already forms the group
     if (lk.w <= 32) {
-        groups[atomicAdd(n_groups, 1)] = make_int2(lk.z, lk.w);
-    } else if (lk.y == 0) {  // a level-21 bucket of more than 32 equal keys
+        if (w == 0) groups[atomicAdd(n_groups, 1)] = make_int2(lk.z, lk.w);  // small root
+        return;  // otherwise its parent packs it
+    }
+    if (lk.y == 0) {
         for (int off = 0; off < lk.w; off += 32)
             groups[atomicAdd(n_groups, 1)] = make_int2(lk.z + off, min(32, lk.w - off));
+        return;
     }
+    int run_first = 0, run_cnt = 0;
+    Box run;
+    run.empty();
+    for (int c = lk.x; c < lk.x + lk.y; c++) {
+        const int4 cl = t.link[c];
+        if (cl.w > 32) {  // handled by its own thread
+            if (run_cnt) groups[atomicAdd(n_groups, 1)] = make_int2(run_first, run_cnt);
+            run_cnt = 0;
+            continue;
+        }
+        Box cb;
+        cb.empty();
+        if (pack > 0.0)
+            for (int b = cl.z; b < cl.z + cl.w; b++) {
+                const double4 p = sbody[b];
+                cb.lo[0] = fmin(cb.lo[0], p.x); cb.hi[0] = fmax(cb.hi[0], p.x);
+                cb.lo[1] = fmin(cb.lo[1], p.y); cb.hi[1] = fmax(cb.hi[1], p.y);
+                cb.lo[2] = fmin(cb.lo[2], p.z); cb.hi[2] = fmax(cb.hi[2], p.z);
+            }
+        bool merge = false;
+        if (pack > 0.0 && run_cnt > 0 && run_cnt + cl.w <= 32) {
+            Box m = run;
+            m.add(cb);
+            merge = m.ext() <= (double)pack * fmax(run.ext(), cb.ext());
+        }
+        if (merge) {
+            run_cnt += cl.w;
+            run.add(cb);
+        } else {
+            if (run_cnt) groups[atomicAdd(n_groups, 1)] = make_int2(run_first, run_cnt);
+            run_first = cl.z;
+            run_cnt = cl.w;
+            run = cb;
+        }
+    }
+    if (run_cnt) groups[atomicAdd(n_groups, 1)] = make_int2(run_first, run_cnt);
 }
 
-void find_groups(cudaStream_t st, const TreeBufs& t, int n, int2* groups, int* n_groups) {
+void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n, int2* groups,
+                 int* n_groups, double pack) {
     cudaMemsetAsync(n_groups, 0, sizeof(int), st);
-    if (n > 0) k_find_groups<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, groups, n_groups);
+    if (n > 0)
+        k_find_groups<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, sbody, groups, n_groups, pack);
 }
 
 void walk_init(int sms, WalkConfig& cfg) {
@@ -419,7 +483,7 @@ void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, b
                 bool pot) {
     if (a.n <= 0) return;
     a.front_cap = cfg.front_cap;
-    find_groups(st, a.t, a.n, a.groups, a.n_groups);
+    find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack);
     cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
     const dim3 g(cfg.blocks), b(kWalkThreads);
     if (pot) {

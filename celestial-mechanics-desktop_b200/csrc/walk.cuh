@@ -21,6 +21,7 @@ struct WalkArgs {
     int front_cap;
     int2* groups;               // walk groups: body_first, body_count (<= 32)
     int* n_groups;
+    double pack;                // sibling packing box-growth limit (0: no packing)
     unsigned* group_ctr;        // dynamic group counter (zeroed)
     unsigned long long* counters;  // [0] body-cell, [1] body-body interactions
     int* err;
@@ -35,7 +36,8 @@ void walk_init(int sms, WalkConfig& cfg);
 // Walk groups: the octree nodes holding <= 32 bodies whose parent holds
 // more (spatially compact sets of consecutive sorted bodies), plus 32-body
 // slices of level-21 buckets that hold more than 32.  groups: >= n entries.
-void find_groups(cudaStream_t st, const TreeBufs& t, int n, int2* groups, int* n_groups);
+void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n, int2* groups,
+                 int* n_groups, double pack);
 size_t walk_front_bytes(const WalkConfig& cfg);
 // Group walk, FP32 monopole(+quadrupole) on FP64-differenced coordinates.
 void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,

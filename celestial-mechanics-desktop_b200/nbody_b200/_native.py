@@ -45,10 +45,11 @@ PARAM_DENSITY_MERGE = 6
 PARAM_TIMING = 7
 PARAM_MAC_BUDGET = 8
 PARAM_GROUP_BODIES = 9
+PARAM_GROUP_PACK = 10
 # timings / counters
 T_BUILD, T_TRAVERSAL, T_TOTAL, T_SORT, T_TREE, T_COUNT = range(6)
-(C_CELL_INTERACTIONS, C_BODY_INTERACTIONS, C_NODES, C_ACTIVE, C_PAIRS, C_MERGES, C_OVERFLOWS,
- C_COUNT) = range(8)
+(C_CELL_INTERACTIONS, C_BODY_INTERACTIONS, C_NODES, C_ACTIVE, C_PAIRS, C_MERGES, C_OVERFLOWS, C_GROUPS,
+ C_MAX_GROUP_WORK, C_COUNT) = range(10)
 
 vp = C.c_void_p
 i32 = C.c_int32

@@ -75,7 +75,10 @@ enum nb_param {
     NB_PARAM_DENSITY_MERGE = 6,    /* i32, 1 = density-preserving merge radius (default 1)     */
     NB_PARAM_TIMING = 7,           /* i32, 1 = record per-stage CUDA events (default 1)        */
     NB_PARAM_MAC_BUDGET = 8,       /* f64, learned MAC: max predicted log10 rel. error         */
-    NB_PARAM_GROUP_BODIES = 9      /* i32, bodies per walk group: 32 or 64 (default 32)        */
+    NB_PARAM_GROUP_BODIES = 9,     /* i32, bodies per walk group (32)                          */
+    NB_PARAM_GROUP_PACK = 10       /* f64, pack sibling cells into one walk group while the
+                                      packed box is at most this many times the larger part's
+                                      box; 0 = no packing (default 2)                          */
 };
 
 /* Indices into nb_get_timings() output (milliseconds, CUDA events).
@@ -99,7 +102,9 @@ enum nb_counter {
     NB_C_PAIRS = 4,                 /* collision pairs found, last step                     */
     NB_C_MERGES = 5,                /* merges performed, last step                          */
     NB_C_OVERFLOWS = 6,             /* walk frontier overflows (non-zero means an error)    */
-    NB_C_COUNT = 7
+    NB_C_GROUPS = 7,                /* walk groups (warps' body sets), last evaluation       */
+    NB_C_MAX_GROUP_WORK = 8,        /* longest interaction list of one group (load balance)  */
+    NB_C_COUNT = 9
 };
 
 /* ---- lifetime -------------------------------------------------------- */
