@@ -75,6 +75,7 @@ _SIGS = {
     "nb_force_error": (i32, [vp, i32, u64, f64, i32, P]),
     "nb_morton_keys": (i32, [vp, i32, P, P, P, P, i32, P, P, P, P]),
     "nb_sort_pairs": (i32, [vp, i32, P, P]),
+    "nb_sort_pairs_noalloc": (i32, [P, P, i32, vp]),
     "nb_build_octree": (i32, [vp, i32, P, P, P, P, P, P, i32, i32, P, P, P, P, P, P, P, P, P,
                               P, P]),
     "nb_compact_indices": (i32, [vp, i32, P, P, P, P]),

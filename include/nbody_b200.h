@@ -190,6 +190,20 @@ NB_API int32_t nb_morton_keys(nb_engine* h, int32_t n,
 /* Stable sort of (key, value) pairs by key, in place; replaces
  * launch_radix_sort (morton_kernel.cu:185-230) with a stable sort. */
 NB_API int32_t nb_sort_pairs(nb_engine* h, int32_t n, uint64_t* keys, int32_t* values);
+/* Stable sort of (key, value) pairs that live in DEVICE memory, in place,
+ * without allocating any device memory.  No counterpart in the reference:
+ * it serves callers that cannot call cudaMalloc - hosts whose device memory
+ * is all owned by their own pool allocator, and latency-critical paths where
+ * cudaMalloc's device-wide synchronisation is not acceptable.  The scratch is
+ * a fixed 14.7 MB __device__ array inside the library, held by every GPU
+ * that loads it until the process exits; n above NB_NOALLOC_SORT_MAX is
+ * rejected with NB_ERR_CAPACITY.  The first call on a device looks up that
+ * array's address (make it before any stream capture).  All calls share the
+ * one array: calls that overlap on the GPU (other streams, other threads)
+ * race and must be serialised by the caller.  `stream` is a cudaStream_t
+ * (NULL: the legacy default stream); the call returns when the sort is done. */
+#define NB_NOALLOC_SORT_MAX 1048576
+NB_API int32_t nb_sort_pairs_noalloc(uint64_t* keys, int32_t* values, int32_t n, void* stream);
 /* Build the octree of the active bodies in cube4 (NULL: bounding cube) and
  * export it, replacing tree_build_kernel (gpu_tree.cu:269-464) and
  * OctreeBuilder::build (octree_builder.cpp:8-135).  Nodes are in walk order
