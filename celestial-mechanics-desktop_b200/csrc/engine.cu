@@ -59,7 +59,7 @@ struct nb_engine {
     int timing = 1;
     double mac_budget = -3.0;
     int group_bodies = 32;
-    double group_pack = 2.0;
+    double group_pack = 2.25;
     // device-resident state
     int n = 0;
     int n_active = 0;

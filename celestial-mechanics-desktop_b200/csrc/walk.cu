@@ -29,7 +29,7 @@ constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr int kCellCap = 128;
 constexpr int kPartCap = 128;
 // per-warp shared memory, in floats
-constexpr int kWarpFloats = kCellCap * 9 + kPartCap * 4 + kPartCap * 2 + kPartCap;
+constexpr int kWarpFloats = kCellCap * 10 + kPartCap * 4 + kPartCap * 2 + kPartCap;
 constexpr int kWalkSmem = kWalkWarps * kWarpFloats * 4;
 constexpr int kMaxWalkRounds = 1 << 22;
 
@@ -40,15 +40,18 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     s = t;
 }
 
-template <bool QUAD, bool SHELL, bool POT>
-__global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
+// GUARD (softening 0 only): 1/r is taken as 0 at r = 0, so a body's own entry
+// in its particle list adds 0 instead of 0 * inf.  With softening > 0 the
+// own entry has r^2 = eps^2 and dx = dy = dz = 0, which adds exactly 0.
+template <bool QUAD, bool SHELL, bool POT, bool GUARD>
+__global__ void __launch_bounds__(kWalkThreads, 3) k_walk_group(WalkArgs a) {
     extern __shared__ __align__(16) float s_walk[];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* base = s_walk + warp * kWarpFloats;
     float4* c0 = (float4*)base;                      // rel com xyz, mass
-    float4* c1 = c0 + kCellCap;                      // Qxx, Qyy, Qxy, Qxz
-    float* c2 = (float*)(c1 + kCellCap);             // Qyz
+    float4* c1 = c0 + kCellCap;                      // Qxx, Qyy, Qzz, Qxy
+    float2* c2 = (float2*)(c1 + kCellCap);           // Qxz, Qyz
     float4* p0 = (float4*)(c2 + kCellCap);           // rel xyz, mass
     float2* p1 = (float2*)(p0 + kPartCap);           // R^2, m / (R^2 + eps^2)^1.5
     int* p2 = (int*)(p1 + kPartCap);                 // sorted index
@@ -64,10 +67,16 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
         g = __shfl_sync(FULL, g, 0);
         if (g >= ngroups) break;
         const int2 grp = a.groups[g];  // body_first, body_count (<= 32)
-        const int s = grp.x + lane;
-        const bool valid = lane < grp.y;
-        const double4 b = a.sbody[valid ? s : grp.x];
         const int nvalid = grp.y;
+        // A group of nvalid <= 16 bodies is replicated over the warp: lane
+        // (rep, slot) holds body `slot` and evaluates every nrep-th list entry
+        // starting at `rep`; the replicas' sums are combined at the end.
+        const int lw = (nvalid <= 1) ? 0 : 32 - __clz(nvalid - 1);  // log2(width)
+        const int slot = lane & ((1 << lw) - 1);
+        const int rep = lane >> lw, nrep = 32 >> lw;
+        const int s = grp.x + slot;
+        const bool valid = slot < nvalid;
+        const double4 b = a.sbody[valid ? s : grp.x];
         const double mnx = warp_min(b.x), mny = warp_min(b.y), mnz = warp_min(b.z);
         const double mxx = warp_max(b.x), mxy = warp_max(b.y), mxz = warp_max(b.z);
         const double gcx = 0.5 * (mnx + mxx), gcy = 0.5 * (mny + mxy), gcz = 0.5 * (mnz + mxz);
@@ -85,7 +94,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
         auto flush_cells = [&]() {
             float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
 #pragma unroll 4
-            for (int j = 0; j < nc; j++) {
+            for (int j = rep; j < nc; j += nrep) {
                 const float4 A = c0[j];
                 const float dx = bx - A.x, dy = by - A.y, dz = bz - A.z;
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
@@ -93,12 +102,11 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
                 const float inv2 = inv * inv;
                 const float inv3 = inv * inv2;
                 if (QUAD) {
-                    const float4 B = c1[j];
-                    const float C = c2[j];
-                    const float qzz = -(B.x + B.y);
-                    const float qx = fmaf(B.x, dx, fmaf(B.z, dy, B.w * dz));
-                    const float qy = fmaf(B.z, dx, fmaf(B.y, dy, C * dz));
-                    const float qz = fmaf(B.w, dx, fmaf(C, dy, qzz * dz));
+                    const float4 B = c1[j];  // Qxx, Qyy, Qzz, Qxy
+                    const float2 C = c2[j];  // Qxz, Qyz
+                    const float qx = fmaf(B.x, dx, fmaf(B.w, dy, C.x * dz));
+                    const float qy = fmaf(B.w, dx, fmaf(B.y, dy, C.y * dz));
+                    const float qz = fmaf(C.x, dx, fmaf(C.y, dy, B.z * dz));
                     const float rqr = fmaf(dx, qx, fmaf(dy, qy, dz * qz));
                     const float inv5 = inv3 * inv2;
                     // a = -M r / r^3 + Q r / r^5 - (5/2) (r.Q.r) r / r^7
@@ -127,12 +135,12 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
         auto flush_parts = [&]() {
             float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
 #pragma unroll 4
-            for (int j = 0; j < np; j++) {
+            for (int j = rep; j < np; j += nrep) {
                 const float4 P = p0[j];
                 const float dx = bx - P.x, dy = by - P.y, dz = bz - P.z;
                 const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 const float r2 = raw + eps2;
-                const float inv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+                const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrtf(r2);
                 float f = P.w * (inv * inv * inv);
                 if (SHELL) {
                     const float2 S = p1[j];
@@ -201,11 +209,12 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
                     const int k = __popc(mcell);
                     if (nc + k > kCellCap) flush_cells();
                     if (take_cell) {
-                        const int slot = nc + __popc(mcell & lanemask_lt());
-                        c0[slot] = make_float4(rx, ry, rz, mass);
+                        const int cs = nc + __popc(mcell & lanemask_lt());
+                        c0[cs] = make_float4(rx, ry, rz, mass);
                         if (QUAD) {
-                            c1[slot] = a.t.q0[node];
-                            c2[slot] = a.t.q1[node].x;
+                            const float4 q = a.t.q0[node];  // Qxx, Qyy, Qxy, Qxz
+                            c1[cs] = make_float4(q.x, q.y, -(q.x + q.y), q.z);
+                            c2[cs] = make_float2(q.w, a.t.q1[node].x);
                         }
                     }
                     nc += k;
@@ -261,12 +270,21 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_walk_group(WalkArgs a) {
         if (nc) flush_cells();
         if (np) flush_parts();
         if (lane == 0 && a.counters) atomicMax(&a.counters[2], grp_entries);
-        if (valid) {
+        // combine the replicas of each body (lanes equal modulo the width)
+        double fx = (double)sax - (double)cax, fy = (double)say - (double)cay;
+        double fz = (double)saz - (double)caz, fp = (double)spot - (double)cpot;
+        for (int o = 1 << lw; o < 32; o <<= 1) {
+            fx += __shfl_xor_sync(FULL, fx, o);
+            fy += __shfl_xor_sync(FULL, fy, o);
+            fz += __shfl_xor_sync(FULL, fz, o);
+            if (POT) fp += __shfl_xor_sync(FULL, fp, o);
+        }
+        if (valid && rep == 0) {
             const uint32_t row = a.sidx[s];
-            a.ax[row] = (double)sax - (double)cax;
-            a.ay[row] = (double)say - (double)cay;
-            a.az[row] = (double)saz - (double)caz;
-            if (POT) a.pot[row] = (double)spot - (double)cpot;
+            a.ax[row] = fx;
+            a.ay[row] = fy;
+            a.az[row] = fz;
+            if (POT) a.pot[row] = fp;
         }
     }
     if (lane == 0 && a.counters) {
@@ -394,7 +412,9 @@ struct Box {
 
 // Sibling runs are packed only while the packed box stays within `pack`
 // times the larger part's box: siblings that sit far apart in a sparse cell
-// would make one group whose opening test walks most of the tree.
+// would make one group whose opening test walks most of the tree.  (Measured
+// at N=1M: factor 2-2.5 raises lane fill from 0.30 to 0.57-0.71; from 3 on,
+// a few groups reach into the dense core and serialise ~1e6 list entries.)
 __global__ void k_find_groups(TreeBufs t, const double4* __restrict__ sbody,
                               int2* __restrict__ groups, int* __restrict__ n_groups, double pack) {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -432,7 +452,7 @@ __global__ void k_find_groups(TreeBufs t, const double4* __restrict__ sbody,
         if (pack > 0.0 && run_cnt > 0 && run_cnt + cl.w <= 32) {
             Box m = run;
             m.add(cb);
-            merge = m.ext() <= (double)pack * fmax(run.ext(), cb.ext());
+            merge = m.ext() <= pack * fmax(run.ext(), cb.ext());
         }
         if (merge) {
             run_cnt += cl.w;
@@ -454,21 +474,33 @@ void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n
         k_find_groups<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, sbody, groups, n_groups, pack);
 }
 
+using WalkKernel = void (*)(WalkArgs);
+
+// The instantiated variants: (quad) x {plain, shell, potential} x (guard).
+static WalkKernel pick_walk(bool quad, bool shell, bool pot, bool guard) {
+#define NB_WALK_PICK(Q, S, P)                                            \
+    return guard ? k_walk_group<Q, S, P, true> : k_walk_group<Q, S, P, false>
+    if (pot) {
+        if (quad) NB_WALK_PICK(true, false, true);
+        NB_WALK_PICK(false, false, true);
+    }
+    if (shell) {
+        if (quad) NB_WALK_PICK(true, true, false);
+        NB_WALK_PICK(false, true, false);
+    }
+    if (quad) NB_WALK_PICK(true, false, false);
+    NB_WALK_PICK(false, false, false);
+#undef NB_WALK_PICK
+}
+
 void walk_init(int sms, WalkConfig& cfg) {
-    cudaFuncSetAttribute((const void*)k_walk_group<true, false, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
-    cudaFuncSetAttribute((const void*)k_walk_group<false, false, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
-    cudaFuncSetAttribute((const void*)k_walk_group<true, true, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
-    cudaFuncSetAttribute((const void*)k_walk_group<false, true, false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
-    cudaFuncSetAttribute((const void*)k_walk_group<true, false, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
-    cudaFuncSetAttribute((const void*)k_walk_group<false, false, true>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    for (int v = 0; v < 16; v++) {
+        const bool pot = v & 4, shell = (v & 2) && !pot;
+        cudaFuncSetAttribute((const void*)pick_walk(v & 1, shell, pot, v & 8),
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_group<true, false, false>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_group<true, false, false, false>,
                                                   kWalkThreads, kWalkSmem);
     if (per_sm < 1) per_sm = 1;
     cfg.blocks = sms * per_sm;
@@ -485,17 +517,8 @@ void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, b
     a.front_cap = cfg.front_cap;
     find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack);
     cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
-    const dim3 g(cfg.blocks), b(kWalkThreads);
-    if (pot) {
-        if (quad) k_walk_group<true, false, true><<<g, b, kWalkSmem, st>>>(a);
-        else k_walk_group<false, false, true><<<g, b, kWalkSmem, st>>>(a);
-    } else if (shell) {
-        if (quad) k_walk_group<true, true, false><<<g, b, kWalkSmem, st>>>(a);
-        else k_walk_group<false, true, false><<<g, b, kWalkSmem, st>>>(a);
-    } else {
-        if (quad) k_walk_group<true, false, false><<<g, b, kWalkSmem, st>>>(a);
-        else k_walk_group<false, false, false><<<g, b, kWalkSmem, st>>>(a);
-    }
+    const WalkKernel k = pick_walk(quad, shell, pot, !(a.eps2 > 0.0));
+    k<<<cfg.blocks, kWalkThreads, kWalkSmem, st>>>(a);
 }
 
 void walk_reference(cudaStream_t st, WalkArgs a, bool shell) {

@@ -78,7 +78,7 @@ enum nb_param {
     NB_PARAM_GROUP_BODIES = 9,     /* i32, bodies per walk group (32)                          */
     NB_PARAM_GROUP_PACK = 10       /* f64, pack sibling cells into one walk group while the
                                       packed box is at most this many times the larger part's
-                                      box; 0 = no packing (default 2)                          */
+                                      box; 0 = no packing (default 2.25)                       */
 };
 
 /* Indices into nb_get_timings() output (milliseconds, CUDA events).
