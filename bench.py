@@ -36,6 +36,14 @@ THETA, EPS, DT, SEED = 0.5, 1e-4, 1e-4, 1
 # FP32 flops per interaction, counted from the walk's own arithmetic
 # (FMA = 2, add/mul/rsqrt = 1): body-body 20, body-cell monopole+quadrupole 51.
 FLOPS_BODY, FLOPS_CELL_QUAD = 20, 51
+# Algorithmic bytes per body of the integer stages (each array read or
+# written once): sort stage = kick-drift+bbox 129 (read pos/vel/acc/mass/
+# active, write pos/vel) + zero acc 24 + keys 37 (read pos+active, write
+# key+row) + 8 radix passes x 24 (read and write key+row) + gather 68 (read
+# row, pos, mass; write double4) = 450; tree stage = radix tree 29 (read key,
+# write children/range/prefix/parent) + mark 35 + scan/base 8 + emit 40 +
+# multipoles 32 + 0.45 nodes/body x 100 = 189.
+SORT_BYTES_PER_BODY, TREE_BYTES_PER_BODY = 450, 189
 
 
 def workload_name(n: int) -> str:
@@ -138,7 +146,7 @@ def peaks():
 
 def walk_traffic_per_launch():
     """DRAM bytes of one walk launch from the committed ncu summary, or None."""
-    f = ROOT / "profiles" / "walk_bh_plummer_1m.md"
+    f = ROOT / "profiles" / "k_walk_group_bh_plummer.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -220,13 +228,15 @@ def run_b200(args, ws, rank, local):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
-    walk_ms, build_ms, inter, flops = 0.0, 0.0, 0, 0.0
+    walk_ms, build_ms, sort_ms, tree_ms, inter, flops = 0.0, 0.0, 0.0, 0.0, 0, 0.0
     for _ in range(args.steps):
         eng.step(1, DT, EPS, flags)
         tm = eng.timings()
         c = eng.counters()
         walk_ms += tm[N.T_TRAVERSAL]
         build_ms += tm[N.T_BUILD]
+        sort_ms += tm[N.T_SORT]
+        tree_ms += tm[N.T_TREE]
         inter += int(c[N.C_CELL_INTERACTIONS] + c[N.C_BODY_INTERACTIONS])
         flops += FLOPS_CELL_QUAD * c[N.C_CELL_INTERACTIONS] + FLOPS_BODY * c[N.C_BODY_INTERACTIONS]
     t1.record(stream)
@@ -291,7 +301,16 @@ def run_b200(args, ws, rank, local):
             "interactions_per_step": inter / args.steps,
             "force_error": {"mean": err[0], "max": err[1], "rms": err[2],
                             "vs": "FP64 direct sum, 4096 uniformly sampled bodies"},
-            "stage_ms": {"build": build_ms / args.steps, "walk": walk_ms / args.steps},
+            "stage_ms": {"build": build_ms / args.steps, "walk": walk_ms / args.steps,
+                         "sort": sort_ms / args.steps, "tree": tree_ms / args.steps},
+            "stage_gbs": {
+                "sort": SORT_BYTES_PER_BODY * args.n / (sort_ms / args.steps / 1e3) / 1e9,
+                "tree": TREE_BYTES_PER_BODY * args.n / (tree_ms / args.steps / 1e3) / 1e9,
+                "hbm_peak": pk.get("hbm_gbs", 6458.1),
+                "bytes_per_body": {"sort": SORT_BYTES_PER_BODY, "tree": TREE_BYTES_PER_BODY},
+                "note": "sort = kick-drift+bbox, keys+histograms, 8 radix passes, gather; "
+                        "tree = radix tree, octree mark/scan/emit, multipoles; at N=2^20 the "
+                        "sort buffers (24 MB) stay in the 126 MB L2"},
             "gpu_launches": None,
             "roofline": {"bound": "fp32", "kernel": "k_walk_group", "achieved": achieved,
                          "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
