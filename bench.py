@@ -44,6 +44,7 @@ FLOPS_BODY, FLOPS_CELL_QUAD = 20, 51
 # write children/range/prefix/parent) + mark 35 + scan/base 8 + emit 40 +
 # multipoles 32 + 0.45 nodes/body x 100 = 189.
 SORT_BYTES_PER_BODY, TREE_BYTES_PER_BODY = 450, 189
+DISK_RADIUS_SCALE = 30.0
 
 
 def workload_name(n: int) -> str:
@@ -333,8 +334,129 @@ def run_b200(args, ws, rank, local):
 def launches_per_step() -> int:
     """Kernels of one device step: kick-drift-bbox, cube, keys, 8 sort passes,
     gather, zero-acc, radix tree, octree mark, block scan, octree base,
-    octree emit, multipoles, walk, kick."""
-    return 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1
+    octree emit, multipoles, walk groups, walk, kick."""
+    return 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1 + 1
+
+
+def _timed_steps(eng, stream, steps, dt, eps, flags, dev, ws):
+    """K device steps bracketed by a barrier, synchronise and CUDA events
+    on the engine's stream; returns (ms over ranks' max, clocks)."""
+    import torch
+
+    clocks = Clocks(dev)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    eng.step(steps, dt, eps, flags)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    clk = clocks.stop()
+    return max_over_ranks(ws, t0.elapsed_time(t1)), clk
+
+
+def run_ds1000(args, ws, rank, local):
+    """FP64 direct sum + velocity Verlet: N=1000 Plummer (scale 1 AU, 1 Msun,
+    seed 0), eps 1e-4, dt 1e-3, 10,000 steps; energy drift against the CPU
+    restatement of CpuParallelBackend + SoAVerletIntegrator run on the same
+    input (its trajectory is bit-identical)."""
+    import torch
+
+    import oracle
+    from nbody_b200 import MODE_DIRECT_FP64, Engine, scenarios
+
+    dev = local
+    torch.cuda.set_device(dev)
+    n, eps, dt, steps = 1000, 1e-4, 1e-3, args.steps if args.steps != 20 else 10_000
+    b = scenarios.plummer(n, 1.0, 1.0, seed=0)
+    eng = Engine(n, device=dev)
+    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
+    eng.set_state(b, old_acc=False)
+    eng.step(max(args.warmup, 3), dt, eps, MODE_DIRECT_FP64)  # warm-up on a copy of the state
+    eng.set_state(b, old_acc=False)
+    e0 = eng.diagnostics(eps)["e"]
+    ms, clk = _timed_steps(eng, stream, steps, dt, eps, MODE_DIRECT_FP64, dev, ws)
+    e1 = eng.diagnostics(eps)["e"]
+    drift = (e1 - e0) / abs(e0)
+    line = None
+    if rank == 0:
+        d = {k: getattr(b, k) for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az",
+                                         "mass", "active")}
+        threads = os.cpu_count() or 1
+        t = time.perf_counter()
+        cpu_steps = steps if not args.no_cpu_baseline else 0
+        w = oracle.verlet_direct(d, eps, dt, cpu_steps, nthreads=threads) if cpu_steps else None
+        cpu_s = time.perf_counter() - t
+        cpu_drift = None
+        if w is not None:
+            w["active"] = b.active
+            cpu_drift = (oracle.energy(w, eps)["e"] - oracle.energy(d, eps)["e"]) / abs(e0)
+        line = {"metric": METRIC, "value": steps / (ms / 1e3), "unit": "steps/s", "n_gpus": ws,
+                "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Plummer sphere)",
+                "config": {"workload": "ds_plummer_1000", "n": n, "eps": eps, "dt": dt,
+                           "seed": 0, "force": "direct sum FP64, CpuParallelBackend rounding"},
+                "energy_drift": drift, "cpu_energy_drift": cpu_drift,
+                "pairs_per_s": n * (n - 1) * steps / (ms / 1e3),
+                "cpu_baseline": None if w is None else {
+                    "value": steps / cpu_s, "unit": "steps/s", "cores": threads, "kind": "port",
+                    "sample": f"the same {steps} steps with the CpuParallelBackend restatement "
+                              "(OpenMP over targets)"},
+                "clocks": clk, "gpu_launches": 5 * steps}
+    eng.close()
+    return line
+
+
+def run_disk(args, ws, rank, local):
+    """Collisional disk: 262,144 bodies + a 1 Msun central body, Barnes-Hut
+    theta 0.5 with shell-theorem leaves, merges (64/frame, 2/body) and
+    compaction every step, eps 1e-4, dt 1e-3."""
+    import torch
+
+    from nbody_b200 import (FLAG_COLLISIONS, FLAG_SHELL_THEOREM, MODE_BARNES_HUT, Engine,
+                            scenarios)
+    from nbody_b200 import _native as N
+
+    dev = local
+    torch.cuda.set_device(dev)
+    n, eps, dt = 262_144, 1e-4, 1e-3
+    steps = args.steps if args.steps != 20 else 1000
+    # radius scale 30: calibrated so ~1 % of the bodies merge per 1000 steps
+    # (a scale of 1000 makes every body overlap ~3 others at the start)
+    d = scenarios.collisional_disk(n, seed=2, radius_scale=DISK_RADIUS_SCALE)
+    eng = Engine(n + 1, device=dev)
+    eng.set_param(N.PARAM_THETA, THETA)
+    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
+    flags = MODE_BARNES_HUT | FLAG_SHELL_THEOREM | FLAG_COLLISIONS
+    eng.set_state(d, old_acc=False)
+    eng.step(max(args.warmup, 3), dt, eps, flags)
+    eng.set_state(d, old_acc=False)
+    p0 = eng.diagnostics(eps, pe_mode=1)
+    ms, clk = _timed_steps(eng, stream, steps, dt, eps, flags, dev, ws)
+    p1 = eng.diagnostics(eps, pe_mode=1)
+    st, ids = eng.get_state()
+    line = None
+    if rank == 0:
+        dp = np.sqrt(sum((p1[k] - p0[k]) ** 2 for k in ("px", "py", "pz")))
+        pn = np.sqrt(sum(p0[k] ** 2 for k in ("px", "py", "pz")))
+        line = {"metric": METRIC, "value": steps / (ms / 1e3), "unit": "steps/s", "n_gpus": ws,
+                "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded Keplerian disk)",
+                "config": {"workload": "disk_262k", "n": n + 1, "eps": eps, "dt": dt, "seed": 2,
+                           "theta": THETA, "radius_scale": DISK_RADIUS_SCALE,
+                           "collisions": "broad phase + merge + compaction every step"},
+                "bodies_left": int(len(ids)), "merged": int(n + 1 - len(ids)),
+                "merges_per_1000_steps_frac": (n + 1 - len(ids)) / (n + 1) * 1000.0 / steps,
+                "energy_drift": (p1["e"] - p0["e"]) / abs(p0["e"]),
+                "momentum_drift_abs": dp, "momentum_scale": pn,
+                "mass_drift": (p1["m"] - p0["m"]) / p0["m"], "clocks": clk}
+    eng.close()
+    return line
 
 
 def main():
@@ -346,11 +468,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=N_BODIES,
                     help="bodies (default the 1,048,576-body workload; smaller for profiling)")
+    ap.add_argument("--workload", default="bh1m", choices=["bh1m", "ds1000", "disk"],
+                    help="bh1m: the headline Barnes-Hut line; ds1000: FP64 direct sum N=1000, "
+                         "10k steps; disk: collisional disk N=262,145, 1000 steps")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank)
+        elif args.workload == "ds1000":
+            line = run_ds1000(args, ws, rank, local)
+            if line is not None:
+                print(json.dumps(line))
+        elif args.workload == "disk":
+            line = run_disk(args, ws, rank, local)
+            if line is not None:
+                print(json.dumps(line))
         else:
             line = run_b200(args, ws, rank, local)
             if line is not None:

@@ -1,11 +1,11 @@
 // direct.cu - softened O(n^2) direct sums.
 //
-// k_direct_fp64 restates CpuParallelBackend.ComputeForces
+// k_direct_fp64_pairs restates CpuParallelBackend.ComputeForces
 // (src/CelestialMechanics.Physics/Solvers/CpuParallelBackend.cs:99-142) with
-// GravityKernel.AccelerationCoeffFromSource (GravityKernel.cs:9-33): one
-// thread per target row, sources in row order through shared-memory tiles,
-// every FP64 operation rounded exactly as the C# code rounds it (no FMA
-// contraction), so its output is bit-identical to that backend's.  It also
+// GravityKernel.AccelerationCoeffFromSource (GravityKernel.cs:9-33): every
+// FP64 operation rounded exactly as the C# code rounds it (no FMA
+// contraction) and every target's terms summed in source-row order, so its
+// output is bit-identical to that backend's.  It also
 // replaces the reference GPU gravity_kernel (engine/src/cuda/gravity_kernel.cu:
 // 20-95), which loads inactive sources with their real mass.
 //
@@ -17,64 +17,6 @@
 #include "direct.cuh"
 
 namespace nb {
-
-constexpr int kD64Threads = 128;
-
-template <bool SHELL>
-__global__ void __launch_bounds__(kD64Threads)
-k_direct_fp64(int n, const double* __restrict__ px, const double* __restrict__ py,
-              const double* __restrict__ pz, const double* __restrict__ m,
-              const double* __restrict__ rad, const uint8_t* __restrict__ act, double eps2,
-              double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az) {
-    __shared__ double4 sj[kD64Threads];
-    __shared__ double sr[kD64Threads];
-    __shared__ uint8_t sa[kD64Threads];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool me = i < n && act[i];
-    const double xi = me ? px[i] : 0.0, yi = me ? py[i] : 0.0, zi = me ? pz[i] : 0.0;
-    double axi = 0.0, ayi = 0.0, azi = 0.0;
-    for (int base = 0; base < n; base += kD64Threads) {
-        const int j = base + threadIdx.x;
-        sj[threadIdx.x] = (j < n) ? make_double4(px[j], py[j], pz[j], m[j]) : make_double4(0, 0, 0, 0);
-        sa[threadIdx.x] = (j < n) ? act[j] : 0;
-        if (SHELL) sr[threadIdx.x] = (j < n && rad) ? rad[j] : 0.0;
-        __syncthreads();
-        const int cnt = min(kD64Threads, n - base);
-        if (me) {
-            for (int k = 0; k < cnt; k++) {
-                const double4 q = sj[k];
-                if (base + k == i || !sa[k]) continue;
-                const double dx = __dsub_rn(xi, q.x);
-                const double dy = __dsub_rn(yi, q.y);
-                const double dz = __dsub_rn(zi, q.z);
-                const double raw = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
-                                             __dmul_rn(dz, dz));
-                double c;
-                const double R = SHELL ? sr[k] : 0.0;
-                if (!SHELL || R <= 0.0) {
-                    const double inv = 1.0 / sqrt(__dadd_rn(raw, eps2));
-                    c = __dmul_rn(__dmul_rn(__dmul_rn(q.w, inv), inv), inv);
-                } else if (sqrt(raw) < R) {
-                    const double den = __dadd_rn(__dmul_rn(R, R), eps2);
-                    const double ids = 1.0 / sqrt(den);
-                    c = __dmul_rn(q.w, ids) / den;
-                } else {
-                    const double inv = 1.0 / sqrt(__dadd_rn(raw, eps2));
-                    c = __dmul_rn(__dmul_rn(__dmul_rn(q.w, inv), inv), inv);
-                }
-                axi = __dsub_rn(axi, __dmul_rn(c, dx));
-                ayi = __dsub_rn(ayi, __dmul_rn(c, dy));
-                azi = __dsub_rn(azi, __dmul_rn(c, dz));
-            }
-        }
-        __syncthreads();
-    }
-    if (i < n) {
-        ax[i] = axi;
-        ay[i] = ayi;
-        az[i] = azi;
-    }
-}
 
 constexpr int kD32Threads = 256;
 constexpr int kD32Per = 2;  // targets per thread
@@ -174,14 +116,99 @@ k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict_
     }
 }
 
+// The arithmetic is split in two phases so that the costly per-pair part
+// (sqrt, division) runs on every thread of the block: for a tile of kPTj
+// sources, 256 threads compute the kPTi x kPTj pair terms c*dx, c*dy, c*dz
+// (each rounded exactly as above) into shared memory; then 3 x kPTi threads
+// subtract them in source order, one (target, component) chain per thread.
+// The sequence of roundings of every target's sum is unchanged, so the
+// result is bit-identical to CpuParallelBackend's.
+constexpr int kPTi = 8;     // targets per block
+constexpr int kPTj = 128;   // sources per tile
+constexpr int kPThreads = 256;
+
+template <bool SHELL>
+__global__ void __launch_bounds__(kPThreads)
+k_direct_fp64_pairs(int n, const double* __restrict__ px, const double* __restrict__ py,
+                    const double* __restrict__ pz, const double* __restrict__ m,
+                    const double* __restrict__ rad, const uint8_t* __restrict__ act,
+                    double eps2, double* __restrict__ ax, double* __restrict__ ay,
+                    double* __restrict__ az) {
+    __shared__ double s_t[3][kPTi][kPTj + 1];  // pair terms (padded against bank conflicts)
+    __shared__ uint8_t s_ok[kPTi][kPTj];        // term is added (active source, not self)
+    __shared__ double s_i[kPTi][3];
+    __shared__ uint8_t s_iact[kPTi];
+    const int i0 = blockIdx.x * kPTi;
+    if (threadIdx.x < kPTi) {
+        const int i = i0 + threadIdx.x;
+        const bool me = i < n && act[i];
+        s_iact[threadIdx.x] = me;
+        s_i[threadIdx.x][0] = me ? px[i] : 0.0;
+        s_i[threadIdx.x][1] = me ? py[i] : 0.0;
+        s_i[threadIdx.x][2] = me ? pz[i] : 0.0;
+    }
+    __syncthreads();
+    // accumulator thread: (target, component)
+    const int acc_t = threadIdx.x / 3, acc_c = threadIdx.x % 3;
+    const bool accum = threadIdx.x < 3 * kPTi;
+    double sum = 0.0;
+    for (int base = 0; base < n; base += kPTj) {
+        for (int p = threadIdx.x; p < kPTi * kPTj; p += kPThreads) {
+            const int ti = p / kPTj, tj = p % kPTj;
+            const int i = i0 + ti, j = base + tj;
+            bool ok = j < n && s_iact[ti] && j != i && act[j];
+            double tx = 0.0, ty = 0.0, tz = 0.0;
+            if (ok) {
+                const double dx = __dsub_rn(s_i[ti][0], px[j]);
+                const double dy = __dsub_rn(s_i[ti][1], py[j]);
+                const double dz = __dsub_rn(s_i[ti][2], pz[j]);
+                const double raw = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                             __dmul_rn(dz, dz));
+                const double mj = m[j];
+                double c;
+                const double R = SHELL ? rad[j] : 0.0;
+                if (!SHELL || R <= 0.0) {
+                    const double inv = 1.0 / sqrt(__dadd_rn(raw, eps2));
+                    c = __dmul_rn(__dmul_rn(__dmul_rn(mj, inv), inv), inv);
+                } else if (sqrt(raw) < R) {
+                    const double den = __dadd_rn(__dmul_rn(R, R), eps2);
+                    const double ids = 1.0 / sqrt(den);
+                    c = __dmul_rn(mj, ids) / den;
+                } else {
+                    const double inv = 1.0 / sqrt(__dadd_rn(raw, eps2));
+                    c = __dmul_rn(__dmul_rn(__dmul_rn(mj, inv), inv), inv);
+                }
+                tx = __dmul_rn(c, dx);
+                ty = __dmul_rn(c, dy);
+                tz = __dmul_rn(c, dz);
+            }
+            s_t[0][ti][tj] = tx;
+            s_t[1][ti][tj] = ty;
+            s_t[2][ti][tj] = tz;
+            s_ok[ti][tj] = ok;
+        }
+        __syncthreads();
+        if (accum) {
+            const int cnt = min(kPTj, n - base);
+            for (int tj = 0; tj < cnt; tj++)
+                if (s_ok[acc_t][tj]) sum = __dsub_rn(sum, s_t[acc_c][acc_t][tj]);
+        }
+        __syncthreads();
+    }
+    if (accum) {
+        const int i = i0 + acc_t;
+        if (i < n) (acc_c == 0 ? ax : acc_c == 1 ? ay : az)[i] = sum;
+    }
+}
+
 void direct_fp64(cudaStream_t st, int n, const double* px, const double* py, const double* pz,
                  const double* m, const double* rad, const uint8_t* act, double eps, bool shell,
                  double* ax, double* ay, double* az) {
     if (n <= 0) return;
     const double eps2 = eps * eps;
-    const int g = ceil_div(n, kD64Threads);
-    if (shell) k_direct_fp64<true><<<g, kD64Threads, 0, st>>>(n, px, py, pz, m, rad, act, eps2, ax, ay, az);
-    else k_direct_fp64<false><<<g, kD64Threads, 0, st>>>(n, px, py, pz, m, rad, act, eps2, ax, ay, az);
+    const int g = ceil_div(n, kPTi);
+    if (shell) k_direct_fp64_pairs<true><<<g, kPThreads, 0, st>>>(n, px, py, pz, m, rad, act, eps2, ax, ay, az);
+    else k_direct_fp64_pairs<false><<<g, kPThreads, 0, st>>>(n, px, py, pz, m, rad, act, eps2, ax, ay, az);
 }
 
 void direct_fp32(cudaStream_t st, int n, const double4* sbody, const float* srad,

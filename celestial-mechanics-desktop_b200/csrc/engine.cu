@@ -87,6 +87,18 @@ struct nb_engine {
     std::vector<void*> allocs;
     // timing
     cudaEvent_t ev[6] = {};
+    // captured single step (CUDA graph) and the parameters it was captured with
+    cudaGraphExec_t graph_exec = nullptr;
+    struct GraphKey {
+        int flags, n, n_active, leaf_cap;
+        double dt, eps, theta, pack;
+        const double* state;  // the state arrays swap after a compaction
+        bool operator==(const GraphKey& o) const {
+            return flags == o.flags && n == o.n && n_active == o.n_active &&
+                   leaf_cap == o.leaf_cap && dt == o.dt && eps == o.eps && theta == o.theta &&
+                   pack == o.pack && state == o.state;
+        }
+    } graph_key{};
     bool ev_valid = false;
     bool ev_tree = false;
     double timings[NB_T_COUNT] = {0};
@@ -251,6 +263,41 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     return NB_OK;
 }
 
+// Capture one device step (forces + second half kick) as a CUDA graph, or
+// reuse the captured one when nothing it depends on changed.  Per-stage
+// timing events are not recorded inside the graph.
+int step_graph(nb_engine* h, int flags, double dt, double eps) {
+    const nb_engine::GraphKey key{flags, h->n, h->n_active, h->leaf_cap, dt,
+                                  eps, h->theta, h->group_pack, h->s.px};
+    if (h->graph_exec && key == h->graph_key) return NB_OK;
+    if (h->graph_exec) {
+        cudaGraphExecDestroy(h->graph_exec);
+        h->graph_exec = nullptr;
+    }
+    NB_CUDA(h, cudaStreamSynchronize(h->st));
+    const int timing = h->timing;
+    h->timing = 0;
+    cudaGraph_t g = nullptr;
+    NB_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int r = force_pipeline(h, flags, eps, true, dt);
+    if (r == NB_OK) nb::launch_kick(h->st, h->n, h->s, dt);
+    const cudaError_t e = cudaStreamEndCapture(h->st, &g);
+    h->timing = timing;
+    if (r != NB_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(h, NB_ERR_CUDA, "step capture: %s", cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&h->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        h->graph_exec = nullptr;
+        return fail(h, NB_ERR_CUDA, "step graph: %s", cudaGetErrorString(ei));
+    }
+    h->graph_key = key;
+    return NB_OK;
+}
+
 void collect_counters(nb_engine* h) {
     unsigned long long c[4];
     if (cudaMemcpy(c, h->scal->counters, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) {
@@ -368,6 +415,7 @@ NB_API int32_t nb_destroy(nb_engine* h) {
     for (void* p : h->allocs) cudaFree(p);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
     return NB_OK;
@@ -534,6 +582,16 @@ NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softenin
     cudaSetDevice(h->device);
     const bool collide = (flags & NB_FLAG_COLLISIONS) != 0;
     int r;
+    if (!collide && n_steps > 1) {
+        // Multi-step calls replay one captured step (a CUDA graph) n times;
+        // the row and active counts do not change without collisions.
+        if ((r = step_graph(h, flags, dt, softening))) return r;
+        for (int k = 0; k < n_steps; k++)
+            NB_CUDA(h, cudaGraphLaunch(h->graph_exec, h->st));
+        if ((r = check_device(h))) return r;
+        collect_counters(h);
+        return NB_OK;
+    }
     for (int k = 0; k < n_steps; k++) {
         if ((r = force_pipeline(h, flags, softening, true, dt))) return r;
         nb::launch_kick(h->st, h->n, h->s, dt);
