@@ -176,12 +176,17 @@ __global__ void k_keys_aabb(int n, State s, const unsigned long long* __restrict
 }
 
 __global__ void k_gather(int n, State s, const uint32_t* __restrict__ sidx,
-                         double4* __restrict__ sbody, float* __restrict__ srad) {
+                         double4* __restrict__ sbody, float* __restrict__ srad,
+                         float* __restrict__ samag) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t i = sidx[k];
     sbody[k] = make_double4(s.px[i], s.py[i], s.pz[i], s.mass[i]);
     if (srad) srad[k] = s.radius ? (float)s.radius[i] : 0.f;
+    if (samag) {  // |a| of the previous step (acceleration buffer before it is overwritten)
+        const double ax = s.ax[i], ay = s.ay[i], az = s.az[i];
+        samag[k] = (float)sqrt(ax * ax + ay * ay + az * az);
+    }
 }
 
 __global__ void k_zero_acc(int n, State s) {
@@ -223,8 +228,8 @@ void launch_keys_aabb(cudaStream_t st, int n, const State& s,
 }
 
 void launch_gather(cudaStream_t st, int n, const State& s, const uint32_t* sidx,
-                   double4* sbody, float* srad) {
-    if (n > 0) k_gather<<<ceil_div(n, 256), 256, 0, st>>>(n, s, sidx, sbody, srad);
+                   double4* sbody, float* srad, float* samag) {
+    if (n > 0) k_gather<<<ceil_div(n, 256), 256, 0, st>>>(n, s, sidx, sbody, srad, samag);
 }
 
 void launch_zero_acc(cudaStream_t st, int n, State s) {

@@ -30,9 +30,10 @@ void launch_keys_cube(cudaStream_t st, int n, const State& s, const double* cube
 // Reference keys: per-axis AABB, scale 2^21-1 (morton_kernel.cu:11-76).
 void launch_keys_aabb(cudaStream_t st, int n, const State& s,
                       const unsigned long long* bbox_ord, uint64_t* keys, uint32_t* vals);
-// Gather the first n sorted rows: sbody = (x, y, z, m), srad = radius.
+// Gather the first n sorted rows: sbody = (x, y, z, m), srad = radius,
+// samag = |acc| (optional; the previous step's acceleration).
 void launch_gather(cudaStream_t st, int n, const State& s, const uint32_t* sidx,
-                   double4* sbody, float* srad);
+                   double4* sbody, float* srad, float* samag = nullptr);
 // Zero acc of all rows (inactive rows keep 0).
 void launch_zero_acc(cudaStream_t st, int n, State s);
 

@@ -8,6 +8,7 @@
 // device memory on the hot path.  Every entry point returns a status; no C++
 // exception leaves this file; there is no CPU fallback.
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -21,6 +22,11 @@
 #include "sort.cuh"
 #include "tree.cuh"
 #include "walk.cuh"
+#include "mac_train.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <random>
 
 namespace {
 
@@ -60,6 +66,24 @@ struct nb_engine {
     double mac_budget = -3.0;
     int group_bodies = 32;
     double group_pack = 2.25;
+    // learned MAC
+    double mac_theta_lo = 0.35, mac_theta_hi = 1.0;
+    double mac_screen_q = 0.9;             // residual quantile that sets the screen margin
+    float mac_screen[nb::kMacScreen] = {0, 0, 0, 0, 0, 0, 0, 0, 0, INFINITY};
+    bool mac_ready = false;               // parameters trained or set
+    float mac_norm_host[nb::kMacNorm] = {0};
+    nb::MacDev* mac_dev = nullptr;        // BF16 fragment image for the walk
+    nb::MacTrainImage* mac_ti = nullptr;  // transposed fragments for training
+    float *mac_P = nullptr, *mac_m = nullptr, *mac_v = nullptr, *mac_G = nullptr;
+    float *mac_norm = nullptr, *mac_loss = nullptr;
+    int mac_adam_step = 0;
+    float* samag = nullptr;               // sorted |a| of the previous step
+    // training set (allocated by the first harvest)
+    float *mac_X = nullptr, *mac_Y = nullptr;
+    int mac_n = 0, mac_cap = 0;
+    nb::MacRecord* mac_rec = nullptr;
+    int mac_rec_cap = 0;
+    int* mac_counts = nullptr;            // [0] records, [1] accepted samples
     // device-resident state
     int n = 0;
     int n_active = 0;
@@ -91,12 +115,13 @@ struct nb_engine {
     cudaGraphExec_t graph_exec = nullptr;
     struct GraphKey {
         int flags, n, n_active, leaf_cap;
-        double dt, eps, theta, pack;
+        double dt, eps, theta, pack, mac_lo, mac_hi, mac_budget;
         const double* state;  // the state arrays swap after a compaction
         bool operator==(const GraphKey& o) const {
             return flags == o.flags && n == o.n && n_active == o.n_active &&
                    leaf_cap == o.leaf_cap && dt == o.dt && eps == o.eps && theta == o.theta &&
-                   pack == o.pack && state == o.state;
+                   pack == o.pack && mac_lo == o.mac_lo && mac_hi == o.mac_hi &&
+                   mac_budget == o.mac_budget && state == o.state;
         }
     } graph_key{};
     bool ev_valid = false;
@@ -211,12 +236,22 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
         return NB_OK;
     }
     const int na = h->n_active;
-    nb::launch_zero_acc(h->st, n, h->s);
+    const bool learned = (flags & NB_FLAG_LEARNED_MAC) != 0;
+    if (learned && (mode != NB_MODE_BARNES_HUT || shell || (flags & NB_FLAG_NO_QUADRUPOLE) ||
+                    !(eps > 0.0)))
+        return fail(h, NB_ERR_INVALID_ARG,
+                    "the learned MAC needs NB_MODE_BARNES_HUT with quadrupoles, no shell "
+                    "theorem and softening > 0");
+    if (learned && !h->mac_ready)
+        return fail(h, NB_ERR_STATE, "the learned MAC has no trained parameters");
     nb::launch_cube(h->st, sc->bbox_ord, nullptr, sc->cube);
     nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws);
     nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err,
                    h->sms);
-    nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, shell ? h->srad : nullptr);
+    // the gather reads the previous step's |a| before the buffer is zeroed
+    nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, shell ? h->srad : nullptr,
+                      learned ? h->samag : nullptr);
+    nb::launch_zero_acc(h->st, n, h->s);
     record(h, 1);
     if (mode == NB_MODE_DIRECT) {
         record(h, 2);
@@ -251,6 +286,15 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
             const double te = h->theta < 0.2 ? 0.2 : h->theta;  // barnes_hut_solver.cpp:16
             a.theta2 = te * te;
             nb::walk_reference(h->st, a, shell);
+        } else if (learned) {
+            // geometric below theta_lo, open from theta_hi, the network in between
+            a.theta2 = h->mac_theta_lo * h->mac_theta_lo;
+            a.mac_theta_hi2 = (float)(h->mac_theta_hi * h->mac_theta_hi);
+            a.samag = h->samag;
+            a.mac = h->mac_dev;
+            a.mac_budget = (float)((h->mac_budget * 3.321928094887362 - h->mac_norm_host[16]) /
+                                   h->mac_norm_host[17]);
+            nb::walk_group(h->st, h->wcfg, a, true, false, false, 2);
         } else {
             a.theta2 = h->theta * h->theta;
             nb::walk_group(h->st, h->wcfg, a, (flags & NB_FLAG_NO_QUADRUPOLE) == 0, shell, false);
@@ -267,8 +311,10 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
 // reuse the captured one when nothing it depends on changed.  Per-stage
 // timing events are not recorded inside the graph.
 int step_graph(nb_engine* h, int flags, double dt, double eps) {
-    const nb_engine::GraphKey key{flags, h->n, h->n_active, h->leaf_cap, dt,
-                                  eps, h->theta, h->group_pack, h->s.px};
+    const nb_engine::GraphKey key{flags,           h->n,           h->n_active,
+                                  h->leaf_cap,     dt,             eps,
+                                  h->theta,        h->group_pack,  h->mac_theta_lo,
+                                  h->mac_theta_hi, h->mac_budget,  h->s.px};
     if (h->graph_exec && key == h->graph_key) return NB_OK;
     if (h->graph_exec) {
         cudaGraphExecDestroy(h->graph_exec);
@@ -304,6 +350,7 @@ void collect_counters(nb_engine* h) {
         h->counters[NB_C_CELL_INTERACTIONS] = (int64_t)c[0];
         h->counters[NB_C_BODY_INTERACTIONS] = (int64_t)c[1];
         h->counters[NB_C_MAX_GROUP_WORK] = (int64_t)c[2];
+        h->counters[NB_C_MAC_EVALS] = (int64_t)c[3];
     }
     int nn = 0;
     if (h->ev_tree && cudaMemcpy(&nn, h->tree.n_nodes, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess)
@@ -391,6 +438,13 @@ NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
         if ((r = dalloc(h, (char**)&h->part, nb::diag_partial_bytes(capacity)))) break;
         if ((r = dalloc(h, &h->targets, cap)) || (r = dalloc(h, &h->tgt_out, 3 * cap))) break;
         if ((r = dalloc(h, &h->groups, cap))) break;
+        if ((r = dalloc(h, &h->samag, cap))) break;
+        if ((r = dalloc(h, &h->mac_dev, 1)) || (r = dalloc(h, &h->mac_ti, 1))) break;
+        if ((r = dalloc(h, &h->mac_P, nb::kMacParams)) || (r = dalloc(h, &h->mac_m, nb::kMacParams)) ||
+            (r = dalloc(h, &h->mac_v, nb::kMacParams)) || (r = dalloc(h, &h->mac_G, nb::kMacParams)))
+            break;
+        if ((r = dalloc(h, &h->mac_norm, nb::kMacNorm)) || (r = dalloc(h, &h->mac_loss, 4))) break;
+        if ((r = dalloc(h, &h->mac_counts, 4))) break;
         if ((r = nb::collide_alloc(h->col, capacity, [h](void** p, size_t b) {
                  return dalloc(h, (char**)p, b);
              })))
@@ -434,6 +488,18 @@ NB_API int32_t nb_set_param_f64(nb_engine* h, int32_t p, double v) {
             return NB_OK;
         case NB_PARAM_MIN_RADIUS: h->min_radius = v; return NB_OK;
         case NB_PARAM_MAC_BUDGET: h->mac_budget = v; return NB_OK;
+        case NB_PARAM_MAC_THETA_LO:
+            if (!(v > 0.0 && v < 2.0)) return fail(h, NB_ERR_INVALID_ARG, "theta_lo must be in (0, 2)");
+            h->mac_theta_lo = v;
+            return NB_OK;
+        case NB_PARAM_MAC_THETA_HI:
+            if (!(v > 0.0 && v < 4.0)) return fail(h, NB_ERR_INVALID_ARG, "theta_hi must be in (0, 4)");
+            h->mac_theta_hi = v;
+            return NB_OK;
+        case NB_PARAM_MAC_SCREEN_QUANTILE:
+            if (!(v >= 0.0 && v <= 1.0)) return fail(h, NB_ERR_INVALID_ARG, "screen quantile must be in [0, 1]");
+            h->mac_screen_q = v;
+            return NB_OK;
         case NB_PARAM_GROUP_PACK:
             if (!(v >= 0.0 && v <= 64.0)) return fail(h, NB_ERR_INVALID_ARG, "group packing must be 0..64");
             h->group_pack = v;
@@ -936,6 +1002,388 @@ NB_API int32_t nb_broad_phase(nb_engine* h, int32_t n, const double* px, const d
     h->has_state = false;
     if (np > max_pairs) return fail(h, NB_ERR_CAPACITY, "%d pairs > max_pairs %d", np, max_pairs);
     return NB_OK;
+}
+
+// ---- learned MAC ------------------------------------------------------------
+
+NB_API int32_t nb_mac_harvest(nb_engine* h, int32_t max_records, double sample_frac,
+                              uint64_t seed, double softening, int32_t* n_added) {
+    if (!h || !n_added) return NB_ERR_INVALID_ARG;
+    *n_added = 0;
+    if (!h->has_state) return fail(h, NB_ERR_STATE, "harvest needs device-resident state");
+    if (max_records <= 0 || !(sample_frac > 0.0 && sample_frac <= 1.0) || !(softening > 0.0))
+        return fail(h, NB_ERR_INVALID_ARG, "bad harvest arguments");
+    cudaSetDevice(h->device);
+    int r;
+    if (!h->mac_X) {
+        h->mac_cap = 1 << 24;
+        if ((r = dalloc(h, &h->mac_X, (size_t)h->mac_cap * nb::kMacIn)) ||
+            (r = dalloc(h, &h->mac_Y, (size_t)h->mac_cap)))
+            return r;
+    }
+    if (h->mac_rec_cap < max_records) {
+        if ((r = dalloc(h, &h->mac_rec, (size_t)max_records))) return r;
+        h->mac_rec_cap = max_records;
+    }
+    const int n = h->n, na = h->n_active;
+    Scal* sc = h->scal;
+    nb::launch_kick_drift_bbox(h->st, n, h->s, false, 0.0, sc->bbox_ord, &sc->n_active, sc->err);
+    nb::launch_cube(h->st, sc->bbox_ord, nullptr, sc->cube);
+    nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws);
+    nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err, h->sms);
+    nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, nullptr, h->samag);
+    nb::launch_zero_acc(h->st, n, h->s);
+    nb::tree_build(h->st, h->tree, na, h->keys0, h->sbody, nullptr, sc->cube, h->leaf_cap, sc->err);
+    NB_CUDA(h, cudaMemsetAsync(h->mac_counts, 0, sizeof(int) * 4, h->st));
+    nb::WalkArgs a{};
+    a.n = na;
+    a.sbody = h->sbody;
+    a.skeys = h->keys0;
+    a.sidx = h->vals0;
+    a.t = h->tree;
+    a.eps2 = softening * softening;
+    a.ax = h->s.ax;
+    a.ay = h->s.ay;
+    a.az = h->s.az;
+    a.front = h->front;
+    a.group_ctr = &sc->group_ctr;
+    a.groups = h->groups;
+    a.n_groups = &sc->n_groups;
+    a.pack = h->group_pack;
+    a.counters = sc->counters;
+    a.err = sc->err;
+    a.theta2 = h->mac_theta_lo * h->mac_theta_lo;
+    a.mac_theta_hi2 = (float)(h->mac_theta_hi * h->mac_theta_hi);
+    a.samag = h->samag;
+    a.records = h->mac_rec;
+    a.n_records = &h->mac_counts[0];
+    a.record_cap = max_records;
+    a.mac_seed = (unsigned)(seed ^ (seed >> 32));
+    a.mac_sample = (unsigned)std::min(65536.0, std::ceil(sample_frac * 65536.0));
+    nb::walk_group(h->st, h->wcfg, a, true, false, false, 1);
+    int nrec = 0;
+    if ((r = download(h, &nrec, &h->mac_counts[0], sizeof(int)))) return r;
+    if ((r = check_device(h))) return r;
+    nrec = std::min(nrec, max_records);
+    nb::mac_targets(h->st, nrec, h->mac_rec, h->sbody, h->tree, softening, h->mac_X, h->mac_Y,
+                    &h->mac_counts[1], h->mac_n, h->mac_cap);
+    int got = 0;
+    if ((r = download(h, &got, &h->mac_counts[1], sizeof(int)))) return r;
+    if ((r = check_device(h))) return r;
+    got = std::min(got, h->mac_cap - h->mac_n);
+    h->mac_n += got;
+    *n_added = got;
+    return NB_OK;
+}
+
+NB_API int32_t nb_mac_dataset(nb_engine* h, int32_t* n, float* X, float* Y) {
+    if (!h || !n) return NB_ERR_INVALID_ARG;
+    *n = h->mac_n;
+    if (h->mac_n == 0) return NB_OK;
+    int r;
+    if ((r = download(h, X, h->mac_X, sizeof(float) * nb::kMacIn * (size_t)h->mac_n)) ||
+        (r = download(h, Y, h->mac_Y, sizeof(float) * (size_t)h->mac_n)))
+        return r;
+    return check_device(h);
+}
+
+NB_API int32_t nb_mac_clear(nb_engine* h) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    h->mac_n = 0;
+    return NB_OK;
+}
+
+namespace {
+
+// The screen block (normalised units) and its raw-feature form with the
+// normalisation folded in: scr_w[k] = w[k] / std[k], scr_b = b - sum w[k]
+// mean[k] / std[k] (inv_std as the device forms it, 1.f / std).
+int mac_upload_screen(nb_engine* h) {
+    constexpr int kIn = nb::kMacIn;
+    float blk[nb::kMacScreen + kIn + 1];
+    std::copy(h->mac_screen, h->mac_screen + nb::kMacScreen, blk);
+    double b = h->mac_screen[kIn];
+    for (int k = 0; k < kIn; k++) {
+        const float inv = 1.f / h->mac_norm_host[kIn + k];
+        blk[nb::kMacScreen + k] = h->mac_screen[k] * inv;
+        b -= (double)h->mac_screen[k] * h->mac_norm_host[k] * inv;
+    }
+    blk[nb::kMacScreen + kIn] = (float)b;
+    static_assert(offsetof(nb::MacDev, scr_w) == offsetof(nb::MacDev, lin_w) + sizeof(float) * nb::kMacScreen,
+                  "screen block layout");
+    return upload(h, h->mac_dev->lin_w, blk, sizeof(blk));
+}
+
+int mac_upload_params(nb_engine* h, const float* P, const float* norm) {
+    int r;
+    if ((r = upload(h, h->mac_P, P, sizeof(float) * nb::kMacParams)) ||
+        (r = upload(h, h->mac_norm, norm, sizeof(float) * nb::kMacNorm)))
+        return r;
+    NB_CUDA(h, cudaMemsetAsync(h->mac_m, 0, sizeof(float) * nb::kMacParams, h->st));
+    NB_CUDA(h, cudaMemsetAsync(h->mac_v, 0, sizeof(float) * nb::kMacParams, h->st));
+    h->mac_adam_step = 0;
+    std::copy(norm, norm + nb::kMacNorm, h->mac_norm_host);
+    nb::mac_image(h->st, h->mac_P, h->mac_norm, h->mac_dev, h->mac_ti);
+    // a new network invalidates the screen: off until the next fit
+    std::fill(h->mac_screen, h->mac_screen + nb::kMacScreen, 0.f);
+    h->mac_screen[nb::kMacScreen - 1] = INFINITY;
+    int r2 = mac_upload_screen(h);
+    return r2 ? r2 : check_device(h);
+}
+
+// Least-squares fit of the screen to the network's predictions on (a strided
+// sample of) the multi-body rows of the training set; margin = the chosen
+// quantile of |residual| in normalised target units.
+int mac_fit_screen(nb_engine* h) {
+    float sc[nb::kMacScreen] = {0, 0, 0, 0, 0, 0, 0, 0, 0, INFINITY};
+    const int n = h->mac_n;
+    constexpr int kIn = nb::kMacIn;
+    if (h->mac_screen_q > 0.0 && n >= 64) {
+        const int m = std::min(n, 1 << 18);
+        const int stride = n / m;
+        float *dX = nullptr, *dy = nullptr;
+        NB_CUDA(h, cudaMalloc(&dX, sizeof(float) * kIn * (size_t)m));
+        if (cudaMalloc(&dy, sizeof(float) * (size_t)m) != cudaSuccess) {
+            cudaFree(dX);
+            return fail(h, NB_ERR_CUDA, "screen fit: out of device memory");
+        }
+        cudaMemcpy2DAsync(dX, sizeof(float) * kIn, h->mac_X, sizeof(float) * kIn * (size_t)stride,
+                          sizeof(float) * kIn, (size_t)m, cudaMemcpyDeviceToDevice, h->st);
+        nb::mac_predict(h->st, dX, m, h->mac_dev, dy);
+        std::vector<float> X((size_t)m * kIn), y((size_t)m);
+        int r = download(h, X.data(), dX, sizeof(float) * X.size());
+        if (!r) r = download(h, y.data(), dy, sizeof(float) * y.size());
+        if (!r) r = check_device(h);
+        cudaFree(dX);
+        cudaFree(dy);
+        if (r) return r;
+        const float* nm = h->mac_norm_host;
+        float inv[kIn];
+        for (int k = 0; k < kIn; k++) inv[k] = 1.f / nm[kIn + k];
+        // normal equations over [x_norm, 1]
+        double A[kIn + 1][kIn + 2] = {};
+        std::vector<float> fn((size_t)m * kIn);
+        std::vector<double> yn((size_t)m);
+        std::vector<char> use((size_t)m);
+        int rows = 0;
+        for (int i = 0; i < m; i++) {
+            const float* xi = &X[(size_t)i * kIn];
+            use[i] = xi[4] > 0.5f;  // log2(count): one-body cells never reach the screen
+            if (!use[i]) continue;
+            double v[kIn + 1];
+            for (int k = 0; k < kIn; k++) v[k] = fn[(size_t)i * kIn + k] = (xi[k] - nm[k]) * inv[k];
+            v[kIn] = 1.0;
+            yn[i] = ((double)y[i] - nm[2 * kIn]) / nm[2 * kIn + 1];
+            for (int a = 0; a <= kIn; a++) {
+                for (int b = 0; b <= kIn; b++) A[a][b] += v[a] * v[b];
+                A[a][kIn + 1] += v[a] * yn[i];
+            }
+            rows++;
+        }
+        if (rows >= 64) {
+            for (int a = 0; a <= kIn; a++) A[a][a] += 1e-9 * (A[a][a] + 1.0);
+            // Gaussian elimination with partial pivoting
+            for (int c = 0; c <= kIn; c++) {
+                int piv = c;
+                for (int r1 = c + 1; r1 <= kIn; r1++)
+                    if (std::fabs(A[r1][c]) > std::fabs(A[piv][c])) piv = r1;
+                for (int k = 0; k <= kIn + 1; k++) std::swap(A[c][k], A[piv][k]);
+                for (int r1 = 0; r1 <= kIn; r1++) {
+                    if (r1 == c) continue;
+                    const double f = A[r1][c] / A[c][c];
+                    for (int k = c; k <= kIn + 1; k++) A[r1][k] -= f * A[c][k];
+                }
+            }
+            float w[kIn + 1];
+            for (int a = 0; a <= kIn; a++) w[a] = (float)(A[a][kIn + 1] / A[a][a]);
+            std::vector<double> res;
+            res.reserve(rows);
+            for (int i = 0; i < m; i++) {
+                if (!use[i]) continue;
+                float s1 = w[kIn];
+                for (int k = 0; k < kIn; k++) s1 = std::fma(w[k], fn[(size_t)i * kIn + k], s1);
+                res.push_back(std::fabs(yn[i] - (double)s1));
+            }
+            const size_t q = std::min(res.size() - 1, (size_t)(h->mac_screen_q * (double)res.size()));
+            std::nth_element(res.begin(), res.begin() + q, res.end());
+            bool finite = std::isfinite(res[q]);
+            for (int a = 0; a <= kIn; a++) finite = finite && std::isfinite(w[a]);
+            if (finite) {
+                std::copy(w, w + kIn + 1, sc);
+                sc[kIn + 1] = (float)(res[q] * 1.0001 + 1e-6);
+            }
+        }
+    }
+    std::copy(sc, sc + nb::kMacScreen, h->mac_screen);
+    int r = mac_upload_screen(h);
+    return r ? r : check_device(h);
+}
+
+}  // namespace
+
+NB_API int32_t nb_mac_set_params(nb_engine* h, const float* params, int32_t n) {
+    if (!h || !params || n != nb::kMacParams + nb::kMacNorm) return NB_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    for (int k = 0; k < nb::kMacIn + 1; k++)
+        if (!(params[nb::kMacParams + nb::kMacIn + k] > 0.f) && k < nb::kMacIn)
+            return fail(h, NB_ERR_INVALID_ARG, "feature scales must be positive");
+    if (!(params[nb::kMacParams + nb::kMacNorm - 1] > 0.f))
+        return fail(h, NB_ERR_INVALID_ARG, "target scale must be positive");
+    int r = mac_upload_params(h, params, params + nb::kMacParams);
+    if (r) return r;
+    h->mac_ready = true;
+    return NB_OK;
+}
+
+NB_API int32_t nb_mac_get_params(nb_engine* h, float* out, int32_t n) {
+    if (!h || !out || n != nb::kMacParams + nb::kMacNorm) return NB_ERR_INVALID_ARG;
+    if (!h->mac_ready) return fail(h, NB_ERR_STATE, "no learned-MAC parameters");
+    cudaSetDevice(h->device);
+    int r;
+    if ((r = download(h, out, h->mac_P, sizeof(float) * nb::kMacParams))) return r;
+    std::copy(h->mac_norm_host, h->mac_norm_host + nb::kMacNorm, out + nb::kMacParams);
+    return check_device(h);
+}
+
+NB_API int32_t nb_mac_train(nb_engine* h, int32_t epochs, int32_t batch, double lr, uint64_t seed,
+                            double* loss_per_epoch) {
+    if (!h || epochs < 0 || batch < 32 || !(lr > 0.0)) return NB_ERR_INVALID_ARG;
+    const int n = h->mac_n;
+    if (n < batch) return fail(h, NB_ERR_STATE, "%d samples < batch %d", n, batch);
+    cudaSetDevice(h->device);
+    int r = NB_OK;
+    if (!h->mac_ready) {
+        // normalisation from the data, He-uniform initial weights
+        std::vector<float> X((size_t)n * nb::kMacIn), Y((size_t)n);
+        if ((r = download(h, X.data(), h->mac_X, sizeof(float) * X.size())) ||
+            (r = download(h, Y.data(), h->mac_Y, sizeof(float) * Y.size())) || (r = check_device(h)))
+            return r;
+        float norm[nb::kMacNorm];
+        for (int k = 0; k <= nb::kMacIn; k++) {
+            double s = 0, s2 = 0;
+            for (int i = 0; i < n; i++) {
+                const double v = k < nb::kMacIn ? X[(size_t)i * nb::kMacIn + k] : Y[i];
+                s += v;
+                s2 += v * v;
+            }
+            const double mean = s / n, var = std::max(s2 / n - mean * mean, 0.0);
+            const float sd = (float)std::max(std::sqrt(var), 1e-3);
+            if (k < nb::kMacIn) {
+                norm[k] = (float)mean;
+                norm[nb::kMacIn + k] = sd;
+            } else {
+                norm[2 * nb::kMacIn] = (float)mean;
+                norm[2 * nb::kMacIn + 1] = sd;
+            }
+        }
+        std::vector<float> P(nb::kMacParams, 0.f);
+        std::mt19937_64 rng(seed);
+        auto fill = [&](int off, int count, int fan_in) {
+            std::uniform_real_distribution<float> u(-std::sqrt(6.f / fan_in), std::sqrt(6.f / fan_in));
+            for (int i = 0; i < count; i++) P[off + i] = u(rng);
+        };
+        fill(nb::kMacW1, nb::kMacIn * nb::kMacHid, nb::kMacIn);
+        fill(nb::kMacW2, nb::kMacHid * nb::kMacHid, nb::kMacHid);
+        fill(nb::kMacW3, nb::kMacHid, nb::kMacHid);
+        if ((r = mac_upload_params(h, P.data(), norm))) return r;
+        h->mac_ready = true;
+    }
+    int* order = nullptr;
+    NB_CUDA(h, cudaMalloc(&order, sizeof(int) * (size_t)n));
+    std::vector<int> perm((size_t)n);
+    for (int i = 0; i < n; i++) perm[i] = i;
+    std::mt19937_64 rng(seed * 0x9E3779B97F4A7C15ull + 1);
+    for (int e = 0; e < epochs && r == NB_OK; e++) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        if ((r = upload(h, order, perm.data(), sizeof(int) * (size_t)n))) break;
+        cudaMemsetAsync(h->mac_loss, 0, sizeof(float), h->st);
+        for (int row0 = 0; row0 < n; row0 += batch) {
+            const int rows = std::min(batch, n - row0);
+            nb::mac_grad(h->st, h->mac_X, h->mac_Y, order, row0, rows, h->mac_dev, h->mac_ti,
+                         h->mac_G, h->mac_loss, h->sms);
+            nb::mac_adam(h->st, h->mac_P, h->mac_G, h->mac_m, h->mac_v, ++h->mac_adam_step, (float)lr);
+            nb::mac_image(h->st, h->mac_P, h->mac_norm, h->mac_dev, h->mac_ti);
+        }
+        float loss = 0.f;
+        if ((r = download(h, &loss, h->mac_loss, sizeof(float)))) break;
+        if ((r = check_device(h))) break;
+        if (loss_per_epoch) loss_per_epoch[e] = (double)loss / n;
+    }
+    cudaStreamSynchronize(h->st);
+    cudaFree(order);
+    if (r == NB_OK) r = mac_fit_screen(h);
+    return r;
+}
+
+NB_API int32_t nb_mac_fit_screen(nb_engine* h) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    if (!h->mac_ready) return fail(h, NB_ERR_STATE, "no learned-MAC parameters");
+    cudaSetDevice(h->device);
+    return mac_fit_screen(h);
+}
+
+NB_API int32_t nb_mac_get_screen(nb_engine* h, float* screen, int32_t n) {
+    if (!h || !screen || n != nb::kMacScreen) return NB_ERR_INVALID_ARG;
+    std::copy(h->mac_screen, h->mac_screen + nb::kMacScreen, screen);
+    return NB_OK;
+}
+
+NB_API int32_t nb_mac_set_screen(nb_engine* h, const float* screen, int32_t n) {
+    if (!h || !screen || n != nb::kMacScreen) return NB_ERR_INVALID_ARG;
+    if (!h->mac_ready) return fail(h, NB_ERR_STATE, "no learned-MAC parameters");
+    for (int k = 0; k < nb::kMacScreen - 1; k++)
+        if (!std::isfinite(screen[k])) return fail(h, NB_ERR_INVALID_ARG, "screen weights must be finite");
+    if (!(screen[nb::kMacScreen - 1] >= 0.f))
+        return fail(h, NB_ERR_INVALID_ARG, "screen margin must be >= 0 (+inf = off)");
+    cudaSetDevice(h->device);
+    std::copy(screen, screen + nb::kMacScreen, h->mac_screen);
+    int r = mac_upload_screen(h);
+    return r ? r : check_device(h);
+}
+
+NB_API int32_t nb_mac_gradient(nb_engine* h, const float* X, const float* Y, int32_t n,
+                               float* grad, double* loss) {
+    if (!h || !X || !Y || !grad || n <= 0) return NB_ERR_INVALID_ARG;
+    if (!h->mac_ready) return fail(h, NB_ERR_STATE, "no learned-MAC parameters");
+    cudaSetDevice(h->device);
+    float *dX = nullptr, *dY = nullptr;
+    int* dO = nullptr;
+    NB_CUDA(h, cudaMalloc(&dX, sizeof(float) * (size_t)n * (nb::kMacIn + 1) + sizeof(int) * (size_t)n));
+    dY = dX + (size_t)n * nb::kMacIn;
+    dO = (int*)(dY + n);
+    std::vector<int> ord((size_t)n);
+    for (int i = 0; i < n; i++) ord[i] = i;
+    int r;
+    if (!(r = upload(h, dX, X, sizeof(float) * (size_t)n * nb::kMacIn)) &&
+        !(r = upload(h, dY, Y, sizeof(float) * (size_t)n)) &&
+        !(r = upload(h, dO, ord.data(), sizeof(int) * (size_t)n))) {
+        cudaMemsetAsync(h->mac_loss, 0, sizeof(float), h->st);
+        nb::mac_grad(h->st, dX, dY, dO, 0, n, h->mac_dev, h->mac_ti, h->mac_G, h->mac_loss, h->sms);
+        float l = 0.f;
+        if (!(r = download(h, grad, h->mac_G, sizeof(float) * nb::kMacParams)) &&
+            !(r = download(h, &l, h->mac_loss, sizeof(float))) && !(r = check_device(h)) && loss)
+            *loss = (double)l / n;
+    }
+    cudaStreamSynchronize(h->st);
+    cudaFree(dX);
+    return r;
+}
+
+NB_API int32_t nb_mac_predict(nb_engine* h, const float* X, int32_t n, float* y) {
+    if (!h || !X || !y || n <= 0) return NB_ERR_INVALID_ARG;
+    if (!h->mac_ready) return fail(h, NB_ERR_STATE, "no learned-MAC parameters");
+    cudaSetDevice(h->device);
+    float* dX = nullptr;
+    NB_CUDA(h, cudaMalloc(&dX, sizeof(float) * (size_t)n * (nb::kMacIn + 1)));
+    int r;
+    if (!(r = upload(h, dX, X, sizeof(float) * (size_t)n * nb::kMacIn))) {
+        nb::mac_predict(h->st, dX, n, h->mac_dev, dX + (size_t)n * nb::kMacIn);
+        if (!(r = download(h, y, dX + (size_t)n * nb::kMacIn, sizeof(float) * (size_t)n)))
+            r = check_device(h);
+    }
+    cudaStreamSynchronize(h->st);
+    cudaFree(dX);
+    return r;
 }
 
 }  // extern "C"

@@ -1,0 +1,400 @@
+// mac.cu - training data, training and the device image of the learned MAC.
+//
+// * k_mac_targets: for every harvested (group, cell) record, the exact FP64
+//   force of the cell's bodies on the group body nearest the cell's centre of
+//   mass against the monopole+quadrupole approximation the walk uses; the
+//   target is log2(|difference| / smallest |a| of the group).  One warp per
+//   record splits the cell's bodies.
+// * k_mac_train: forward and backward of the 8-64-64-1 network on 16-row
+//   tiles per warp with BF16 mma.sync tensor-core tiles (FP32 accumulate) for
+//   every product: X W1, H1 W2, the activation gradient G2 W2^T, and the
+//   weight gradients H1^T G2 and X^T G1.  Block partial gradients go to shared
+//   memory, then once per block to the global FP32 gradient.
+// * k_mac_adam: Adam on the FP32 master parameters; k_mac_image rebuilds the
+//   BF16 fragment image (MacDev) the walk and the training kernel read.
+#include "mac.cuh"
+#include "mac_train.cuh"
+#include "tree.cuh"
+
+namespace nb {
+
+// ---- targets ---------------------------------------------------------------
+
+__global__ void k_mac_targets(int nrec, const MacRecord* __restrict__ rec,
+                              const double4* __restrict__ sbody, TreeBufs t, double eps2,
+                              float* __restrict__ X, float* __restrict__ Y, int* __restrict__ n_out,
+                              int out_off, int out_cap) {
+    const int lane = threadIdx.x & 31;
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= nrec) return;
+    const MacRecord R = rec[r];
+    const double4 b = sbody[R.body];
+    const int4 lk = t.link[R.node];
+    double ex = 0, ey = 0, ez = 0;
+    for (int j = lk.z + lane; j < lk.z + lk.w; j += 32) {
+        if (j == R.body) continue;
+        const double4 p = sbody[j];
+        const double dx = p.x - b.x, dy = p.y - b.y, dz = p.z - b.z;
+        const double inv = 1.0 / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+        const double f = p.w * inv * inv * inv;
+        ex += f * dx;
+        ey += f * dy;
+        ez += f * dz;
+    }
+    ex = warp_sum(ex);
+    ey = warp_sum(ey);
+    ez = warp_sum(ez);
+    if (lane != 0) return;
+    // the walk's approximation, in FP64: d = body - COM
+    const double4 cm = t.com[R.node];
+    const float4 q0 = t.q0[R.node];
+    const double qxx = q0.x, qyy = q0.y, qxy = q0.z, qxz = q0.w, qyz = t.q1[R.node].x;
+    const double qzz = -(qxx + qyy);
+    const double dx = b.x - cm.x, dy = b.y - cm.y, dz = b.z - cm.z;
+    const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+    const double inv = 1.0 / sqrt(r2);
+    const double inv2 = inv * inv, inv3 = inv * inv2, inv5 = inv3 * inv2;
+    const double qx = qxx * dx + qxy * dy + qxz * dz;
+    const double qy = qxy * dx + qyy * dy + qyz * dz;
+    const double qz = qxz * dx + qyz * dy + qzz * dz;
+    const double rqr = dx * qx + dy * qy + dz * qz;
+    const double f = -cm.w * inv3 - 2.5 * rqr * inv5 * inv2;
+    const double ax = f * dx + qx * inv5, ay = f * dy + qy * inv5, az = f * dz + qz * inv5;
+    const double err = sqrt((ax - ex) * (ax - ex) + (ay - ey) * (ay - ey) + (az - ez) * (az - ez));
+    if (!(R.a_min > 0.f)) return;  // no acceleration estimate: not a usable sample
+    const int slot = atomicAdd(n_out, 1);
+    if (out_off + slot >= out_cap) return;
+    for (int k = 0; k < kMacIn; k++) X[(size_t)(out_off + slot) * kMacIn + k] = R.f[k];
+    Y[out_off + slot] = (float)log2(err / (double)R.a_min + 1e-30);
+}
+
+void mac_targets(cudaStream_t st, int nrec, const MacRecord* rec, const double4* sbody,
+                 const TreeBufs& t, double eps, float* X, float* Y, int* n_out, int out_off,
+                 int out_cap) {
+    if (nrec <= 0) return;
+    k_mac_targets<<<ceil_div((long long)nrec * 32, 256), 256, 0, st>>>(
+        nrec, rec, sbody, t, eps * eps, X, Y, n_out, out_off, out_cap);
+}
+
+// ---- device image ------------------------------------------------------------
+
+__global__ void k_mac_image(const float* __restrict__ P, const float* __restrict__ norm,
+                            MacDev* __restrict__ w, MacTrainImage* __restrict__ ti) {
+    const int tid = threadIdx.x;
+    // lane-ordered B fragments: lane = 4 * g + t holds (k = 2t, 2t+1 | 2t+8, 2t+9; n = g)
+    for (int e = tid; e < 8 * 32; e += blockDim.x) {
+        const int nt = e / 32, lane = e % 32, g = lane >> 2, t4 = lane & 3;
+        const int n = nt * 8 + g;
+        auto W1 = [&](int k) { return k < kMacIn ? P[kMacW1 + k * kMacHid + n] : 0.f; };
+        w->w1f[nt][lane] = make_uint2(pack_bf16(W1(2 * t4), W1(2 * t4 + 1)),
+                                      pack_bf16(W1(2 * t4 + 8), W1(2 * t4 + 9)));
+    }
+    for (int e = tid; e < 4 * 8 * 32; e += blockDim.x) {
+        const int kt = e / 256, nt = (e / 32) % 8, lane = e % 32, g = lane >> 2, t4 = lane & 3;
+        const int n = nt * 8 + g, k0 = kt * 16 + 2 * t4;
+        auto W2 = [&](int k) { return P[kMacW2 + k * kMacHid + n]; };    // W2[k][n]
+        auto W2T = [&](int k) { return P[kMacW2 + n * kMacHid + k]; };   // W2^T[k][n] = W2[n][k]
+        w->w2f[kt][nt][lane] = make_uint2(pack_bf16(W2(k0), W2(k0 + 1)), pack_bf16(W2(k0 + 8), W2(k0 + 9)));
+        ti->w2tf[kt][nt][lane] =
+            make_uint2(pack_bf16(W2T(k0), W2T(k0 + 1)), pack_bf16(W2T(k0 + 8), W2T(k0 + 9)));
+    }
+    for (int e = tid; e < kMacHid; e += blockDim.x) {
+        w->b1[e] = P[kMacB1 + e];
+        w->b2[e] = P[kMacB2 + e];
+        w->w3[e] = P[kMacW3 + e];
+    }
+    if (tid == 0) w->b3 = P[kMacB3];
+    if (tid < kMacIn) {
+        w->mean[tid] = norm[tid];
+        w->inv_std[tid] = 1.f / norm[kMacIn + tid];
+    }
+    if (tid == 0) {
+        w->y_mean = norm[2 * kMacIn];
+        w->y_std = norm[2 * kMacIn + 1];
+    }
+}
+
+void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w, MacTrainImage* ti) {
+    k_mac_image<<<1, 256, 0, st>>>(P, norm, w, ti);
+}
+
+// ---- training --------------------------------------------------------------
+
+constexpr int kTrainWarps = 4;
+
+struct TrainSmem {
+    float dW1[kMacIn][kMacHid];
+    float dW2[kMacHid][kMacHid];
+    float db1[kMacHid], db2[kMacHid], dw3[kMacHid];
+    float db3, loss;
+    // per warp staging of one 16-row tile
+    __nv_bfloat16 xs[kTrainWarps][16][16];
+    __nv_bfloat16 h1[kTrainWarps][16][kMacHid];
+    __nv_bfloat16 g2[kTrainWarps][16][kMacHid];
+    __nv_bfloat16 g1[kTrainWarps][16][kMacHid];
+};
+
+__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16* p) {
+    return *reinterpret_cast<const uint32_t*>(p);
+}
+__device__ __forceinline__ uint32_t pair_of(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// rows [row0, row0 + nrows) of the batch; X raw features, Y raw targets;
+// grad (4801 floats) and loss accumulate over the whole launch.
+__global__ void __launch_bounds__(kTrainWarps * 32)
+k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
+            const int* __restrict__ order, int row0, int nrows, const MacDev* __restrict__ w,
+            const MacTrainImage* __restrict__ ti, float inv_batch, float* __restrict__ grad,
+            float* __restrict__ loss) {
+    __shared__ TrainSmem S;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t4 = lane & 3;
+    for (int e = threadIdx.x; e < kMacIn * kMacHid; e += blockDim.x) (&S.dW1[0][0])[e] = 0.f;
+    for (int e = threadIdx.x; e < kMacHid * kMacHid; e += blockDim.x) (&S.dW2[0][0])[e] = 0.f;
+    for (int e = threadIdx.x; e < kMacHid; e += blockDim.x) S.db1[e] = S.db2[e] = S.dw3[e] = 0.f;
+    if (threadIdx.x == 0) S.db3 = S.loss = 0.f;
+    __syncthreads();
+    const int tiles = (nrows + 15) / 16;
+    for (int tile = blockIdx.x * kTrainWarps + warp; tile < tiles; tile += gridDim.x * kTrainWarps) {
+        // 1. stage 16 normalised rows (rows past the end get zero gradient)
+        const int r_lo = tile * 16;
+        for (int e = lane; e < 16 * 16; e += 32) {
+            const int r = e / 16, k = e % 16;
+            float v = 0.f;
+            if (k < kMacIn && r_lo + r < nrows) {
+                const int row = order[row0 + r_lo + r];
+                v = (X[(size_t)row * kMacIn + k] - w->mean[k]) * w->inv_std[k];
+            }
+            S.xs[warp][r][k] = __float2bfloat16_rn(v);
+        }
+        __syncwarp();
+        // 2. layer 1 -> h1 (bf16, row-major in smem)
+        const uint32_t a0 = ld_pair(&S.xs[warp][g][2 * t4]), a1 = ld_pair(&S.xs[warp][g + 8][2 * t4]);
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const float bl = w->b1[nt * 8 + 2 * t4], bh = w->b1[nt * 8 + 2 * t4 + 1];
+            float c[4] = {bl, bh, bl, bh};
+            mma_bf16(c, a0, a1, 0u, 0u, w->w1f[nt][lane]);
+            const int col = nt * 8 + 2 * t4;
+            S.h1[warp][g][col] = __float2bfloat16_rn(fmaxf(c[0], 0.f));
+            S.h1[warp][g][col + 1] = __float2bfloat16_rn(fmaxf(c[1], 0.f));
+            S.h1[warp][g + 8][col] = __float2bfloat16_rn(fmaxf(c[2], 0.f));
+            S.h1[warp][g + 8][col + 1] = __float2bfloat16_rn(fmaxf(c[3], 0.f));
+        }
+        __syncwarp();
+        // 3. layer 2 (pre-activations kept in registers) and output
+        float z2[8][4];
+        float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const float bl = w->b2[nt * 8 + 2 * t4], bh = w->b2[nt * 8 + 2 * t4 + 1];
+            z2[nt][0] = bl; z2[nt][1] = bh; z2[nt][2] = bl; z2[nt][3] = bh;
+#pragma unroll
+            for (int kt = 0; kt < 4; kt++) {
+                const int k0 = kt * 16 + 2 * t4;
+                mma_bf16(z2[nt], ld_pair(&S.h1[warp][g][k0]), ld_pair(&S.h1[warp][g + 8][k0]),
+                         ld_pair(&S.h1[warp][g][k0 + 8]), ld_pair(&S.h1[warp][g + 8][k0 + 8]),
+                         w->w2f[kt][nt][lane]);
+            }
+            const float wl = w->w3[nt * 8 + 2 * t4], wh = w->w3[nt * 8 + 2 * t4 + 1];
+            y0 = fmaf(fmaxf(z2[nt][0], 0.f), wl, fmaf(fmaxf(z2[nt][1], 0.f), wh, y0));
+            y1 = fmaf(fmaxf(z2[nt][2], 0.f), wl, fmaf(fmaxf(z2[nt][3], 0.f), wh, y1));
+        }
+        y0 += __shfl_xor_sync(0xFFFFFFFFu, y0, 1);
+        y0 += __shfl_xor_sync(0xFFFFFFFFu, y0, 2);
+        y1 += __shfl_xor_sync(0xFFFFFFFFu, y1, 1);
+        y1 += __shfl_xor_sync(0xFFFFFFFFu, y1, 2);
+        y0 += w->b3;
+        y1 += w->b3;
+        // 4. loss and dL/dy for rows g and g + 8 (mean squared error)
+        float d0 = 0.f, d1 = 0.f;
+        if (r_lo + g < nrows) {
+            const float tg = (Y[order[row0 + r_lo + g]] - w->y_mean) / w->y_std;
+            d0 = 2.f * (y0 - tg) * inv_batch;
+            if (t4 == 0) atomicAdd(&S.loss, (y0 - tg) * (y0 - tg));
+        }
+        if (r_lo + g + 8 < nrows) {
+            const float tg = (Y[order[row0 + r_lo + g + 8]] - w->y_mean) / w->y_std;
+            d1 = 2.f * (y1 - tg) * inv_batch;
+            if (t4 == 0) atomicAdd(&S.loss, (y1 - tg) * (y1 - tg));
+        }
+        // 5. g2 = dy w3 [z2 > 0]; dw3, db2 partials; db3
+        float pdb3 = (t4 == 0) ? d0 + d1 : 0.f;
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const int col = nt * 8 + 2 * t4;
+            const float wl = w->w3[col], wh = w->w3[col + 1];
+            const float g00 = z2[nt][0] > 0.f ? d0 * wl : 0.f, g01 = z2[nt][1] > 0.f ? d0 * wh : 0.f;
+            const float g10 = z2[nt][2] > 0.f ? d1 * wl : 0.f, g11 = z2[nt][3] > 0.f ? d1 * wh : 0.f;
+            S.g2[warp][g][col] = __float2bfloat16_rn(g00);
+            S.g2[warp][g][col + 1] = __float2bfloat16_rn(g01);
+            S.g2[warp][g + 8][col] = __float2bfloat16_rn(g10);
+            S.g2[warp][g + 8][col + 1] = __float2bfloat16_rn(g11);
+            float w3l = fmaxf(z2[nt][0], 0.f) * d0 + fmaxf(z2[nt][2], 0.f) * d1;
+            float w3h = fmaxf(z2[nt][1], 0.f) * d0 + fmaxf(z2[nt][3], 0.f) * d1;
+            float b2l = g00 + g10, b2h = g01 + g11;
+#pragma unroll
+            for (int o = 4; o < 32; o <<= 1) {  // sum over g (lanes with the same t)
+                w3l += __shfl_xor_sync(0xFFFFFFFFu, w3l, o);
+                w3h += __shfl_xor_sync(0xFFFFFFFFu, w3h, o);
+                b2l += __shfl_xor_sync(0xFFFFFFFFu, b2l, o);
+                b2h += __shfl_xor_sync(0xFFFFFFFFu, b2h, o);
+            }
+            if (g == 0) {
+                atomicAdd(&S.dw3[col], w3l);
+                atomicAdd(&S.dw3[col + 1], w3h);
+                atomicAdd(&S.db2[col], b2l);
+                atomicAdd(&S.db2[col + 1], b2h);
+            }
+        }
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1) pdb3 += __shfl_xor_sync(0xFFFFFFFFu, pdb3, o);
+        if (lane == 0) atomicAdd(&S.db3, pdb3);
+        __syncwarp();
+        // 6. dW2 += H1^T G2: M = 64 inputs (4 m-tiles), N = 64 outputs, K = 16 rows
+#pragma unroll
+        for (int mt = 0; mt < 4; mt++) {
+            const int i0 = mt * 16 + g;
+            const uint32_t b_a0 = pair_of(S.h1[warp][2 * t4][i0], S.h1[warp][2 * t4 + 1][i0]);
+            const uint32_t b_a1 = pair_of(S.h1[warp][2 * t4][i0 + 8], S.h1[warp][2 * t4 + 1][i0 + 8]);
+            const uint32_t b_a2 = pair_of(S.h1[warp][2 * t4 + 8][i0], S.h1[warp][2 * t4 + 9][i0]);
+            const uint32_t b_a3 = pair_of(S.h1[warp][2 * t4 + 8][i0 + 8], S.h1[warp][2 * t4 + 9][i0 + 8]);
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++) {
+                const int j = nt * 8 + g;
+                const uint2 bb = make_uint2(pair_of(S.g2[warp][2 * t4][j], S.g2[warp][2 * t4 + 1][j]),
+                                            pair_of(S.g2[warp][2 * t4 + 8][j], S.g2[warp][2 * t4 + 9][j]));
+                float c[4] = {0.f, 0.f, 0.f, 0.f};
+                mma_bf16(c, b_a0, b_a1, b_a2, b_a3, bb);
+                const int col = nt * 8 + 2 * t4;
+                atomicAdd(&S.dW2[i0][col], c[0]);
+                atomicAdd(&S.dW2[i0][col + 1], c[1]);
+                atomicAdd(&S.dW2[i0 + 8][col], c[2]);
+                atomicAdd(&S.dW2[i0 + 8][col + 1], c[3]);
+            }
+        }
+        // 7. dH1 = G2 W2^T, g1 = dH1 [h1 > 0]; db1
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kt = 0; kt < 4; kt++) {
+                const int k0 = kt * 16 + 2 * t4;
+                mma_bf16(c, ld_pair(&S.g2[warp][g][k0]), ld_pair(&S.g2[warp][g + 8][k0]),
+                         ld_pair(&S.g2[warp][g][k0 + 8]), ld_pair(&S.g2[warp][g + 8][k0 + 8]),
+                         ti->w2tf[kt][nt][lane]);
+            }
+            const int col = nt * 8 + 2 * t4;
+            const float m00 = __bfloat162float(S.h1[warp][g][col]) > 0.f ? c[0] : 0.f;
+            const float m01 = __bfloat162float(S.h1[warp][g][col + 1]) > 0.f ? c[1] : 0.f;
+            const float m10 = __bfloat162float(S.h1[warp][g + 8][col]) > 0.f ? c[2] : 0.f;
+            const float m11 = __bfloat162float(S.h1[warp][g + 8][col + 1]) > 0.f ? c[3] : 0.f;
+            S.g1[warp][g][col] = __float2bfloat16_rn(m00);
+            S.g1[warp][g][col + 1] = __float2bfloat16_rn(m01);
+            S.g1[warp][g + 8][col] = __float2bfloat16_rn(m10);
+            S.g1[warp][g + 8][col + 1] = __float2bfloat16_rn(m11);
+            float bl = m00 + m10, bh = m01 + m11;
+#pragma unroll
+            for (int o = 4; o < 32; o <<= 1) {
+                bl += __shfl_xor_sync(0xFFFFFFFFu, bl, o);
+                bh += __shfl_xor_sync(0xFFFFFFFFu, bh, o);
+            }
+            if (g == 0) {
+                atomicAdd(&S.db1[col], bl);
+                atomicAdd(&S.db1[col + 1], bh);
+            }
+        }
+        __syncwarp();
+        // 8. dW1 += X^T G1: M = 16 features (8 used), N = 64, K = 16 rows
+        {
+            const uint32_t x_a0 = pair_of(S.xs[warp][2 * t4][g], S.xs[warp][2 * t4 + 1][g]);
+            const uint32_t x_a1 = pair_of(S.xs[warp][2 * t4][g + 8], S.xs[warp][2 * t4 + 1][g + 8]);
+            const uint32_t x_a2 = pair_of(S.xs[warp][2 * t4 + 8][g], S.xs[warp][2 * t4 + 9][g]);
+            const uint32_t x_a3 = pair_of(S.xs[warp][2 * t4 + 8][g + 8], S.xs[warp][2 * t4 + 9][g + 8]);
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++) {
+                const int j = nt * 8 + g;
+                const uint2 bb = make_uint2(pair_of(S.g1[warp][2 * t4][j], S.g1[warp][2 * t4 + 1][j]),
+                                            pair_of(S.g1[warp][2 * t4 + 8][j], S.g1[warp][2 * t4 + 9][j]));
+                float c[4] = {0.f, 0.f, 0.f, 0.f};
+                mma_bf16(c, x_a0, x_a1, x_a2, x_a3, bb);
+                const int col = nt * 8 + 2 * t4;
+                if (g < kMacIn) {  // rows g + 8 are padding features
+                    atomicAdd(&S.dW1[g][col], c[0]);
+                    atomicAdd(&S.dW1[g][col + 1], c[1]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kMacIn * kMacHid; e += blockDim.x)
+        atomicAdd(&grad[kMacW1 + e], (&S.dW1[0][0])[e]);
+    for (int e = threadIdx.x; e < kMacHid * kMacHid; e += blockDim.x)
+        atomicAdd(&grad[kMacW2 + e], (&S.dW2[0][0])[e]);
+    for (int e = threadIdx.x; e < kMacHid; e += blockDim.x) {
+        atomicAdd(&grad[kMacB1 + e], S.db1[e]);
+        atomicAdd(&grad[kMacB2 + e], S.db2[e]);
+        atomicAdd(&grad[kMacW3 + e], S.dw3[e]);
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&grad[kMacB3], S.db3);
+        atomicAdd(loss, S.loss);
+    }
+}
+
+__global__ void k_mac_adam(float* __restrict__ P, const float* __restrict__ G, float* __restrict__ m,
+                           float* __restrict__ v, int n, float lr, float b1, float b2,
+                           float c1, float c2, float eps) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = G[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    P[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order, int row0,
+              int nrows, const MacDev* w, const MacTrainImage* ti, float* grad, float* loss,
+              int sms) {
+    cudaMemsetAsync(grad, 0, sizeof(float) * kMacParams, st);
+    if (nrows <= 0) return;
+    const int tiles = (nrows + 15) / 16;
+    const int blocks = min(ceil_div(tiles, kTrainWarps), sms * 4);
+    k_mac_train<<<blocks, kTrainWarps * 32, 0, st>>>(X, Y, order, row0, nrows, w, ti,
+                                                      1.f / (float)nrows, grad, loss);
+}
+
+void mac_adam(cudaStream_t st, float* P, const float* G, float* m, float* v, int step, float lr) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    k_mac_adam<<<ceil_div(kMacParams, 256), 256, 0, st>>>(P, G, m, v, kMacParams, lr, b1, b2, c1,
+                                                            c2, 1e-8f);
+}
+
+// ---- prediction (the walk's inference routine on given feature rows) -------
+
+__global__ void k_mac_predict(const float* __restrict__ X, int n, const MacDev* __restrict__ w,
+                              float* __restrict__ out) {
+    __shared__ uint32_t xs[4][32 * 4];
+    __shared__ float ys[4][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r0 = (blockIdx.x * 4 + warp) * 32;
+    const int r = r0 + lane;
+    float f[kMacIn];
+    for (int k = 0; k < kMacIn; k++)
+        f[k] = r < n ? (X[(size_t)r * kMacIn + k] - w->mean[k]) * w->inv_std[k] : 0.f;
+    for (int k = 0; k < kMacIn; k += 2) xs[warp][lane * 4 + k / 2] = pack_bf16(f[k], f[k + 1]);
+    __syncwarp();
+    mac_mlp_warp(w, xs[warp], ys[warp], 32);
+    if (r < n) out[r] = ys[warp][lane] * w->y_std + w->y_mean;
+}
+
+void mac_predict(cudaStream_t st, const float* X, int n, const MacDev* w, float* out) {
+    if (n > 0) k_mac_predict<<<ceil_div(n, 128), 128, 0, st>>>(X, n, w, out);
+}
+
+}  // namespace nb

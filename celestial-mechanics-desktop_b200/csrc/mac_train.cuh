@@ -1,0 +1,30 @@
+// mac_train.cuh - training-side pieces of the learned MAC.
+#pragma once
+#include "mac.cuh"
+#include "tree.cuh"
+
+namespace nb {
+
+// Transposed layer-2 weights as B fragments, for the activation gradient
+// G2 W2^T of the backward pass.
+struct MacTrainImage {
+    uint2 w2tf[4][8][32];
+};
+
+// Normalisation block: 8 feature means, 8 feature stds, target mean, target std.
+constexpr int kMacNorm = 2 * kMacIn + 2;
+
+void mac_targets(cudaStream_t st, int nrec, const MacRecord* rec, const double4* sbody,
+                 const TreeBufs& t, double eps, float* X, float* Y, int* n_out, int out_off,
+                 int out_cap);
+void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w, MacTrainImage* ti);
+// Gradient of the mean squared error of rows order[row0 .. row0+nrows) into
+// grad (kMacParams floats, overwritten); the sum of squared errors is added
+// to *loss.
+void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order, int row0,
+              int nrows, const MacDev* w, const MacTrainImage* ti, float* grad, float* loss,
+              int sms);
+void mac_adam(cudaStream_t st, float* P, const float* G, float* m, float* v, int step, float lr);
+void mac_predict(cudaStream_t st, const float* X, int n, const MacDev* w, float* out);
+
+}  // namespace nb

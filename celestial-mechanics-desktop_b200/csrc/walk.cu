@@ -32,6 +32,17 @@ constexpr int kPartCap = 128;
 constexpr int kWarpFloats = kCellCap * 10 + kPartCap * 4 + kPartCap * 2 + kPartCap;
 constexpr int kWalkSmem = kWalkWarps * kWarpFloats * 4;
 constexpr int kMaxWalkRounds = 1 << 22;
+constexpr int kMacGeometric = 0, kMacHarvest = 1, kMacLearned = 2;
+// blocks per SM the learned walk is compiled for (2: 128 registers, no
+// spills; 3: 80 registers)
+#ifndef NB_WALK_MAC_BLOCKS
+#define NB_WALK_MAC_BLOCKS 2
+#endif
+// learned variant: + per warp 32 staged rows (4 words), 32 outputs and 32
+// pending node ids; three blocks still fit the SM's 228 KB
+constexpr int kMacWarpWords = 32 * 4 + 32 + 32;
+constexpr int kWalkSmemMac = kWalkSmem + kWalkWarps * kMacWarpWords * 4;
+static_assert(3 * (kWalkSmemMac + 1024) <= 228 * 1024, "three walk blocks per SM");
 
 __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     float y = x - c;
@@ -43,8 +54,14 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
 // GUARD (softening 0 only): 1/r is taken as 0 at r = 0, so a body's own entry
 // in its particle list adds 0 instead of 0 * inf.  With softening > 0 the
 // own entry has r^2 = eps^2 and dx = dy = dz = 0, which adds exactly 0.
-template <bool QUAD, bool SHELL, bool POT, bool GUARD>
-__global__ void __launch_bounds__(kWalkThreads, 3) k_walk_group(WalkArgs a) {
+// MAC selects the acceptance test: kMacGeometric (4h^2 < theta^2 d^2);
+// kMacHarvest (geometric at theta, and every candidate of a sampled group
+// with theta <= 2h/d < theta_hi is recorded for training); kMacLearned
+// (geometric below theta, open at or above theta_hi, the network decides in
+// between).
+template <bool QUAD, bool SHELL, bool POT, bool GUARD, int MAC>
+__global__ void __launch_bounds__(kWalkThreads, MAC == kMacLearned ? NB_WALK_MAC_BLOCKS : 3)
+k_walk_group(WalkArgs a) {
     extern __shared__ __align__(16) float s_walk[];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -59,7 +76,18 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk_group(WalkArgs a) {
     const float eps2 = (float)a.eps2;
     const float theta2 = (float)a.theta2;
     const int ngroups = *a.n_groups;
-    unsigned long long cnt_cell = 0, cnt_body = 0;
+    unsigned long long cnt_cell = 0, cnt_body = 0, cnt_mlp = 0;
+    // learned MAC: the network is read through L1 from global memory (11 KB,
+    // shared by every block of the SM), rows are staged per warp in shared
+    const MacDev* __restrict__ wmac = a.mac;
+    uint32_t* xs = nullptr;
+    float* ys = nullptr;
+    int* pend = nullptr;
+    if (MAC == kMacLearned) {
+        xs = (uint32_t*)(s_walk + kWalkWarps * kWarpFloats) + warp * kMacWarpWords;
+        ys = (float*)(xs + 32 * 4);
+        pend = (int*)(ys + 32);
+    }
 
     for (;;) {
         int g = 0;
@@ -85,6 +113,28 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk_group(WalkArgs a) {
         const float ghy = (float)(0.5 * (mxy - mny)) * 1.000001f + 1e-30f;
         const float ghz = (float)(0.5 * (mxz - mnz)) * 1.000001f + 1e-30f;
         const float bx = (float)(b.x - gcx), by = (float)(b.y - gcy), bz = (float)(b.z - gcz);
+        // smallest / largest |a| of the group's bodies (previous step), and
+        // whether this group's candidates are recorded (harvest)
+        float a_min = 0.f, a_max = 0.f, r_grp = 0.f;
+        bool sampled = false;
+        if (MAC != kMacGeometric) {
+            const float am = a.samag[valid ? s : grp.x];
+            a_min = am;
+            a_max = am;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a_min = fminf(a_min, __shfl_xor_sync(FULL, a_min, o));
+                a_max = fmaxf(a_max, __shfl_xor_sync(FULL, a_max, o));
+            }
+            r_grp = fmaxf(ghx, fmaxf(ghy, ghz));
+            if (MAC == kMacHarvest) {
+                unsigned hsh = (unsigned)grp.x * 2654435761u ^ (unsigned)a.mac_seed;
+                hsh ^= hsh >> 15;
+                hsh *= 2246822519u;
+                hsh ^= hsh >> 13;
+                sampled = (hsh & 0xFFFFu) < a.mac_sample;
+            }
+        }
 
         float sax = 0.f, say = 0.f, saz = 0.f, cax = 0.f, cay = 0.f, caz = 0.f;
         float spot = 0.f, cpot = 0.f;
@@ -169,25 +219,129 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk_group(WalkArgs a) {
         int sp = 1;
         if (lane == 0) stk[0] = 0;
         __syncwarp();
+        // One candidate node per lane, decided: accepted cells -> cell list,
+        // children of opened nodes -> stack, bodies of leaves -> particle list.
+        auto emit = [&](int node, bool take_cell, bool is_leaf, bool open, int4 lk, float rx,
+                        float ry, float rz, float mass) {
+            // 1. accepted cells -> cell list
+            const unsigned mcell = __ballot_sync(FULL, take_cell);
+            if (mcell) {
+                const int k = __popc(mcell);
+                if (nc + k > kCellCap) flush_cells();
+                if (take_cell) {
+                    const int cs = nc + __popc(mcell & lanemask_lt());
+                    c0[cs] = make_float4(rx, ry, rz, mass);
+                    if (QUAD) {
+                        const float4 q = a.t.q0[node];  // Qxx, Qyy, Qxy, Qxz
+                        c1[cs] = make_float4(q.x, q.y, -(q.x + q.y), q.z);
+                        c2[cs] = make_float2(q.w, a.t.q1[node].x);
+                    }
+                }
+                nc += k;
+                __syncwarp();
+            }
+            // 2. children of opened nodes -> pushed on the stack
+            const int nch = open ? lk.y : 0;
+            const int inc = warp_incl_scan(nch);
+            const int tot = __shfl_sync(FULL, inc, 31);
+            if (tot > 0) {
+                if (sp + tot > a.front_cap) {
+                    if (lane == 0) dev_flag(a.err, kErrOverflow);
+                } else {
+                    for (int k = 0; k < nch; k++) stk[sp + inc - nch + k] = lk.x + k;
+                    sp += tot;
+                }
+                __syncwarp();
+            }
+            // 3. bodies of leaves that were not accepted -> particle list
+            const int cb = is_leaf ? lk.w : 0;
+            const int incl = warp_incl_scan(cb);
+            const int T = __shfl_sync(FULL, incl, 31);
+            for (int t0 = 0; t0 < T; t0 += 32) {
+                if (np + 32 > kPartCap) flush_parts();
+                const int t = t0 + lane;
+                int pos = 0;  // first lane whose inclusive count exceeds t
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int v = __shfl_sync(FULL, incl, pos + step - 1);
+                    if (v <= t) pos += step;
+                }
+                const int ofirst = __shfl_sync(FULL, lk.z, pos);
+                const int oexcl = __shfl_sync(FULL, incl - cb, pos);
+                const int take = min(32, T - t0);
+                if (lane < take) {
+                    const int bi = ofirst + (t - oexcl);
+                    const double4 q = a.sbody[bi];
+                    p0[np + lane] = make_float4((float)(q.x - gcx), (float)(q.y - gcy),
+                                                (float)(q.z - gcz), (float)q.w);
+                    if (SHELL) {
+                        const float R = a.srad[bi];
+                        const float R2 = R * R;
+                        const float id = rsqrtf(R2 + eps2);
+                        p1[np + lane] = make_float2(R > 0.f ? R2 : 0.f, (float)q.w * id * id * id);
+                    }
+                    if (POT) p2[np + lane] = bi;
+                }
+                np += take;
+                __syncwarp();
+            }
+        };
+        // Learned MAC: candidates the screen leaves undecided wait in the
+        // pending list (node ids in pend, normalised features in xs); the
+        // network decides a full list, or whatever is pending when the stack
+        // runs dry, in one call, and the decisions are emitted then.
+        int npend = 0;
+        auto flush_pending = [&]() {
+            __syncwarp();
+            mac_mlp_warp(wmac, xs, ys, npend);
+            cnt_mlp += npend;
+            const bool mine = lane < npend;
+            const int pn = mine ? pend[lane] : -1;
+            int4 plk = make_int4(0, 0, 0, 0);
+            float prx = 0.f, pry = 0.f, prz = 0.f, pm = 0.f;
+            bool tc = false, lf = false, op = false;
+            if (mine) {
+                plk = a.t.link[pn];
+                const double4 cm = a.t.com[pn];
+                prx = (float)(cm.x - gcx);
+                pry = (float)(cm.y - gcy);
+                prz = (float)(cm.z - gcz);
+                pm = (float)cm.w;
+                tc = ys[lane] < a.mac_budget;
+                if (!tc) {
+                    if (plk.y == 0) lf = true;
+                    else op = true;
+                }
+            }
+            npend = 0;
+            __syncwarp();
+            emit(pn, tc, lf, op, plk, prx, pry, prz, pm);
+        };
         int rounds = 0;
-        while (sp > 0) {
+        while (sp > 0 || (MAC == kMacLearned && npend > 0)) {
             if (++rounds > kMaxWalkRounds) {
                 if (lane == 0) dev_flag(a.err, kErrOverflow);
                 break;
+            }
+            if (MAC == kMacLearned && sp == 0) {
+                flush_pending();
+                continue;
             }
             {
                 const int take = min(32, sp);
                 const int node = (lane < take) ? stk[sp - take + lane] : -1;
                 sp -= take;
                 __syncwarp();  // every lane holds its node before the pushes below
-                bool take_cell = false, is_leaf = false, open = false;
+                bool take_cell = false, is_leaf = false, open = false, in_band = false;
                 int4 lk = make_int4(0, 0, 0, 0);
-                float rx = 0.f, ry = 0.f, rz = 0.f, mass = 0.f;
+                float rx = 0.f, ry = 0.f, rz = 0.f, mass = 0.f, half = 0.f, d2 = 0.f;
+                bool live = false;
                 if (node >= 0) {
                     lk = a.t.link[node];
                     const double4 cm = a.t.com[node];
                     if (cm.w > 0.0) {
-                        const float half = a.t.q1[node].y;
+                        live = true;
+                        half = a.t.q1[node].y;
                         rx = (float)(cm.x - gcx);
                         ry = (float)(cm.y - gcy);
                         rz = (float)(cm.z - gcz);
@@ -195,76 +349,88 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk_group(WalkArgs a) {
                         const float dx = fmaxf(fabsf(rx) - ghx, 0.f);
                         const float dy = fmaxf(fabsf(ry) - ghy, 0.f);
                         const float dz = fmaxf(fabsf(rz) - ghz, 0.f);
-                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        take_cell = d2 > 0.f && 4.f * half * half < theta2 * d2;
-                        if (!take_cell) {
-                            if (lk.y == 0) is_leaf = true;
-                            else open = true;
-                        }
+                        d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float s2 = 4.f * half * half;
+                        take_cell = d2 > 0.f && s2 < theta2 * d2;
+                        if (MAC != kMacGeometric)
+                            in_band = d2 > 0.f && !take_cell && s2 < a.mac_theta_hi2 * d2;
                     }
                 }
-                // 1. accepted cells -> cell list
-                const unsigned mcell = __ballot_sync(FULL, take_cell);
-                if (mcell) {
-                    const int k = __popc(mcell);
-                    if (nc + k > kCellCap) flush_cells();
-                    if (take_cell) {
-                        const int cs = nc + __popc(mcell & lanemask_lt());
-                        c0[cs] = make_float4(rx, ry, rz, mass);
-                        if (QUAD) {
-                            const float4 q = a.t.q0[node];  // Qxx, Qyy, Qxy, Qxz
-                            c1[cs] = make_float4(q.x, q.y, -(q.x + q.y), q.z);
-                            c2[cs] = make_float2(q.w, a.t.q1[node].x);
-                        }
-                    }
-                    nc += k;
-                    __syncwarp();
-                }
-                // 2. children of opened nodes -> pushed on the stack
-                const int nch = open ? lk.y : 0;
-                const int inc = warp_incl_scan(nch);
-                const int tot = __shfl_sync(FULL, inc, 31);
-                if (tot > 0) {
-                    if (sp + tot > a.front_cap) {
-                        if (lane == 0) dev_flag(a.err, kErrOverflow);
-                    } else {
-                        for (int k = 0; k < nch; k++) stk[sp + inc - nch + k] = lk.x + k;
-                        sp += tot;
-                    }
-                    __syncwarp();
-                }
-                // 3. bodies of leaves that were not accepted -> particle list
-                const int cb = is_leaf ? lk.w : 0;
-                const int incl = warp_incl_scan(cb);
-                const int T = __shfl_sync(FULL, incl, 31);
-                for (int t0 = 0; t0 < T; t0 += 32) {
-                    if (np + 32 > kPartCap) flush_parts();
-                    const int t = t0 + lane;
-                    int pos = 0;  // first lane whose inclusive count exceeds t
+                if (MAC == kMacLearned) {
+                    // In the band a cell of one body is exact and taken; a
+                    // linear screen fitted to the network decides the clear
+                    // cases; the network decides the rest.
+                    bool unsure = false;
+                    float f[kMacIn];
+                    if (in_band && lk.w == 1) {
+                        take_cell = true;
+                    } else if (in_band) {
+                        const float4 q = a.t.q0[node];
+                        const float qyz = a.t.q1[node].x, qzz = -(q.x + q.y);
+                        const float qn2 = q.x * q.x + q.y * q.y + qzz * qzz +
+                                          2.f * (q.z * q.z + q.w * q.w + qyz * qyz);
+                        mac_features(f, d2, half, mass, qn2, lk.w, r_grp, nvalid, a_min, a_max,
+                                     sqrtf(eps2));
+                        float yl = mac_ldf(&wmac->scr_b);
 #pragma unroll
-                    for (int step = 16; step >= 1; step >>= 1) {
-                        const int v = __shfl_sync(FULL, incl, pos + step - 1);
-                        if (v <= t) pos += step;
+                        for (int k = 0; k < kMacIn; k++) yl = fmaf(mac_ldf(&wmac->scr_w[k]), f[k], yl);
+                        const float mg = mac_ldf(&wmac->lin_margin);
+                        if (yl < a.mac_budget - mg) take_cell = true;
+                        else if (yl <= a.mac_budget + mg) unsure = true;
                     }
-                    const int ofirst = __shfl_sync(FULL, lk.z, pos);
-                    const int oexcl = __shfl_sync(FULL, incl - cb, pos);
-                    const int take = min(32, T - t0);
-                    if (lane < take) {
-                        const int bi = ofirst + (t - oexcl);
-                        const double4 q = a.sbody[bi];
-                        p0[np + lane] = make_float4((float)(q.x - gcx), (float)(q.y - gcy),
-                                                    (float)(q.z - gcz), (float)q.w);
-                        if (SHELL) {
-                            const float R = a.srad[bi];
-                            const float R2 = R * R;
-                            const float id = rsqrtf(R2 + eps2);
-                            p1[np + lane] = make_float2(R > 0.f ? R2 : 0.f, (float)q.w * id * id * id);
+                    const unsigned hard = __ballot_sync(FULL, unsure);
+                    if (hard) {
+                        const int nh = __popc(hard);
+                        if (npend + nh > 32) flush_pending();
+                        const int rank = npend + __popc(hard & lanemask_lt());
+                        if (unsure) {
+#pragma unroll
+                            for (int k = 0; k < kMacIn; k += 2)
+                                xs[rank * 4 + k / 2] = pack_bf16(
+                                    (f[k] - mac_ldf(&wmac->mean[k])) * mac_ldf(&wmac->inv_std[k]),
+                                    (f[k + 1] - mac_ldf(&wmac->mean[k + 1])) *
+                                        mac_ldf(&wmac->inv_std[k + 1]));
+                            pend[rank] = node;
+                            live = false;  // decided when the pending list is flushed
                         }
-                        if (POT) p2[np + lane] = bi;
+                        npend += nh;
+                        __syncwarp();
                     }
-                    np += take;
-                    __syncwarp();
                 }
+                if (MAC == kMacHarvest && sampled && in_band) {
+                    // record the pair: features and the group body nearest the COM
+                    float f[kMacIn];
+                    const float4 q = a.t.q0[node];
+                    const float qyz = a.t.q1[node].x, qzz = -(q.x + q.y);
+                    const float qn2 = q.x * q.x + q.y * q.y + qzz * qzz +
+                                      2.f * (q.z * q.z + q.w * q.w + qyz * qyz);
+                    mac_features(f, d2, half, mass, qn2, lk.w, r_grp, nvalid, a_min, a_max,
+                                 sqrtf(eps2));
+                    const double4 cm = a.t.com[node];
+                    int best = grp.x;
+                    double bd = 1e300;
+                    for (int j = grp.x; j < grp.x + nvalid; j++) {
+                        const double4 p = a.sbody[j];
+                        const double ex = p.x - cm.x, ey = p.y - cm.y, ez = p.z - cm.z;
+                        const double dd = ex * ex + ey * ey + ez * ez;
+                        if (dd < bd) { bd = dd; best = j; }
+                    }
+                    const int slot_r = atomicAdd(a.n_records, 1);
+                    if (slot_r < a.record_cap) {
+                        MacRecord r;
+                        for (int k = 0; k < kMacIn; k++) r.f[k] = f[k];
+                        r.node = node;
+                        r.body = best;
+                        r.a_min = a_min;
+                        r.pad = 0.f;
+                        a.records[slot_r] = r;
+                    }
+                }
+                if (live && !take_cell) {
+                    if (lk.y == 0) is_leaf = true;
+                    else open = true;
+                }
+                emit(node, take_cell, is_leaf, open, lk, rx, ry, rz, mass);
             }
         }
         if (nc) flush_cells();
@@ -290,6 +456,7 @@ __global__ void __launch_bounds__(kWalkThreads, 3) k_walk_group(WalkArgs a) {
     if (lane == 0 && a.counters) {
         atomicAdd(&a.counters[0], cnt_cell);
         atomicAdd(&a.counters[1], cnt_body);
+        if (MAC == kMacLearned) atomicAdd(&a.counters[3], cnt_mlp);
     }
 }
 
@@ -479,7 +646,8 @@ using WalkKernel = void (*)(WalkArgs);
 // The instantiated variants: (quad) x {plain, shell, potential} x (guard).
 static WalkKernel pick_walk(bool quad, bool shell, bool pot, bool guard) {
 #define NB_WALK_PICK(Q, S, P)                                            \
-    return guard ? k_walk_group<Q, S, P, true> : k_walk_group<Q, S, P, false>
+    return guard ? k_walk_group<Q, S, P, true, kMacGeometric>                \
+                 : k_walk_group<Q, S, P, false, kMacGeometric>
     if (pot) {
         if (quad) NB_WALK_PICK(true, false, true);
         NB_WALK_PICK(false, false, true);
@@ -499,11 +667,21 @@ void walk_init(int sms, WalkConfig& cfg) {
         cudaFuncSetAttribute((const void*)pick_walk(v & 1, shell, pot, v & 8),
                              cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
     }
+    cudaFuncSetAttribute((const void*)k_walk_group<true, false, false, false, kMacHarvest>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmem);
+    cudaFuncSetAttribute((const void*)k_walk_group<true, false, false, false, kMacLearned>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmemMac);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_group<true, false, false, false>,
-                                                  kWalkThreads, kWalkSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_walk_group<true, false, false, false, kMacGeometric>, kWalkThreads, kWalkSmem);
     if (per_sm < 1) per_sm = 1;
     cfg.blocks = sms * per_sm;
+    int per_sm_mac = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm_mac, k_walk_group<true, false, false, false, kMacLearned>, kWalkThreads,
+        kWalkSmemMac);
+    if (per_sm_mac < 1) per_sm_mac = 1;
+    cfg.blocks_mac = sms * (per_sm_mac < per_sm ? per_sm_mac : per_sm);
     cfg.front_cap = 16384;
 }
 
@@ -512,11 +690,21 @@ size_t walk_front_bytes(const WalkConfig& cfg) {
 }
 
 void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,
-                bool pot) {
+                bool pot, int mac) {
     if (a.n <= 0) return;
     a.front_cap = cfg.front_cap;
     find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack);
     cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
+    if (mac == kMacHarvest) {
+        k_walk_group<true, false, false, false, kMacHarvest>
+            <<<cfg.blocks, kWalkThreads, kWalkSmem, st>>>(a);
+        return;
+    }
+    if (mac == kMacLearned) {
+        k_walk_group<true, false, false, false, kMacLearned>
+            <<<cfg.blocks_mac, kWalkThreads, kWalkSmemMac, st>>>(a);
+        return;
+    }
     const WalkKernel k = pick_walk(quad, shell, pot, !(a.eps2 > 0.0));
     k<<<cfg.blocks, kWalkThreads, kWalkSmem, st>>>(a);
 }

@@ -1,6 +1,7 @@
 // walk.cuh - Barnes-Hut tree walks.
 #pragma once
 #include "common.cuh"
+#include "mac.cuh"
 #include "tree.cuh"
 
 namespace nb {
@@ -22,6 +23,16 @@ struct WalkArgs {
     int2* groups;               // walk groups: body_first, body_count (<= 32)
     int* n_groups;
     double pack;                // sibling packing box-growth limit (0: no packing)
+    // learned MAC / harvest
+    const float* samag;         // |a| of each sorted body from the previous step
+    const MacDev* mac;          // network image (learned mode)
+    float mac_theta_hi2;        // band upper edge, (2h/d)^2
+    float mac_budget;           // normalised log2 error budget (learned mode)
+    MacRecord* records;         // harvest output
+    int* n_records;
+    int record_cap;
+    unsigned mac_seed;          // harvest group sampling
+    unsigned mac_sample;        // groups kept per 65536
     unsigned* group_ctr;        // dynamic group counter (zeroed)
     unsigned long long* counters;  // [0] body-cell, [1] body-body interactions
     int* err;
@@ -29,6 +40,7 @@ struct WalkArgs {
 
 struct WalkConfig {
     int blocks;        // persistent grid size
+    int blocks_mac;    // persistent grid size of the learned-MAC walk
     int front_cap;
 };
 
@@ -40,8 +52,10 @@ void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n
                  int* n_groups, double pack);
 size_t walk_front_bytes(const WalkConfig& cfg);
 // Group walk, FP32 monopole(+quadrupole) on FP64-differenced coordinates.
+// mac: 0 geometric, 1 harvest, 2 learned (1 and 2 need quad, no shell, no
+// potential, softening > 0).
 void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,
-                bool pot);
+                bool pot, int mac = 0);
 // Per-body FP64 walk with the reference's MAC, monopole, child order.
 void walk_reference(cudaStream_t st, WalkArgs a, bool shell);
 

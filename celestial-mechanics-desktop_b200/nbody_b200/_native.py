@@ -46,10 +46,13 @@ PARAM_TIMING = 7
 PARAM_MAC_BUDGET = 8
 PARAM_GROUP_BODIES = 9
 PARAM_GROUP_PACK = 10
+PARAM_MAC_THETA_LO = 11
+PARAM_MAC_THETA_HI = 12
+PARAM_MAC_SCREEN_QUANTILE = 13
 # timings / counters
 T_BUILD, T_TRAVERSAL, T_TOTAL, T_SORT, T_TREE, T_COUNT = range(6)
 (C_CELL_INTERACTIONS, C_BODY_INTERACTIONS, C_NODES, C_ACTIVE, C_PAIRS, C_MERGES, C_OVERFLOWS, C_GROUPS,
- C_MAX_GROUP_WORK, C_COUNT) = range(10)
+ C_MAX_GROUP_WORK, C_MAC_EVALS, C_COUNT) = range(11)
 
 vp = C.c_void_p
 i32 = C.c_int32
@@ -80,7 +83,21 @@ _SIGS = {
                               P, P]),
     "nb_compact_indices": (i32, [vp, i32, P, P, P, P]),
     "nb_broad_phase": (i32, [vp, i32, P, P, P, P, P, P, i32, P, P, P]),
+    "nb_mac_harvest": (i32, [vp, i32, f64, u64, f64, P]),
+    "nb_mac_dataset": (i32, [vp, P, P, P]),
+    "nb_mac_clear": (i32, [vp]),
+    "nb_mac_train": (i32, [vp, i32, i32, f64, u64, P]),
+    "nb_mac_set_params": (i32, [vp, P, i32]),
+    "nb_mac_get_params": (i32, [vp, P, i32]),
+    "nb_mac_gradient": (i32, [vp, P, P, i32, P, P]),
+    "nb_mac_predict": (i32, [vp, P, i32, P]),
+    "nb_mac_fit_screen": (i32, [vp]),
+    "nb_mac_get_screen": (i32, [vp, P, i32]),
+    "nb_mac_set_screen": (i32, [vp, P, i32]),
 }
+MAC_PARAMS = 4801
+MAC_NORM = 18
+MAC_SCREEN = 10
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
     _f.restype = _res

@@ -210,6 +210,68 @@ class Engine:
         return lo[:k].copy(), hi[:k].copy()
 
 
+    # -- learned MAC ---------------------------------------------------------
+    def mac_harvest(self, max_records: int, sample_frac: float, seed: int, softening: float) -> int:
+        out = np.zeros(1, np.int32)
+        self._check(N.lib.nb_mac_harvest(self._h, int(max_records), float(sample_frac), int(seed),
+                                         float(softening), N.ptr(out)))
+        return int(out[0])
+
+    def mac_dataset(self):
+        n = np.zeros(1, np.int32)
+        self._check(N.lib.nb_mac_dataset(self._h, N.ptr(n), None, None))
+        X = np.empty((int(n[0]), 8), np.float32)
+        Y = np.empty(int(n[0]), np.float32)
+        if n[0]:
+            self._check(N.lib.nb_mac_dataset(self._h, N.ptr(n), N.ptr(X), N.ptr(Y)))
+        return X, Y
+
+    def mac_clear(self):
+        self._check(N.lib.nb_mac_clear(self._h))
+
+    def mac_train(self, epochs: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0):
+        losses = np.zeros(max(epochs, 1))
+        self._check(N.lib.nb_mac_train(self._h, int(epochs), int(batch), float(lr), int(seed),
+                                       N.ptr(losses)))
+        return losses[:epochs]
+
+    def mac_set_params(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, np.float32)
+        self._check(N.lib.nb_mac_set_params(self._h, N.ptr(p), len(p)))
+
+    def mac_get_params(self) -> np.ndarray:
+        p = np.empty(N.MAC_PARAMS + N.MAC_NORM, np.float32)
+        self._check(N.lib.nb_mac_get_params(self._h, N.ptr(p), len(p)))
+        return p
+
+    def mac_gradient(self, X, Y):
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.float32)
+        g = np.empty(N.MAC_PARAMS, np.float32)
+        loss = np.zeros(1)
+        self._check(N.lib.nb_mac_gradient(self._h, N.ptr(X), N.ptr(Y), len(Y), N.ptr(g),
+                                          N.ptr(loss)))
+        return g, float(loss[0])
+
+    def mac_predict(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.empty(len(X), np.float32)
+        self._check(N.lib.nb_mac_predict(self._h, N.ptr(X), len(X), N.ptr(y)))
+        return y
+
+    def mac_fit_screen(self):
+        self._check(N.lib.nb_mac_fit_screen(self._h))
+
+    def mac_get_screen(self) -> np.ndarray:
+        s = np.empty(N.MAC_SCREEN, np.float32)
+        self._check(N.lib.nb_mac_get_screen(self._h, N.ptr(s), len(s)))
+        return s
+
+    def mac_set_screen(self, screen):
+        s = np.ascontiguousarray(screen, np.float32)
+        self._check(N.lib.nb_mac_set_screen(self._h, N.ptr(s), len(s)))
+
+
 class B200PhysicsBackend:
     """IPhysicsComputeBackend + IGravityModelAwareBackend on the B200 engine.
 

@@ -71,14 +71,22 @@ enum nb_param {
     NB_PARAM_LEAF_CAPACITY = 2,    /* i32, bodies per leaf bucket of the walk tree, default 8  */
     NB_PARAM_MAX_MERGES_FRAME = 3, /* i32, default 64 (simulation_config.hpp:57)               */
     NB_PARAM_MAX_MERGES_BODY = 4,  /* i32, default 2  (simulation_config.hpp:58)               */
-    NB_PARAM_MIN_RADIUS = 5,       /* f64, density-model floor for merged radii, default 1e-10 */
+    NB_PARAM_MIN_RADIUS = 5,       /* f64, density-model floor for merged radii, default 1e-6
+                                      (engine/include/celestial/physics/density_model.hpp:12) */
     NB_PARAM_DENSITY_MERGE = 6,    /* i32, 1 = density-preserving merge radius (default 1)     */
     NB_PARAM_TIMING = 7,           /* i32, 1 = record per-stage CUDA events (default 1)        */
     NB_PARAM_MAC_BUDGET = 8,       /* f64, learned MAC: max predicted log10 rel. error         */
     NB_PARAM_GROUP_BODIES = 9,     /* i32, bodies per walk group (32)                          */
-    NB_PARAM_GROUP_PACK = 10       /* f64, pack sibling cells into one walk group while the
+    NB_PARAM_GROUP_PACK = 10,      /* f64, pack sibling cells into one walk group while the
                                       packed box is at most this many times the larger part's
                                       box; 0 = no packing (default 2.25)                       */
+    NB_PARAM_MAC_THETA_LO = 11,    /* f64, learned MAC: cells with 2h/d below this are accepted
+                                      geometrically (default 0.35)                            */
+    NB_PARAM_MAC_THETA_HI = 12,    /* f64, learned MAC: cells with 2h/d at or above this are
+                                      opened; in between the network decides (default 1.0)   */
+    NB_PARAM_MAC_SCREEN_QUANTILE = 13 /* f64, learned MAC: quantile of |network - screen| over
+                                      the training set that sets the linear screen's margin;
+                                      0 = no screen (default 0.9, used by the next fit)       */
 };
 
 /* Indices into nb_get_timings() output (milliseconds, CUDA events).
@@ -104,7 +112,8 @@ enum nb_counter {
     NB_C_OVERFLOWS = 6,             /* walk frontier overflows (non-zero means an error)    */
     NB_C_GROUPS = 7,                /* walk groups (warps' body sets), last evaluation       */
     NB_C_MAX_GROUP_WORK = 8,        /* longest interaction list of one group (load balance)  */
-    NB_C_COUNT = 9
+    NB_C_MAC_EVALS = 9,             /* learned MAC: (group, cell) rows the network evaluated */
+    NB_C_COUNT = 10
 };
 
 /* ---- lifetime -------------------------------------------------------- */
@@ -236,6 +245,60 @@ NB_API int32_t nb_broad_phase(nb_engine* h, int32_t n,
                               const double* radius, const uint8_t* active,
                               const uint8_t* collidable, int32_t max_pairs,
                               int32_t* pair_lo, int32_t* pair_hi, int32_t* n_pairs);
+
+/* ---- learned multipole acceptance criterion --------------------------- */
+/* No reference counterpart: these replace the geometric opening test
+ * (engine/src/cuda/gpu_tree.cu:567-569, BarnesHutBackend.cs:431-447) inside
+ * the band theta_lo <= 2h/d < theta_hi by an MLP 8-64-64-1 (BF16 tensor-core
+ * tiles, FP32 accumulate) that predicts log2 of the cell's monopole +
+ * quadrupole force error relative to the group's smallest |a|; the cell is
+ * accepted when the prediction is below NB_PARAM_MAC_BUDGET (log10).  Enable
+ * with NB_FLAG_LEARNED_MAC in nb_step / nb_compute_forces. */
+#define NB_MAC_PARAMS 4801  /* W1 8x64, b1 64, W2 64x64, b2 64, w3 64, b3 1 */
+#define NB_MAC_NORM 18      /* feature means[8], feature stds[8], target mean, target std */
+
+/* Harvest training samples from the device state: one Barnes-Hut force
+ * evaluation with the geometric test at theta_lo (it updates the state's
+ * accelerations) that records, for a `sample_frac` share of the walk groups,
+ * every candidate cell in the band with its exact FP64 error target.  Up to
+ * max_records records per call; samples are appended to the handle's
+ * training set (16,777,216 rows).  Needs an acceleration estimate from a
+ * previous force evaluation. */
+NB_API int32_t nb_mac_harvest(nb_engine* h, int32_t max_records, double sample_frac,
+                              uint64_t seed, double softening, int32_t* n_added);
+/* Size of the training set, and a copy (X: n x 8 features, Y: n targets;
+ * either may be NULL). */
+NB_API int32_t nb_mac_dataset(nb_engine* h, int32_t* n, float* X, float* Y);
+NB_API int32_t nb_mac_clear(nb_engine* h);
+/* Train on the handle's set with Adam (MSE on normalised log2 errors); the
+ * first call fixes the normalisation and initialises the weights from seed.
+ * loss_per_epoch (may be NULL) receives the mean normalised loss per epoch. */
+NB_API int32_t nb_mac_train(nb_engine* h, int32_t epochs, int32_t batch, double lr, uint64_t seed,
+                            double* loss_per_epoch);
+/* Parameters: NB_MAC_PARAMS weights followed by NB_MAC_NORM normalisation. */
+NB_API int32_t nb_mac_set_params(nb_engine* h, const float* params, int32_t n);
+NB_API int32_t nb_mac_get_params(nb_engine* h, float* params, int32_t n);
+/* Gradient (NB_MAC_PARAMS floats) of the mean squared error over the given
+ * rows with the current parameters, computed by the training kernel. */
+NB_API int32_t nb_mac_gradient(nb_engine* h, const float* X, const float* Y, int32_t n,
+                               float* grad, double* loss);
+/* Predictions (log2 error units) of the walk's inference routine. */
+NB_API int32_t nb_mac_predict(nb_engine* h, const float* X, int32_t n, float* y);
+
+/* Linear screen in front of the network: in the band the walk first forms
+ * s = w . x_norm + b (x_norm: features normalised as the network's input,
+ * s in normalised target units); s < budget - margin accepts, s > budget +
+ * margin opens, and only in between the network is evaluated.  Cells of one
+ * body are accepted without either (their monopole is exact).
+ * nb_mac_fit_screen fits w, b by least squares to the network's own
+ * predictions on the multi-body rows of the training set and sets margin to
+ * the NB_PARAM_MAC_SCREEN_QUANTILE quantile of the residuals; nb_mac_train
+ * calls it at the end, nb_mac_set_params switches the screen off (margin =
+ * +inf) until a fit or nb_mac_set_screen. */
+#define NB_MAC_SCREEN 10  /* w[8], b, margin */
+NB_API int32_t nb_mac_fit_screen(nb_engine* h);
+NB_API int32_t nb_mac_get_screen(nb_engine* h, float* screen, int32_t n);
+NB_API int32_t nb_mac_set_screen(nb_engine* h, const float* screen, int32_t n);
 
 #ifdef __cplusplus
 }
