@@ -1,12 +1,18 @@
 """Benchmark of the Barnes-Hut force path on one B200 per rank.
 
-Default workload (the headline configuration): Plummer sphere, N=1,048,576,
-scale radius 1 AU, total mass 1 Msun, seed 1; softening 1e-4, dt 1e-4;
-Barnes-Hut with the geometric MAC theta=0.5, monopole+quadrupole, FP64 state,
-FP32 pair forces.  A step is one velocity-Verlet step on device-resident
-state (kick-drift + bbox, keys, sort, tree, multipoles, walk, kick).
+Default workload: learned vs geometric multipole acceptance at a fixed force
+error on the N=1,048,576 Plummer sphere (scale radius 1 AU, total mass
+1 Msun, seed 1; softening 1e-4, dt 1e-4; monopole+quadrupole, FP64 state,
+FP32 pair forces).  The network is first trained on the GPU from engine runs
+of Plummer/Hernquist spheres (seeds 10-19); then the geometric theta and the
+learned budget are each set to the loosest value with rms relative force
+error <= 1e-3 against the FP64 direct sum, and both are timed, with the
+plain theta = 0.5 configuration beside them.  `value` is the learned MAC's
+steps/s.  A step is one velocity-Verlet step on device-resident state
+(kick-drift + bbox, keys, sort, tree, multipoles, walk, kick).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload bh1m|mac4m|ds1000|disk]
 
 N > 1 runs N independent replicas (the path does not shard across GPUs:
 one system per GPU), one process per GPU under torchrun; time is the max
@@ -145,9 +151,12 @@ def peaks():
     return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def walk_traffic_per_launch():
+def walk_traffic_per_launch(which: str | None = "geometric"):
     """DRAM bytes of one walk launch from the committed ncu summary, or None."""
-    f = ROOT / "profiles" / "k_walk_group_bh_plummer.md"
+    if which is None:
+        return None
+    f = ROOT / "profiles" / ("k_walk_group_bh_plummer.md" if which == "geometric" else
+                             "k_walk_group_learned_plummer.md")
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -204,127 +213,246 @@ def run_reference(args, ws, rank):
     }))
 
 
-def run_b200(args, ws, rank, local):
+TRAIN_SYSTEMS = [  # (generator, N, seed): the learned MAC's training runs
+    ("plummer", 65_536, 10), ("hernquist", 65_536, 11), ("plummer", 131_072, 12),
+    ("hernquist", 131_072, 13), ("plummer", 262_144, 14), ("hernquist", 262_144, 15),
+    ("plummer", 524_288, 16), ("hernquist", 524_288, 17), ("plummer", 1_048_576, 18),
+    ("hernquist", 1_048_576, 19)]
+TRAIN_ROWS = 10_000_000
+RMS_TARGET = 1e-3
+THETA_GRID = [round(0.5 + 0.025 * i, 3) for i in range(17)]          # 0.5 .. 0.9
+BUDGET_GRID = [round(-4.5 + 0.1 * i, 2) for i in range(21)]           # log10 budget -4.5 .. -2.5
+ERR_SAMPLES, ERR_SEED = 4096, 12345
+
+
+def train_learned_mac(eng, N, scenarios, log):
+    """Harvest (group, cell) samples from engine runs of Plummer and Hernquist
+    spheres (seeds 10-19, N = 65,536 .. 1,048,576) and train the network on
+    the GPU; returns a summary."""
+    from nbody_b200 import MODE_BARNES_HUT
+
+    t0 = time.perf_counter()
+    per = TRAIN_ROWS // len(TRAIN_SYSTEMS)
+    rows = []
+    for gen, n, seed in TRAIN_SYSTEMS:
+        if n > eng.capacity:
+            continue
+        b = getattr(scenarios, gen)(n, seed=seed)
+        eng.set_param(N.PARAM_THETA, 0.5)
+        eng.set_state(b, old_acc=False)
+        eng.step(1, 0.0, EPS, MODE_BARNES_HUT)  # |a| estimate for the features
+        # about 60 band candidates per body: sample the groups to land near `per`
+        frac = min(1.0, per / (60.0 * n))
+        rows.append(eng.mac_harvest(per * 2, frac, seed, EPS))
+    harvest_s = time.perf_counter() - t0
+    losses = eng.mac_train(6, 4096, 2e-3, seed=3)
+    log(f"learned MAC: {sum(rows)} rows in {harvest_s:.1f} s, losses {np.round(losses, 4)}")
+    return {"rows": int(sum(rows)), "systems": len(rows), "epochs": 6, "batch": 4096, "lr": 2e-3,
+            "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
+            "harvest_s": harvest_s, "total_s": time.perf_counter() - t0,
+            "screen_margin": float(eng.mac_get_screen()[-1])}
+
+
+def force_rms(eng, b, flags, mode_geo):
+    """rms relative force error of one force evaluation of `b` (positions as
+    given, |a| estimate from a geometric evaluation) against the FP64 direct
+    sum on sampled bodies."""
+    eng.set_state(b, old_acc=False)
+    eng.step(1, 0.0, EPS, mode_geo)
+    eng.step(1, 0.0, EPS, flags)
+    return eng.force_error(ERR_SAMPLES, ERR_SEED, EPS)[2]
+
+
+def calibrate(eng, b, N, param, grid, flags, mode_geo, log):
+    """Largest grid value whose rms error is <= RMS_TARGET (grid ascending in
+    error); returns (value, rms, scanned)."""
+    best, best_rms, scanned = None, None, []
+    for v in grid:
+        eng.set_param(param, v)
+        rms = force_rms(eng, b, flags, mode_geo)
+        scanned.append([v, rms])
+        if rms <= RMS_TARGET:
+            best, best_rms = v, rms
+        elif best is not None:
+            break
+    log(f"calibrated param {param}: {best} (rms {best_rms})")
+    eng.set_param(param, best if best is not None else grid[0])
+    return best, best_rms, scanned
+
+
+def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
+    """Warm-up then K device-resident steps bracketed by barrier +
+    synchronize and CUDA events on the engine's stream; the timed steps sit
+    in an NVTX range named `label` (ncu --nvtx-include "<label>/")."""
     import torch
 
-    from nbody_b200 import MODE_BARNES_HUT, Engine, scenarios
-    from nbody_b200 import _native as N
-
-    dev = local
-    torch.cuda.set_device(dev)
-    b = scenarios.plummer(args.n, 1.0, 1.0, seed=SEED)
-    eng = Engine(args.n, device=dev)
-    eng.set_param(N.PARAM_THETA, THETA)
-    flags = MODE_BARNES_HUT
-    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     eng.set_state(b, old_acc=False)
+    eng.step(1, 0.0, EPS, mode_geo)
     eng.step(max(args.warmup, 3), DT, EPS, flags)
     torch.cuda.synchronize(dev)
-
-    # ---- device-resident timed region ---------------------------------
     clocks = Clocks(dev)
     barrier(ws)
     torch.cuda.synchronize(dev)
     clocks.start()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push(label)
     t0.record(stream)
-    walk_ms, build_ms, sort_ms, tree_ms, inter, flops = 0.0, 0.0, 0.0, 0.0, 0, 0.0
+    acc = dict(walk=0.0, build=0.0, sort=0.0, tree=0.0, inter=0, flops=0.0, evals=0)
     for _ in range(args.steps):
         eng.step(1, DT, EPS, flags)
         tm = eng.timings()
         c = eng.counters()
-        walk_ms += tm[N.T_TRAVERSAL]
-        build_ms += tm[N.T_BUILD]
-        sort_ms += tm[N.T_SORT]
-        tree_ms += tm[N.T_TREE]
-        inter += int(c[N.C_CELL_INTERACTIONS] + c[N.C_BODY_INTERACTIONS])
-        flops += FLOPS_CELL_QUAD * c[N.C_CELL_INTERACTIONS] + FLOPS_BODY * c[N.C_BODY_INTERACTIONS]
+        acc["walk"] += tm[N.T_TRAVERSAL]
+        acc["build"] += tm[N.T_BUILD]
+        acc["sort"] += tm[N.T_SORT]
+        acc["tree"] += tm[N.T_TREE]
+        acc["inter"] += int(c[N.C_CELL_INTERACTIONS] + c[N.C_BODY_INTERACTIONS])
+        acc["flops"] += FLOPS_CELL_QUAD * c[N.C_CELL_INTERACTIONS] + FLOPS_BODY * c[N.C_BODY_INTERACTIONS]
+        acc["evals"] += int(c[N.C_MAC_EVALS])
     t1.record(stream)
     torch.cuda.synchronize(dev)
+    torch.cuda.nvtx.range_pop()
     barrier(ws)
     clk = clocks.stop()
-    ms = t0.elapsed_time(t1)
-    ms_max = max_over_ranks(ws, ms)
-    steps_total = sum_over_ranks(ws, args.steps)
-    value = steps_total / (ms_max / 1e3)
-    inter_total = sum_over_ranks(ws, inter)
+    ms = max_over_ranks(ws, t0.elapsed_time(t1))
+    err = eng.force_error(ERR_SAMPLES, ERR_SEED, EPS)
+    k = args.steps
+    out = {"steps_per_s": sum_over_ranks(ws, k) / (ms / 1e3), "ms_per_step": ms / k,
+           "interactions_per_s": sum_over_ranks(ws, acc["inter"]) / (ms / 1e3),
+           "interactions_per_step": acc["inter"] / k,
+           "force_error": {"mean": err[0], "max": err[1], "rms": err[2]},
+           "stage_ms": {s: acc[s] / k for s in ("build", "walk", "sort", "tree")},
+           "walk_flops_per_step": acc["flops"] / k, "network_rows_per_step": acc["evals"] / k,
+           "clocks": clk}
+    return out
 
-    # ---- force error of the last step against the FP64 direct sum -----
-    err = eng.force_error(4096, 12345, EPS)
 
-    # ---- end to end through the seam with host buffers -----------------
+def run_b200(args, ws, rank, local):
+    """Learned vs geometric MAC at a fixed force error on one system: the
+    network is trained on the GPU, the geometric theta and the learned budget
+    are each set to the loosest value whose rms relative force error against
+    the FP64 direct sum stays <= 1e-3, and both are timed; theta = 0.5 (the
+    plain Barnes-Hut configuration) is timed beside them."""
+    import torch
+
+    from nbody_b200 import FLAG_LEARNED_MAC, MODE_BARNES_HUT, Engine, scenarios
+    from nbody_b200 import _native as N
+
+    log = (lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
+    dev = local
+    torch.cuda.set_device(dev)
+    big = args.workload == "mac4m"
+    n = args.n if not big or args.n != N_BODIES else 4 * N_BODIES
+    b = (scenarios.hernquist(n, 1.0, 1.0, seed=4) if big else
+         scenarios.plummer(n, 1.0, 1.0, seed=SEED))
+    eng = Engine(max(n, N_BODIES), device=dev)
+    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
+    geo, learned = MODE_BARNES_HUT, MODE_BARNES_HUT | FLAG_LEARNED_MAC
+
+    train = train_learned_mac(eng, N, scenarios, log)
+    theta_g, rms_g, scan_g = calibrate(eng, b, N, N.PARAM_THETA, THETA_GRID, geo, geo, log)
+    budget, rms_l, scan_l = calibrate(eng, b, N, N.PARAM_MAC_BUDGET, BUDGET_GRID, learned, geo, log)
+
+    arm_l = timed_arm(eng, b, stream, args, ws, dev, learned, N, geo, "learned")
+    arm_g = timed_arm(eng, b, stream, args, ws, dev, geo, N, geo, "geometric")
+    eng.set_param(N.PARAM_THETA, THETA)
+    arm_05 = timed_arm(eng, b, stream, args, ws, dev, geo, N, geo, "theta_0_5")
+    eng.set_param(N.PARAM_THETA, theta_g)
+
+    # ---- end to end through the seam with host buffers (learned MAC) ----
     st, _ = eng.get_state()
-    n = st.n
+    nn = st.n
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     hp = [pin(st.px), pin(st.py), pin(st.pz), pin(st.mass), pin(st.active)]
-    out = [pin(np.empty(n)), pin(np.empty(n)), pin(np.empty(n))]
-    eng.compute_forces(*hp[:4], hp[4], EPS, flags, out=out)
+    out = [pin(np.empty(nn)), pin(np.empty(nn)), pin(np.empty(nn))]
+    # the learned MAC's |a| estimate is the handle's previous evaluation
+    eng.compute_forces(*hp[:4], hp[4], EPS, geo, out=out)
+    eng.compute_forces(*hp[:4], hp[4], EPS, learned, out=out)
     barrier(ws)
     torch.cuda.synchronize(dev)
     e0 = time.perf_counter()
     e_steps = max(1, args.steps)
     for _ in range(e_steps):
-        eng.compute_forces(*hp[:4], hp[4], EPS, flags, out=out)
+        eng.compute_forces(*hp[:4], hp[4], EPS, learned, out=out)
     e_s = max_over_ranks(ws, time.perf_counter() - e0)
     e2e_value = sum_over_ranks(ws, e_steps) / e_s
-    h2d = 4 * 8 * n + n
-    d2h = 3 * 8 * n
 
-    # ---- roofline of the dominant kernel (the walk) --------------------
+    # ---- roofline of the dominant kernel (the learned walk) -------------
     pk, pk_kind = peaks()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     fp32_peak = sms * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-    achieved = (flops / args.steps) / (walk_ms / args.steps / 1e3) / 1e12
-    traffic = walk_traffic_per_launch()
+    walk_s = arm_l["stage_ms"]["walk"] / 1e3
+    achieved = arm_l["walk_flops_per_step"] / walk_s / 1e12
+    clk = arm_l["clocks"]
 
     line = None
     if rank == 0:
         cpu = None
-        if ws == 1 and not args.no_cpu_baseline:
+        if ws == 1 and not args.no_cpu_baseline and not big:
             threads = os.cpu_count() or 1
             s, kind = reference_bh_seconds(b, threads)
             cpu = {"value": 1.0 / s, "unit": "steps/s", "cores": threads, "kind": kind,
                    "sample": "one full force evaluation of the same N=1,048,576 Plummer input "
                              "(reference BarnesHutSolver: serial tree build + parallel walk, "
                              "theta 0.5, monopole)"}
+        sort_s = arm_l["stage_ms"]["sort"] / 1e3
+        tree_s = arm_l["stage_ms"]["tree"] / 1e3
         line = {
-            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws,
-            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
+            "metric": METRIC, "value": arm_l["steps_per_s"], "unit": "steps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": arm_l["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded Plummer sphere, numpy PCG64)",
-            "config": {"workload": workload_name(args.n), "n": args.n, "theta": THETA, "eps": EPS,
-                       "dt": DT, "seed": SEED, "multipole": "monopole+quadrupole",
-                       "mac": "geometric", "state": "f64", "pair_forces": "f32",
+            "data": ("synthetic (seeded Hernquist sphere, numpy PCG64)" if big else
+                     "synthetic (seeded Plummer sphere, numpy PCG64)"),
+            "config": {"workload": ("learned_mac_hernquist_4m" if big else workload_name(n)),
+                       "n": n, "eps": EPS, "dt": DT, "seed": 4 if big else SEED,
+                       "force_error_target": f"rms <= {RMS_TARGET} vs FP64 direct sum "
+                                             f"({ERR_SAMPLES} sampled bodies)",
+                       "mac": "learned (MLP 8-64-64-1, BF16 tensor cores)",
+                       "learned_budget_log10": budget, "theta_band": [0.35, 1.0],
+                       "multipole": "monopole+quadrupole", "state": "f64", "pair_forces": "f32",
                        "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (state, sort and tree buffers > 300 MB)"},
-            "interactions_per_s": inter_total / (ms_max / 1e3),
-            "interactions_per_step": inter / args.steps,
-            "force_error": {"mean": err[0], "max": err[1], "rms": err[2],
-                            "vs": "FP64 direct sum, 4096 uniformly sampled bodies"},
-            "stage_ms": {"build": build_ms / args.steps, "walk": walk_ms / args.steps,
-                         "sort": sort_ms / args.steps, "tree": tree_ms / args.steps},
+            "interactions_per_s": arm_l["interactions_per_s"],
+            "interactions_per_step": arm_l["interactions_per_step"],
+            "force_error": dict(arm_l["force_error"], vs=f"FP64 direct sum, {ERR_SAMPLES} "
+                                                        "uniformly sampled bodies, last step"),
+            "learned": {"budget_log10": budget, "calibration_rms": rms_l,
+                        "network_rows_per_step": arm_l["network_rows_per_step"],
+                        "stage_ms": arm_l["stage_ms"], "training": train, "scan": scan_l},
+            "geometric_same_error": {k: arm_g[k] for k in ("steps_per_s", "ms_per_step",
+                                                           "interactions_per_s",
+                                                           "interactions_per_step",
+                                                           "force_error", "stage_ms")}
+                                    | {"theta": theta_g, "calibration_rms": rms_g, "scan": scan_g},
+            "learned_over_geometric_steps": arm_l["steps_per_s"] / arm_g["steps_per_s"],
+            "geometric_theta_0_5": {k: arm_05[k] for k in ("steps_per_s", "ms_per_step",
+                                                           "interactions_per_s",
+                                                           "force_error", "stage_ms")},
             "stage_gbs": {
-                "sort": SORT_BYTES_PER_BODY * args.n / (sort_ms / args.steps / 1e3) / 1e9,
-                "tree": TREE_BYTES_PER_BODY * args.n / (tree_ms / args.steps / 1e3) / 1e9,
+                "sort": SORT_BYTES_PER_BODY * n / sort_s / 1e9,
+                "tree": TREE_BYTES_PER_BODY * n / tree_s / 1e9,
                 "hbm_peak": pk.get("hbm_gbs", 6458.1),
                 "bytes_per_body": {"sort": SORT_BYTES_PER_BODY, "tree": TREE_BYTES_PER_BODY},
                 "note": "sort = kick-drift+bbox, keys+histograms, 8 radix passes, gather; "
-                        "tree = radix tree, octree mark/scan/emit, multipoles; at N=2^20 the "
-                        "sort buffers (24 MB) stay in the 126 MB L2"},
+                        "tree = radix tree, octree mark/scan/emit, multipoles"},
             "gpu_launches": None,
-            "roofline": {"bound": "fp32", "kernel": "k_walk_group", "achieved": achieved,
-                         "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+            "roofline": {"bound": "fp32", "kernel": "k_walk_group (learned MAC)",
+                         "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak,
                          "peak_kind": f"SMs x 128 x 2 x sm_max_mhz ({pk_kind} max clock)",
                          "frac_at_median_clock": (achieved / (fp32_peak * clk["sm_mhz"] /
                                                               pk.get("sm_max_mhz", 1965.0))
                                                   if clk.get("sm_mhz") else None),
-                         "traffic": traffic},
+                         "network_tflops": 9344 * arm_l["network_rows_per_step"] / walk_s / 1e12,
+                         "traffic": walk_traffic_per_launch("learned" if not big else None)},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h,
-                    "path": "nb_compute_forces (IPhysicsComputeBackend.ComputeForces) on pinned "
-                            "host arrays: H2D pos+mass+active, BH force evaluation, D2H acc"},
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 4 * 8 * nn + nn,
+                    "d2h_bytes_per_step": 3 * 8 * nn,
+                    "path": "nb_compute_forces (IPhysicsComputeBackend.ComputeForces) with the "
+                            "learned MAC on pinned host arrays: H2D pos+mass+active, force "
+                            "evaluation, D2H acc"},
             "clocks": clk,
         }
     eng.close()
@@ -370,7 +498,7 @@ def run_ds1000(args, ws, rank, local):
 
     dev = local
     torch.cuda.set_device(dev)
-    n, eps, dt, steps = 1000, 1e-4, 1e-3, args.steps if args.steps != 20 else 10_000
+    n, eps, dt, steps = 1000, 1e-4, 1e-3, args.steps
     b = scenarios.plummer(n, 1.0, 1.0, seed=0)
     eng = Engine(n, device=dev)
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
@@ -424,7 +552,7 @@ def run_disk(args, ws, rank, local):
     dev = local
     torch.cuda.set_device(dev)
     n, eps, dt = 262_144, 1e-4, 1e-3
-    steps = args.steps if args.steps != 20 else 1000
+    steps = args.steps
     # radius scale 30: calibrated so ~1 % of the bodies merge per 1000 steps
     # (a scale of 1000 makes every body overlap ~3 others at the start)
     d = scenarios.collisional_disk(n, seed=2, radius_scale=DISK_RADIUS_SCALE)
@@ -462,16 +590,21 @@ def run_disk(args, ws, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: bh1m 100, mac4m 50, ds1000 10,000, disk 1000)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=N_BODIES,
                     help="bodies (default the 1,048,576-body workload; smaller for profiling)")
-    ap.add_argument("--workload", default="bh1m", choices=["bh1m", "ds1000", "disk"],
-                    help="bh1m: the headline Barnes-Hut line; ds1000: FP64 direct sum N=1000, "
-                         "10k steps; disk: collisional disk N=262,145, 1000 steps")
+    ap.add_argument("--workload", default="bh1m", choices=["bh1m", "mac4m", "ds1000", "disk"],
+                    help="bh1m: the headline line, learned vs geometric MAC at rms <= 1e-3 on "
+                         "the N=1,048,576 Plummer sphere; mac4m: the same on the N=4,194,304 "
+                         "Hernquist sphere; ds1000: FP64 direct sum N=1000, 10k steps; disk: "
+                         "collisional disk N=262,145, 1000 steps")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = {"bh1m": 100, "mac4m": 50, "ds1000": 10_000, "disk": 1000}[args.workload]
     ws, rank, local = dist_setup()
     try:
         if args.impl == "reference":
