@@ -8,6 +8,11 @@
 
 namespace nb {
 
+// Batched systems: keys = system (12 bits, bits 62..51) | 3 x 17-bit Morton.
+constexpr int kEnsSysShift = 51;
+constexpr int kEnsSysBits = 12;
+constexpr int kEnsAxisBits = 17;
+
 constexpr int kSMs = 148;            // B200; the launch code queries the real count
 constexpr int kWarp = 32;
 constexpr uint64_t kInactiveKey = ~0ull;

@@ -279,14 +279,22 @@ __device__ __forceinline__ void quad_add(double q[6], double m, double dx, doubl
     q[4] += m * (3.0 * dy * dz);
 }
 
+// sys_half16: batched systems (keys carry the system in their top bits): the
+// half-size of each system's cube times 2^4, the half-size its level-0 cell
+// would have; null for one system in `cube`.
 __global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody,
-                           const float* __restrict__ srad, const double* __restrict__ cube) {
+                           const float* __restrict__ srad, const double* __restrict__ cube,
+                           const uint64_t* __restrict__ skeys,
+                           const double* __restrict__ sys_half16) {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
     int nn = *t.n_nodes;
     if (w >= nn) return;
     int4 lk = t.link[w];
     if (lk.y != 0) return;  // internal nodes are reduced by their last child
-    const double root_half = cube[3];
+    auto root_half_of = [&](int first) {
+        return sys_half16 ? sys_half16[skeys[first] >> kEnsSysShift] : cube[3];
+    };
+    double root_half = root_half_of(lk.z);
     {
         // leaf: moments straight from its bodies
         double M = 0, sx = 0, sy = 0, sz = 0;
@@ -354,6 +362,7 @@ __global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody
         }
         t.com[p] = make_double4(cx, cy, cz, M);
         t.q0[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+        root_half = root_half_of(pl.z);
         t.q1[p] = make_float4((float)q[4], (float)ldexp(root_half, -__ldcg(&t.level[p])), rmax,
                               0.f);
         pb = __ldcg(&t.parent_bin[p]);
@@ -362,7 +371,7 @@ __global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody
 
 void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys,
                 const double4* sbody, const float* srad, const double* cube, int leaf_cap,
-                int* err) {
+                int* err, const double* sys_half16) {
     (void)err;
     if (n <= 0) {
         cudaMemsetAsync(t.n_nodes, 0, sizeof(int), st);
@@ -378,7 +387,7 @@ void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys
     if (m > 0) k_octree_base<<<nblk, kMarkThreads, 0, st>>>(n, t);
     k_octree_emit<<<ceil_div(m > 0 ? m : 1, 256), 256, 0, st>>>(n, t, leaf_cap);
     cudaMemsetAsync(t.counter, 0, sizeof(int) * 2 * (size_t)n, st);
-    k_multipole<<<ceil_div(2 * n, 256), 256, 0, st>>>(n, t, sbody, srad, cube);
+    k_multipole<<<ceil_div(2 * n, 256), 256, 0, st>>>(n, t, sbody, srad, cube, skeys, sys_half16);
 }
 
 }  // namespace nb

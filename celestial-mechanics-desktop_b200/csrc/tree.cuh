@@ -35,9 +35,12 @@ void tree_carve(TreeBufs& t, void* base, int capacity);
 
 // Build the walk tree over n sorted keys (already in sorted order) with the
 // bodies sorted in `sbody` (x, y, z, m).  cube: device (cx, cy, cz, half).
-// srad may be null (then max radius is 0).
+// srad may be null (then max radius is 0).  Batched systems: the keys hold
+// the system index in bits 62..51 (four octree levels) and a 17-bit-per-axis
+// Morton code in that system's own cube below; sys_half16[s] = that cube's
+// half-size x 16 (cube is then unused).
 void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys,
                 const double4* sbody, const float* srad, const double* cube, int leaf_cap,
-                int* err);
+                int* err, const double* sys_half16 = nullptr);
 
 }  // namespace nb

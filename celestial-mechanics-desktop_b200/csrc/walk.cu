@@ -217,7 +217,8 @@ k_walk_group(WalkArgs a) {
         // round (one per lane), children of opened nodes are pushed on top.
         int* stk = fa;
         int sp = 1;
-        if (lane == 0) stk[0] = 0;
+        // batched systems: the walk starts at the group's own system root
+        if (lane == 0) stk[0] = a.sys_root ? a.sys_root[a.skeys[grp.x] >> kEnsSysShift] : 0;
         __syncwarp();
         // One candidate node per lane, decided: accepted cells -> cell list,
         // children of opened nodes -> stack, bodies of leaves -> particle list.

@@ -33,6 +33,8 @@ struct WalkArgs {
     int record_cap;
     unsigned mac_seed;          // harvest group sampling
     unsigned mac_sample;        // groups kept per 65536
+    const int* sys_root;        // batched systems: walk-tree root of each system
+                                // (indexed by the key's system field), else null
     unsigned* group_ctr;        // dynamic group counter (zeroed)
     unsigned long long* counters;  // [0] body-cell, [1] body-body interactions
     int* err;

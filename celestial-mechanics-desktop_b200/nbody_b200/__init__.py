@@ -9,6 +9,8 @@ from ._native import (FLAG_COLLISIONS, FLAG_LEARNED_MAC, FLAG_NO_QUADRUPOLE,  # 
                       FLAG_SHELL_THEOREM, MODE_BARNES_HUT, MODE_BARNES_HUT_REF, MODE_DIRECT,
                       MODE_DIRECT_FP64)
 from .engine import B200PhysicsBackend, B200SoAIntegrator, Engine, NBodyError  # noqa: F401
+from .ensemble import Ensemble  # noqa: F401
 from .scenarios import Bodies  # noqa: F401
 
-__all__ = ["Engine", "NBodyError", "B200PhysicsBackend", "B200SoAIntegrator", "Bodies"]
+__all__ = ["Engine", "Ensemble", "NBodyError", "B200PhysicsBackend", "B200SoAIntegrator",
+           "Bodies"]

@@ -49,6 +49,8 @@ PARAM_GROUP_PACK = 10
 PARAM_MAC_THETA_LO = 11
 PARAM_MAC_THETA_HI = 12
 PARAM_MAC_SCREEN_QUANTILE = 13
+PARAM_ENS_DIRECT_SHAPE = 14
+ENS_SHAPES = [(64, 1), (64, 2), (64, 4), (128, 1), (128, 2), (128, 4), (256, 1), (256, 2), (256, 4)]
 # timings / counters
 T_BUILD, T_TRAVERSAL, T_TOTAL, T_SORT, T_TREE, T_COUNT = range(6)
 (C_CELL_INTERACTIONS, C_BODY_INTERACTIONS, C_NODES, C_ACTIVE, C_PAIRS, C_MERGES, C_OVERFLOWS, C_GROUPS,
@@ -94,6 +96,21 @@ _SIGS = {
     "nb_mac_fit_screen": (i32, [vp]),
     "nb_mac_get_screen": (i32, [vp, P, i32]),
     "nb_mac_set_screen": (i32, [vp, P, i32]),
+    "nb_ens_create": (i32, [i32, P, i32, i32, C.POINTER(vp)]),
+    "nb_ens_destroy": (i32, [vp]),
+    "nb_ens_last_error": (C.c_char_p, [vp]),
+    "nb_ens_info": (i32, [vp, P, i32]),
+    "nb_ens_set_param_f64": (i32, [vp, i32, f64]),
+    "nb_ens_set_param_i32": (i32, [vp, i32, i32]),
+    "nb_ens_set_state": (i32, [vp, P, P, P, P, P, P, P]),
+    "nb_ens_get_state": (i32, [vp, P, P, P, P, P, P, P, P, P]),
+    "nb_ens_compute_forces": (i32, [vp, f64]),
+    "nb_ens_step": (i32, [vp, i32, f64, f64]),
+    "nb_ens_autotune": (i32, [vp, f64, P, P]),
+    "nb_ens_force_error": (i32, [vp, i32, u64, f64, P, P]),
+    "nb_ens_energy": (i32, [vp, f64, P, P, P]),
+    "nb_ens_get_counters": (i32, [vp, P, i32]),
+    "nb_ens_get_timings": (i32, [vp, P]),
 }
 MAC_PARAMS = 4801
 MAC_NORM = 18

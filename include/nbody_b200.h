@@ -84,9 +84,12 @@ enum nb_param {
                                       geometrically (default 0.35)                            */
     NB_PARAM_MAC_THETA_HI = 12,    /* f64, learned MAC: cells with 2h/d at or above this are
                                       opened; in between the network decides (default 1.0)   */
-    NB_PARAM_MAC_SCREEN_QUANTILE = 13 /* f64, learned MAC: quantile of |network - screen| over
+    NB_PARAM_MAC_SCREEN_QUANTILE = 13, /* f64, learned MAC: quantile of |network - screen| over
                                       the training set that sets the linear screen's margin;
                                       0 = no screen (default 0.9, used by the next fit)       */
+    NB_PARAM_ENS_DIRECT_SHAPE = 14 /* i32, ensembles: direct-sum tile shape 0..8 (threads x
+                                      targets/thread: 64x1 64x2 64x4 128x1 128x2 128x4 256x1
+                                      256x2 256x4; default 4), normally set by nb_ens_autotune */
 };
 
 /* Indices into nb_get_timings() output (milliseconds, CUDA events).
@@ -299,6 +302,59 @@ NB_API int32_t nb_mac_predict(nb_engine* h, const float* X, int32_t n, float* y)
 NB_API int32_t nb_mac_fit_screen(nb_engine* h);
 NB_API int32_t nb_mac_get_screen(nb_engine* h, float* screen, int32_t n);
 NB_API int32_t nb_mac_set_screen(nb_engine* h, const float* screen, int32_t n);
+
+/* ---- batched ensembles of independent systems -------------------------- */
+/* No reference counterpart (the reference steps one system per
+ * NBodySolver.Step, src/CelestialMechanics.Physics/Solvers/NBodySolver.cs:
+ * 290-391).  An ensemble holds many independent systems of uneven size, each
+ * with G = 1 gravity among its own bodies only.  Systems of at most ds_max_n
+ * bodies are summed directly (FP32 pair forces on FP64-differenced
+ * coordinates, compensated); larger ones use the Barnes-Hut group walk
+ * (NB_PARAM_THETA, default 0.5, monopole + quadrupole) over one shared sort
+ * and tree.  One velocity-Verlet step of all systems is one CUDA-graph launch.
+ * Arrays are the systems' bodies concatenated in the order of `sizes`. */
+typedef struct nb_ensemble nb_ensemble;
+
+/* At most 4096 systems above ds_max_n. */
+NB_API int32_t nb_ens_create(int32_t n_systems, const int32_t* sizes, int32_t ds_max_n,
+                             int32_t device, nb_ensemble** out);
+NB_API int32_t nb_ens_destroy(nb_ensemble* h);
+NB_API const char* nb_ens_last_error(const nb_ensemble* h);
+/* systems, direct systems, tree systems, bodies, direct bodies, tree bodies */
+NB_API int32_t nb_ens_info(const nb_ensemble* h, int64_t* out, int32_t n);
+/* NB_PARAM_THETA (f64); NB_PARAM_LEAF_CAPACITY, NB_PARAM_ENS_DIRECT_SHAPE (i32) */
+NB_API int32_t nb_ens_set_param_f64(nb_ensemble* h, int32_t param, double value);
+NB_API int32_t nb_ens_set_param_i32(nb_ensemble* h, int32_t param, int32_t value);
+/* Positions, velocities, masses; accelerations are unknown until the first
+ * force evaluation (nb_ens_step does one first when needed). */
+NB_API int32_t nb_ens_set_state(nb_ensemble* h, const double* px, const double* py,
+                                const double* pz, const double* vx, const double* vy,
+                                const double* vz, const double* mass);
+/* Any pointer may be NULL. */
+NB_API int32_t nb_ens_get_state(nb_ensemble* h, double* px, double* py, double* pz, double* vx,
+                                double* vy, double* vz, double* ax, double* ay, double* az);
+/* Accelerations at the current positions. */
+NB_API int32_t nb_ens_compute_forces(nb_ensemble* h, double softening);
+/* n_steps velocity-Verlet steps (SoAVerletIntegrator.cs:48-116 per system),
+ * one graph launch each. */
+NB_API int32_t nb_ens_step(nb_ensemble* h, int32_t n_steps, double dt, double softening);
+/* Times every direct tile shape on the current state (3 runs each, CUDA
+ * events) and keeps the fastest; ms_per_shape (9 entries, may be NULL) gets
+ * the times, -1 for a shape that cannot run. */
+NB_API int32_t nb_ens_autotune(nb_ensemble* h, double softening, int32_t* shape,
+                               double* ms_per_shape);
+/* Per system (in `sizes` order): rms and max relative error of the current
+ * accelerations against an FP64 direct sum on up to `samples` bodies. */
+NB_API int32_t nb_ens_force_error(nb_ensemble* h, int32_t samples, uint64_t seed,
+                                  double softening, double* rms, double* max_err);
+/* Per system: total, kinetic and softened potential energy (FP64). */
+NB_API int32_t nb_ens_energy(nb_ensemble* h, double softening, double* energy, double* kinetic,
+                             double* potential);
+/* direct pairs per evaluation, tree body-cell and body-body interactions of
+ * the last evaluation, graph launches so far, direct work items, direct shape */
+NB_API int32_t nb_ens_get_counters(const nb_ensemble* h, int64_t* out, int32_t n);
+/* Device time per step of the last nb_ens_step (or of the last evaluation). */
+NB_API int32_t nb_ens_get_timings(const nb_ensemble* h, double* ms_per_step);
 
 #ifdef __cplusplus
 }
