@@ -459,6 +459,212 @@ def run_b200(args, ws, rank, local):
     return line
 
 
+def run_theta05(args, ws, rank, local):
+    """Plain Barnes-Hut with the geometric MAC theta = 0.5 on the Plummer
+    sphere (no training, no calibration): the configuration the stage
+    profiles are taken on."""
+    import torch
+
+    from nbody_b200 import MODE_BARNES_HUT, Engine, scenarios
+    from nbody_b200 import _native as N
+
+    dev = local
+    torch.cuda.set_device(dev)
+    n = args.n
+    b = scenarios.plummer(n, 1.0, 1.0, seed=SEED)
+    eng = Engine(n, device=dev)
+    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
+    eng.set_param(N.PARAM_THETA, THETA)
+    arm = timed_arm(eng, b, stream, args, ws, dev, MODE_BARNES_HUT, N, MODE_BARNES_HUT,
+                    "theta_0_5")
+    pk, _ = peaks()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = sms * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    achieved = arm["walk_flops_per_step"] / (arm["stage_ms"]["walk"] / 1e3) / 1e12
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": arm["steps_per_s"], "unit": "steps/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": max(args.warmup, 3),
+                "ms_per_step": arm["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded Plummer sphere, numpy PCG64)",
+                "config": {"workload": f"bh_plummer_theta05_n{n}", "n": n, "theta": THETA,
+                           "eps": EPS, "dt": DT, "seed": SEED, "mac": "geometric",
+                           "multipole": "monopole+quadrupole"},
+                "interactions_per_s": arm["interactions_per_s"],
+                "force_error": arm["force_error"], "stage_ms": arm["stage_ms"],
+                "roofline": {"bound": "fp32", "kernel": "k_walk_group", "achieved": achieved,
+                             "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                             "traffic": walk_traffic_per_launch() if n == N_BODIES else None},
+                "gpu_launches": launches_per_step() * args.steps, "clocks": arm["clocks"]}
+    eng.close()
+    return line
+
+
+ENS_SYSTEMS, ENS_SEED, ENS_DS_MAX, ENS_DT = 512, 3, 2048, 1e-4
+# kernels of one ensemble step: kick-drift, direct work queue, cubes, keys,
+# 8 sort passes, gather, tree (radix, mark, scan, base, emit, multipoles),
+# system roots (2), walk groups, walk, kick
+ENS_LAUNCHES_PER_STEP = 1 + 1 + 1 + 1 + 8 + 1 + 6 + 2 + 1 + 1 + 1
+
+
+def cpu_ensemble_seconds(systems, threads):
+    """One force evaluation of every system on the host with all threads:
+    the oracle's CpuParallelBackend restatement (OpenMP over targets) for the
+    direct systems, then the reference's serial BarnesHutSolver (oracle/_ref,
+    theta 0.5) on the larger systems, one system per pool thread.  (The
+    reference's own parallel solver, whose job system shares the process
+    with the OpenMP direct sums, crashed intermittently when the two were
+    interleaved, so the tree systems run its serial solver side by side.)"""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import oracle
+
+    t = time.perf_counter()
+    for b in systems:
+        if b.n <= ENS_DS_MAX:
+            oracle.direct_forces(b.px, b.py, b.pz, b.mass, b.active, EPS, nthreads=threads)
+    big = [b for b in systems if b.n > ENS_DS_MAX]
+    if oracle.ref() is not None:
+        kind = "reference+port"
+        fn = lambda b: oracle.ref_bh_forces(b.px, b.py, b.pz, b.mass, b.active, EPS,  # noqa: E731
+                                            THETA, False, 1)
+    else:
+        kind = "port"
+        fn = lambda b: oracle.bh_forces(b.px, b.py, b.pz, b.mass, b.active, EPS,  # noqa: E731
+                                        THETA, nthreads=1)
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(fn, big))
+    return time.perf_counter() - t, kind
+
+
+def run_ensemble(args, ws, rank, local):
+    """512 independent Plummer systems (N log-uniform in [64, 8192], seed 3,
+    scale 1 AU, 1 Msun each): direct sum for N <= 2048, Barnes-Hut theta 0.5
+    above, one CUDA-graph launch per velocity-Verlet step."""
+    import torch
+
+    from nbody_b200 import Ensemble, scenarios
+
+    dev = local
+    torch.cuda.set_device(dev)
+    systems = scenarios.ensemble(ENS_SYSTEMS, seed=ENS_SEED)
+    sizes = [b.n for b in systems]
+    ens = Ensemble(sizes, ds_max_n=ENS_DS_MAX, device=dev)
+    ens.set_state(systems)
+    shape, shape_ms = ens.autotune(EPS)
+    e0, _, _ = ens.energy(EPS)
+    ens.step(max(args.warmup, 3), ENS_DT, EPS)
+    ens.set_state(systems)
+    ens.compute_forces(EPS)
+    info = ens.info()
+    c = ens.counters()
+    inter_per_step = c["direct_pairs"] + c["tree_cell"] + c["tree_body"]
+    clocks = Clocks(dev)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    torch.cuda.nvtx.range_push("ensemble")
+    w0 = time.perf_counter()
+    ens.step(args.steps, ENS_DT, EPS)  # CUDA events on the ensemble's stream
+    wall = time.perf_counter() - w0
+    torch.cuda.nvtx.range_pop()
+    barrier(ws)
+    clk = clocks.stop()
+    ms = max_over_ranks(ws, ens.ms_per_step() * args.steps)
+    e1, _, _ = ens.energy(EPS)
+    rms, mx = ens.force_error(256, 11, EPS)
+    small = np.array(sizes) <= ENS_DS_MAX
+    drift = np.abs((e1 - e0) / e0)
+
+    # end to end: host state in, 100 steps, host state out (pinned arrays)
+    k_e2e = min(args.steps, 100)
+    st = ens.get_state()
+    ens.step(1, ENS_DT, EPS)
+    e2e0 = time.perf_counter()
+    ens.set_state(systems)
+    ens.step(k_e2e, ENS_DT, EPS)
+    st = ens.get_state()
+    e2e_s = max_over_ranks(ws, time.perf_counter() - e2e0)
+    n = info["bodies"]
+
+    pk, pk_kind = peaks()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = sms * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    flops = (FLOPS_BODY * (c["direct_pairs"] + c["tree_body"]) + FLOPS_CELL_QUAD * c["tree_cell"])
+    achieved = flops / (ms / args.steps / 1e3) / 1e12
+    line = None
+    if rank == 0:
+        cpu = None
+        # the system with the largest energy drift, integrated again with the
+        # FP64 direct sum + Verlet on the host (up to 4096 bodies: seconds)
+        iw = int(np.argmax(drift))
+        worst = {"index": iw, "n": sizes[iw], "drift": float(drift[iw]), "fp64_cpu_drift": None}
+        if sizes[iw] <= 4096 and not args.no_cpu_baseline:
+            import oracle
+
+            bw = systems[iw]
+            dw = {k: getattr(bw, k) for k in ("px", "py", "pz", "vx", "vy", "vz", "mass",
+                                                "active")}
+            dw["ax"], dw["ay"], dw["az"] = oracle.direct_forces(bw.px, bw.py, bw.pz, bw.mass,
+                                                                bw.active, EPS)
+            ww = oracle.verlet_direct(dw, EPS, ENS_DT, args.steps)
+            ww["active"] = bw.active
+            ew0, ew1 = oracle.energy(dw, EPS)["e"], oracle.energy(ww, EPS)["e"]
+            worst["fp64_cpu_drift"] = abs((ew1 - ew0) / ew0)
+        if ws == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            s, kind = cpu_ensemble_seconds(systems, threads)
+            cpu = {"value": 1.0 / s, "unit": "steps/s", "cores": threads, "kind": kind,
+                   "sample": "one force evaluation of all 512 systems: oracle direct sum "
+                             "(CpuParallelBackend restatement, OpenMP) for N <= 2048, the "
+                             "reference's serial BarnesHutSolver theta 0.5 above, one system "
+                             "per thread"}
+        line = {
+            "metric": METRIC, "value": sum_over_ranks(ws, args.steps) / (ms / 1e3),
+            "unit": "steps/s", "n_gpus": ws, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (512 seeded Plummer spheres, numpy PCG64)",
+            "config": {"workload": "ensemble_512_plummer", "systems": ENS_SYSTEMS,
+                       "sizes": "log-uniform [64, 8192], seed 3", "bodies": n,
+                       "direct_systems": info["direct_systems"],
+                       "tree_systems": info["tree_systems"], "ds_max_n": ENS_DS_MAX,
+                       "theta": THETA, "eps": EPS, "dt": ENS_DT,
+                       "launch": "one CUDA graph per step (direct and tree branches)",
+                       "l2": "state and tree buffers ~0.2 GB, sizes > L2"},
+            "interactions_per_s": sum_over_ranks(ws, inter_per_step * args.steps) / (ms / 1e3),
+            "interactions_per_step": {"direct_pairs": c["direct_pairs"],
+                                      "tree_cell": c["tree_cell"], "tree_body": c["tree_body"]},
+            "autotune": {"shape": list(__import__("nbody_b200")._native.ENS_SHAPES[shape]),
+                         "ms_per_shape": [round(float(x), 4) for x in shape_ms]},
+            "force_error": {"direct_rms_max": float(rms[small].max()),
+                            "direct_rms_median": float(np.median(rms[small])),
+                            "tree_rms_max": float(rms[~small].max()) if (~small).any() else None,
+                            "tree_rms_median": (float(np.median(rms[~small]))
+                                                if (~small).any() else None),
+                            "max_rel": float(mx.max()),
+                            "vs": "FP64 direct sum per system, 256 sampled bodies, last step"},
+            "energy_drift": {"max_abs": float(drift.max()), "median_abs": float(np.median(drift)),
+                             "steps": args.steps, "worst_system": worst},
+            "roofline": {"bound": "fp32", "kernel": "whole step (direct + tree walk)",
+                         "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak,
+                         "peak_kind": f"SMs x 128 x 2 x sm_max_mhz ({pk_kind} max clock)",
+                         "traffic": None},
+            "wall_s_timed": wall,
+            "cpu_baseline": cpu,
+            "e2e": {"value": k_e2e / e2e_s, "unit": "steps/s",
+                    "h2d_bytes_per_step": 7 * 8 * n / k_e2e, "d2h_bytes_per_step": 9 * 8 * n / k_e2e,
+                    "path": f"nb_ens_set_state + nb_ens_step({k_e2e}) + nb_ens_get_state on host "
+                            "arrays"},
+            "gpu_launches": ENS_LAUNCHES_PER_STEP * args.steps,
+            "clocks": clk,
+        }
+    ens.close()
+    return line
+
+
 def launches_per_step() -> int:
     """Kernels of one device step: kick-drift-bbox, cube, keys, 8 sort passes,
     gather, zero-acc, radix tree, octree mark, block scan, octree base,
@@ -597,20 +803,28 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=N_BODIES,
                     help="bodies (default the 1,048,576-body workload; smaller for profiling)")
-    ap.add_argument("--workload", default="bh1m", choices=["bh1m", "mac4m", "ds1000", "disk"],
+    ap.add_argument("--workload", default="bh1m",
+                    choices=["bh1m", "mac4m", "theta05", "ensemble", "ds1000", "disk"],
                     help="bh1m: the headline line, learned vs geometric MAC at rms <= 1e-3 on "
                          "the N=1,048,576 Plummer sphere; mac4m: the same on the N=4,194,304 "
-                         "Hernquist sphere; ds1000: FP64 direct sum N=1000, 10k steps; disk: "
-                         "collisional disk N=262,145, 1000 steps")
+                         "Hernquist sphere; theta05: plain geometric theta 0.5 only; ensemble: "
+                         "512 Plummer systems, 1000 steps; ds1000: FP64 direct sum N=1000, 10k "
+                         "steps; disk: collisional disk N=262,145, 1000 steps")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"bh1m": 100, "mac4m": 50, "ds1000": 10_000, "disk": 1000}[args.workload]
+        args.steps = {"bh1m": 100, "mac4m": 50, "theta05": 100, "ensemble": 1000,
+                      "ds1000": 10_000, "disk": 1000}[args.workload]
     ws, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank)
         elif args.workload == "ds1000":
             line = run_ds1000(args, ws, rank, local)
+            if line is not None:
+                print(json.dumps(line))
+        elif args.workload in ("theta05", "ensemble"):
+            line = (run_theta05 if args.workload == "theta05" else run_ensemble)(args, ws, rank,
+                                                                                 local)
             if line is not None:
                 print(json.dumps(line))
         elif args.workload == "disk":

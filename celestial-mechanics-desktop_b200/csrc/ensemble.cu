@@ -10,7 +10,8 @@
 //     kernel over a work queue of (system, target tile) items, largest
 //     systems first; each item stages its system's sources through shared
 //     memory and evaluates FP32 pair forces on coordinates differenced in
-//     FP64 against the system's first body, with a compensated sum per tile.
+//     FP64 against the system's centre of mass, with a compensated sum per
+//     tile.
 //     Tile shape (threads x targets per thread) is picked by nb_ens_autotune.
 //   * tree branch (larger systems): one Morton sort and one tree over all of
 //     them, keys = system index (12 bits, four octree levels) | a 17-bit per
@@ -52,6 +53,7 @@ struct EnsDirect {
     const double *px, *py, *pz, *m;
     double *ax, *ay, *az;
     const int* off;        // system offsets (internal order)
+    const double4* ref;    // per system: centre of mass (reference point), mass
     const int2* items;     // (system, tile)
     int n_items;
     unsigned* ctr;         // work-queue counter (zeroed per launch)
@@ -77,7 +79,8 @@ __global__ void __launch_bounds__(TPB) k_ens_direct(EnsDirect a) {
         if (it >= a.n_items) break;
         const int2 w = a.items[it];
         const int b0 = a.off[w.x], ns = a.off[w.x + 1] - b0;
-        const double cx = a.px[b0], cy = a.py[b0], cz = a.pz[b0];
+        const double4 c = a.ref[w.x];
+        const double cx = c.x, cy = c.y, cz = c.z;
         float xi[TPT], yi[TPT], zi[TPT];
         float fx[TPT], fy[TPT], fz[TPT], kx[TPT], ky[TPT], kz[TPT];
 #pragma unroll
@@ -166,38 +169,50 @@ DirectKernel pick_direct(int shape, bool guard) {
 
 // ---- tree branch -----------------------------------------------------------
 
-// One block per tree system: bounding box -> cube (cx, cy, cz, half) with the
-// single-system rule (max extent / 2, floor 1e-10, x 1.001), and half x 16.
+// One block per system: bounding box -> cube (cx, cy, cz, half) with the
+// single-system rule (max extent / 2, floor 1e-10, x 1.001), half x 16, and
+// the centre of mass (the bounding-box centre for a massless system).  Sums
+// are reduced in a fixed order, so the result does not depend on timing.
 __global__ void k_ens_cubes(const int* __restrict__ off, State s, double4* __restrict__ cubes,
-                            double* __restrict__ half16) {
-    __shared__ double red[6][32];
+                            double* __restrict__ half16, double4* __restrict__ com) {
+    __shared__ double red[10][32];
     const int sys = blockIdx.x;
     const int b0 = off[sys], b1 = off[sys + 1];
     double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    double sm[4] = {0.0, 0.0, 0.0, 0.0};  // m, m x, m y, m z
     for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
         const double p[3] = {s.px[i], s.py[i], s.pz[i]};
+        const double m = s.mass[i];
         for (int k = 0; k < 3; k++) {
             mn[k] = fmin(mn[k], p[k]);
             mx[k] = fmax(mx[k], p[k]);
+            sm[1 + k] += m * p[k];
         }
+        sm[0] += m;
     }
     for (int k = 0; k < 3; k++) {
         mn[k] = warp_min(mn[k]);
         mx[k] = warp_max(mx[k]);
     }
+    for (int k = 0; k < 4; k++)
+        for (int o = 16; o > 0; o >>= 1) sm[k] += __shfl_xor_sync(0xFFFFFFFFu, sm[k], o);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (lane == 0)
+    if (lane == 0) {
         for (int k = 0; k < 3; k++) {
             red[k][wid] = mn[k];
             red[3 + k][wid] = mx[k];
         }
+        for (int k = 0; k < 4; k++) red[6 + k][wid] = sm[k];
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int w = 1; w < nw; w++)
+        for (int w = 1; w < nw; w++) {
             for (int k = 0; k < 3; k++) {
                 red[k][0] = fmin(red[k][0], red[k][w]);
                 red[3 + k][0] = fmax(red[3 + k][0], red[3 + k][w]);
             }
+            for (int k = 0; k < 4; k++) red[6 + k][0] += red[6 + k][w];
+        }
         const double cx = __dmul_rn(__dadd_rn(red[0][0], red[3][0]), 0.5);
         const double cy = __dmul_rn(__dadd_rn(red[1][0], red[4][0]), 0.5);
         const double cz = __dmul_rn(__dadd_rn(red[2][0], red[5][0]), 0.5);
@@ -207,6 +222,9 @@ __global__ void k_ens_cubes(const int* __restrict__ off, State s, double4* __res
         h = __dmul_rn(h, 1.001);
         cubes[sys] = make_double4(cx, cy, cz, h);
         half16[sys] = h * 16.0;
+        const double M = red[6][0];
+        com[sys] = M > 0.0 ? make_double4(red[7][0] / M, red[8][0] / M, red[9][0] / M, M)
+                           : make_double4(cx, cy, cz, 0.0);
     }
 }
 
@@ -376,8 +394,9 @@ struct nb_ensemble {
     int *d_off = nullptr, *d_off_bh = nullptr, *d_sys_of_bh = nullptr, *d_sys_of = nullptr;
     int* d_perm = nullptr;                // internal row -> caller row
     double* d_stage = nullptr;
-    double4* d_cubes = nullptr;
+    double4* d_cubes = nullptr;           // per system (internal order)
     double* d_half16 = nullptr;
+    double4* d_com = nullptr;
     int* d_root = nullptr;
     unsigned long long* d_root_best = nullptr;
     int2* d_items = nullptr;
@@ -490,6 +509,7 @@ void launch_direct(nb_ensemble* h, cudaStream_t st, double eps) {
     a.ay = h->s.ay;
     a.az = h->s.az;
     a.off = h->d_off;
+    a.ref = h->d_com;
     a.items = h->d_items;
     a.n_items = h->n_items;
     a.ctr = &h->scal->ds_ctr;
@@ -498,10 +518,17 @@ void launch_direct(nb_ensemble* h, cudaStream_t st, double eps) {
     nb::pick_direct(h->shape, !(eps > 0.0))<<<grid, nb::kShapes[h->shape].tpb, 0, st>>>(a);
 }
 
+// Per-system cubes and centres of mass of the current positions.
+void launch_cubes(nb_ensemble* h) {
+    nb::k_ens_cubes<<<h->nsys, 256, 0, h->st>>>(h->d_off, h->s, h->d_cubes, h->d_half16,
+                                                h->d_com);
+}
+
 // Forces at the current positions: the direct branch on the second stream,
 // the tree branch on the first; the first stream waits for both.
 void enqueue_forces(nb_ensemble* h, double eps) {
     EnsScal* sc = h->scal;
+    launch_cubes(h);
     cudaEventRecord(h->ev_fork, h->st);
     cudaStreamWaitEvent(h->st2, h->ev_fork, 0);
     launch_direct(h, h->st2, eps);
@@ -510,16 +537,17 @@ void enqueue_forces(nb_ensemble* h, double eps) {
     if (h->n_bh > 0) {
         cudaStream_t st = h->st;
         const int n = h->n_bh;
-        nb::k_ens_cubes<<<h->nbh, 256, 0, st>>>(h->d_off_bh, h->sbh, h->d_cubes, h->d_half16);
+        const double4* cubes = h->d_cubes + h->nds;  // tree systems follow the direct ones
+        const double* half16 = h->d_half16 + h->nds;
         uint32_t* hist = (uint32_t*)h->sort_ws;
         cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, st);
-        nb::k_ens_keys<<<nb::ceil_div(n, 256), 256, 0, st>>>(n, h->sbh, h->d_sys_of_bh, h->d_cubes,
+        nb::k_ens_keys<<<nb::ceil_div(n, 256), 256, 0, st>>>(n, h->sbh, h->d_sys_of_bh, cubes,
                                                             h->keys0, h->vals0, hist);
         nb::sort_pairs(st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err,
                        h->sms);
         nb::launch_gather(st, n, h->sbh, h->vals0, h->sbody, nullptr, nullptr);
-        nb::tree_build(st, h->tree, n, h->keys0, h->sbody, nullptr, h->d_half16, h->leaf_cap,
-                       sc->err, h->d_half16);
+        nb::tree_build(st, h->tree, n, h->keys0, h->sbody, nullptr, half16, h->leaf_cap, sc->err,
+                       half16);
         cudaMemsetAsync(h->d_root_best, 0xFF, sizeof(unsigned long long) * h->nbh, st);
         nb::k_ens_roots<<<nb::ceil_div(2 * (long long)n, 256), 256, 0, st>>>(h->tree, h->keys0,
                                                                             h->d_off_bh,
@@ -669,8 +697,9 @@ NB_API int32_t nb_ens_create(int32_t n_systems, const int32_t* sizes, int32_t ds
         if ((r = ealloc(h, &h->d_off_bh, (size_t)h->nbh + 1))) break;
         if ((r = ealloc(h, &h->d_sys_of, n)) || (r = ealloc(h, &h->d_sys_of_bh, nbhb))) break;
         if ((r = ealloc(h, &h->d_perm, n)) || (r = ealloc(h, &h->d_stage, n))) break;
-        if ((r = ealloc(h, &h->d_cubes, (size_t)std::max(h->nbh, 1))) ||
-            (r = ealloc(h, &h->d_half16, (size_t)std::max(h->nbh, 1))) ||
+        if ((r = ealloc(h, &h->d_cubes, (size_t)n_systems)) ||
+            (r = ealloc(h, &h->d_half16, (size_t)n_systems)) ||
+            (r = ealloc(h, &h->d_com, (size_t)n_systems)) ||
             (r = ealloc(h, &h->d_root, (size_t)std::max(h->nbh, 1))) ||
             (r = ealloc(h, &h->d_root_best, (size_t)std::max(h->nbh, 1))))
             break;
@@ -872,6 +901,7 @@ NB_API int32_t nb_ens_autotune(nb_ensemble* h, double softening, int32_t* shape,
     cudaSetDevice(h->device);
     int best = h->shape;
     float best_ms = 1e30f;
+    launch_cubes(h);  // reference points of the direct systems
     for (int k = 0; k < nb::kNumShapes; k++) {
         if (ms_per_shape) ms_per_shape[k] = -1.0;
         if (h->shape_blocks[k] <= 0) continue;
