@@ -100,9 +100,12 @@ def sum_over_ranks(ws, x: float) -> float:
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """nvidia-smi samples (every 50 ms) of SM clock and throttle reasons.
+    start() returns once the first sample is in; stop(window) keeps the
+    samples whose timestamps fall inside the given wall-clock window (the
+    timed region), or all of them."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -116,11 +119,23 @@ class Clocks:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device),
                                           f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                          "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        t = time.time()
+        while time.time() - t < 3.0 and not Path(self.f.name).read_text().strip():
+            time.sleep(0.02)
 
-    def stop(self) -> dict:
+    @staticmethod
+    def _stamp(s: str):
+        import datetime
+        try:
+            return datetime.datetime.strptime(s.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
+    def stop(self, window=None) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -128,19 +143,24 @@ class Clocks:
         self.f.flush()
         rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
         os.unlink(self.f.name)
-        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        rows = [r for r in rows if len(r) >= 10]
+        if window is not None:
+            kept = [r for r in rows if (ts := self._stamp(r[0])) is not None
+                    and window[0] <= ts <= window[1]]
+            rows = kept
+        num = lambda v: v.strip().replace(".", "").isdigit()  # noqa: E731
+        sm = [float(r[2]) for r in rows if num(r[2])]
+        mx = [float(r[3]) for r in rows if num(r[3])]
         reasons = set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
         for r in rows:
-            if len(r) < 9:
-                continue
-            for name, v in zip(names, r[5:9]):
+            for name, v in zip(names, r[6:10]):
                 if v.strip() == "Active":
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "interval_ms": 50,
+                "window": "timed region" if window is not None else "whole sampling run"}
 
 
 def peaks():
@@ -286,14 +306,15 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
     in an NVTX range named `label` (ncu --nvtx-include "<label>/")."""
     import torch
 
+    clocks = Clocks(dev)
+    clocks.start()
     eng.set_state(b, old_acc=False)
     eng.step(1, 0.0, EPS, mode_geo)
     eng.step(max(args.warmup, 3), DT, EPS, flags)
     torch.cuda.synchronize(dev)
-    clocks = Clocks(dev)
     barrier(ws)
     torch.cuda.synchronize(dev)
-    clocks.start()
+    w0 = time.time()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.nvtx.range_push(label)
@@ -313,8 +334,9 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
     t1.record(stream)
     torch.cuda.synchronize(dev)
     torch.cuda.nvtx.range_pop()
+    w1 = time.time()
     barrier(ws)
-    clk = clocks.stop()
+    clk = clocks.stop((w0, w1))
     ms = max_over_ranks(ws, t0.elapsed_time(t1))
     err = eng.force_error(ERR_SAMPLES, ERR_SEED, EPS)
     k = args.steps
@@ -462,11 +484,15 @@ def run_b200(args, ws, rank, local):
 def run_theta05(args, ws, rank, local):
     """Plain Barnes-Hut with the geometric MAC theta = 0.5 on the Plummer
     sphere (no training, no calibration): the configuration the stage
-    profiles are taken on."""
+    profiles are taken on.  With --workload direct32 the same steps use the
+    FP32 direct sum instead (all N^2 pairs)."""
     import torch
 
-    from nbody_b200 import MODE_BARNES_HUT, Engine, scenarios
+    from nbody_b200 import MODE_BARNES_HUT, MODE_DIRECT, Engine, scenarios
     from nbody_b200 import _native as N
+
+    direct = args.workload == "direct32"
+    mode = MODE_DIRECT if direct else MODE_BARNES_HUT
 
     dev = local
     torch.cuda.set_device(dev)
@@ -475,8 +501,8 @@ def run_theta05(args, ws, rank, local):
     eng = Engine(n, device=dev)
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     eng.set_param(N.PARAM_THETA, THETA)
-    arm = timed_arm(eng, b, stream, args, ws, dev, MODE_BARNES_HUT, N, MODE_BARNES_HUT,
-                    "theta_0_5")
+    arm = timed_arm(eng, b, stream, args, ws, dev, mode, N, mode,
+                    "direct32" if direct else "theta_0_5")
     pk, _ = peaks()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     fp32_peak = sms * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
@@ -488,15 +514,22 @@ def run_theta05(args, ws, rank, local):
                 "ms_per_step": arm["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded Plummer sphere, numpy PCG64)",
-                "config": {"workload": f"bh_plummer_theta05_n{n}", "n": n, "theta": THETA,
-                           "eps": EPS, "dt": DT, "seed": SEED, "mac": "geometric",
-                           "multipole": "monopole+quadrupole"},
+                "config": ({"workload": f"direct_fp32_plummer_n{n}", "n": n, "eps": EPS,
+                            "dt": DT, "seed": SEED, "force": "direct sum, FP32 pairs on "
+                            "FP64-differenced coordinates"} if direct else
+                           {"workload": f"bh_plummer_theta05_n{n}", "n": n, "theta": THETA,
+                            "eps": EPS, "dt": DT, "seed": SEED, "mac": "geometric",
+                            "multipole": "monopole+quadrupole"}),
                 "interactions_per_s": arm["interactions_per_s"],
                 "force_error": arm["force_error"], "stage_ms": arm["stage_ms"],
-                "roofline": {"bound": "fp32", "kernel": "k_walk_group", "achieved": achieved,
-                             "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                             "traffic": walk_traffic_per_launch() if n == N_BODIES else None},
-                "gpu_launches": launches_per_step() * args.steps, "clocks": arm["clocks"]}
+                "roofline": {"bound": "fp32",
+                             "kernel": "k_direct_fp32" if direct else "k_walk_group",
+                             "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                             "frac": achieved / fp32_peak, "flop_per_pair": FLOPS_BODY,
+                             "traffic": (walk_traffic_per_launch()
+                                         if n == N_BODIES and not direct else None)},
+                "gpu_launches": (15 if direct else launches_per_step()) * args.steps,
+                "clocks": arm["clocks"]}
     eng.close()
     return line
 
@@ -566,11 +599,13 @@ def run_ensemble(args, ws, rank, local):
     clocks.start()
     torch.cuda.nvtx.range_push("ensemble")
     w0 = time.perf_counter()
+    ws0 = time.time()
     ens.step(args.steps, ENS_DT, EPS)  # CUDA events on the ensemble's stream
     wall = time.perf_counter() - w0
+    ws1 = time.time()
     torch.cuda.nvtx.range_pop()
     barrier(ws)
-    clk = clocks.stop()
+    clk = clocks.stop((ws0, ws1))
     ms = max_over_ranks(ws, ens.ms_per_step() * args.steps)
     e1, _, _ = ens.energy(EPS)
     rms, mx = ens.force_error(256, 11, EPS)
@@ -683,12 +718,14 @@ def _timed_steps(eng, stream, steps, dt, eps, flags, dev, ws):
     clocks.start()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
     t0.record(stream)
     eng.step(steps, dt, eps, flags)
     t1.record(stream)
     torch.cuda.synchronize(dev)
+    w1 = time.time()
     barrier(ws)
-    clk = clocks.stop()
+    clk = clocks.stop((w0, w1))
     return max_over_ranks(ws, t0.elapsed_time(t1)), clk
 
 
@@ -804,15 +841,17 @@ def main():
     ap.add_argument("--n", type=int, default=N_BODIES,
                     help="bodies (default the 1,048,576-body workload; smaller for profiling)")
     ap.add_argument("--workload", default="bh1m",
-                    choices=["bh1m", "mac4m", "theta05", "ensemble", "ds1000", "disk"],
+                    choices=["bh1m", "mac4m", "theta05", "direct32", "ensemble", "ds1000",
+                             "disk"],
                     help="bh1m: the headline line, learned vs geometric MAC at rms <= 1e-3 on "
                          "the N=1,048,576 Plummer sphere; mac4m: the same on the N=4,194,304 "
-                         "Hernquist sphere; theta05: plain geometric theta 0.5 only; ensemble: "
+                         "Hernquist sphere; theta05: plain geometric theta 0.5 only; direct32: "
+                         "FP32 direct sum on the same sphere; ensemble: "
                          "512 Plummer systems, 1000 steps; ds1000: FP64 direct sum N=1000, 10k "
                          "steps; disk: collisional disk N=262,145, 1000 steps")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"bh1m": 100, "mac4m": 50, "theta05": 100, "ensemble": 1000,
+        args.steps = {"bh1m": 100, "mac4m": 50, "theta05": 100, "direct32": 3, "ensemble": 1000,
                       "ds1000": 10_000, "disk": 1000}[args.workload]
     ws, rank, local = dist_setup()
     try:
@@ -822,9 +861,9 @@ def main():
             line = run_ds1000(args, ws, rank, local)
             if line is not None:
                 print(json.dumps(line))
-        elif args.workload in ("theta05", "ensemble"):
-            line = (run_theta05 if args.workload == "theta05" else run_ensemble)(args, ws, rank,
-                                                                                 local)
+        elif args.workload in ("theta05", "direct32", "ensemble"):
+            line = (run_ensemble if args.workload == "ensemble" else run_theta05)(args, ws, rank,
+                                                                                  local)
             if line is not None:
                 print(json.dumps(line))
         elif args.workload == "disk":

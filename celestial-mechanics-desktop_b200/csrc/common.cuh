@@ -8,6 +8,15 @@
 
 namespace nb {
 
+// 1/sqrt(x), one approximate MUFU instruction with denormal inputs flushed to
+// zero (the pair kernels only pass r^2 + eps^2, far from the denormal range,
+// or guard r^2 = 0 themselves).
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Batched systems: keys = system (12 bits, bits 62..51) | 3 x 17-bit Morton.
 constexpr int kEnsSysShift = 51;
 constexpr int kEnsSysBits = 12;

@@ -9,18 +9,28 @@
 // replaces the reference GPU gravity_kernel (engine/src/cuda/gravity_kernel.cu:
 // 20-95), which loads inactive sources with their real mass.
 //
-// k_direct_fp32 is the throughput kernel: Morton-sorted targets, j-tiles of
-// bodies staged in shared memory as FP32 coordinates differenced in FP64
-// against the block's reference body, two targets per thread so every
-// broadcast shared-memory read feeds two pair evaluations, and a Kahan fold
-// of each tile's FP32 partial sum.
+// k_direct_fp32 is the throughput kernel: Morton-sorted targets in tiles of
+// 256 x kD32Per, sources in chunks, one persistent launch over a work queue
+// of (target tile, source chunk) items so the grid ends evenly; j-tiles of
+// sources staged in shared memory as FP32 coordinates differenced in FP64
+// against the target tile's centre of mass; kD32Per targets per thread so every
+// broadcast shared-memory read feeds several pair evaluations; a Kahan fold
+// of each j-tile's FP32 partial sum.  The chunk partials are written in FP64
+// and k_direct_reduce adds them in chunk order, so the result does not depend
+// on scheduling.
+#include <algorithm>
+
 #include "direct.cuh"
 
 namespace nb {
 
 constexpr int kD32Threads = 256;
-constexpr int kD32Per = 2;  // targets per thread
+#ifndef NB_D32_PER
+#define NB_D32_PER 4
+#endif
+constexpr int kD32Per = NB_D32_PER;  // targets per thread
 constexpr int kD32Tile = kD32Threads;
+constexpr int kD32MinChunk = 4096;    // sources per chunk at least
 
 __device__ __forceinline__ void kahan32(float& s, float& c, float x) {
     float y = x - c;
@@ -29,91 +39,153 @@ __device__ __forceinline__ void kahan32(float& s, float& c, float x) {
     s = t;
 }
 
-// Targets and sources are the n sorted bodies (all active).  Block b handles
-// targets [b*512, b*512+512); its reference point is its first body.  The
-// self pair has dx = dy = dz = 0 and contributes 0 when eps > 0; GUARD (used
-// when eps == 0) zeroes 1/r at r = 0 instead of evaluating 0 * inf.
+// Targets and sources are the n sorted bodies (all active).  Item it covers
+// target tile it / chunks and source chunk it % chunks; its partial sums go
+// to part[(chunk * 3 + axis) * n + target].  The self pair has
+// dx = dy = dz = 0 and contributes 0 when eps > 0; GUARD (used when
+// eps == 0) zeroes 1/r at r = 0 instead of evaluating 0 * inf.
 template <bool SHELL, bool GUARD>
 __global__ void __launch_bounds__(kD32Threads)
 k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict__ srad,
-              const uint32_t* __restrict__ sidx, float eps2, double* __restrict__ ax,
-              double* __restrict__ ay, double* __restrict__ az,
-              unsigned long long* __restrict__ counter) {
+              float eps2, int n_items, int chunks, int chunk_len, unsigned* __restrict__ ctr,
+              double* __restrict__ part, unsigned long long* __restrict__ counter) {
     __shared__ float4 sj[kD32Tile];
     __shared__ float2 ss[kD32Tile];
-    const int t0 = blockIdx.x * (kD32Threads * kD32Per);
-    const double4 ref = sbody[t0];
-    float bx[kD32Per], by[kD32Per], bz[kD32Per];
-    float sx[kD32Per], sy[kD32Per], sz[kD32Per], cx[kD32Per], cy[kD32Per], cz[kD32Per];
-#pragma unroll
-    for (int u = 0; u < kD32Per; u++) {
-        const int i = t0 + u * kD32Threads + threadIdx.x;
-        const double4 b = sbody[i < n ? i : n - 1];
-        bx[u] = (float)(b.x - ref.x);
-        by[u] = (float)(b.y - ref.y);
-        bz[u] = (float)(b.z - ref.z);
-        sx[u] = sy[u] = sz[u] = cx[u] = cy[u] = cz[u] = 0.f;
-    }
-    for (int base = 0; base < n; base += kD32Tile) {
-        const int j = base + threadIdx.x;
-        if (j < n) {
-            const double4 q = sbody[j];
-            sj[threadIdx.x] = make_float4((float)(q.x - ref.x), (float)(q.y - ref.y),
-                                          (float)(q.z - ref.z), (float)q.w);
-            if (SHELL) {
-                const float R = srad[j];
-                const float id = rsqrtf(R * R + eps2);
-                ss[threadIdx.x] = make_float2(R > 0.f ? R * R : 0.f, (float)q.w * id * id * id);
-            }
-        } else {
-            sj[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (SHELL) ss[threadIdx.x] = make_float2(0.f, 0.f);
-        }
+    __shared__ double s_box[4][kD32Threads / 32];
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(ctr, 1u);
         __syncthreads();
-        const int cnt = min(kD32Tile, n - base);
-        float tx[kD32Per], ty[kD32Per], tz[kD32Per];
+        const int it = s_item;
+        __syncthreads();  // every thread has the item before thread 0 fetches the next
+        if (it >= n_items) break;
+        const int tile = it / chunks, chunk = it - tile * chunks;
+        const int t0 = tile * (kD32Threads * kD32Per);
+        const int j0 = chunk * chunk_len, j1 = min(n, j0 + chunk_len);
+        // reference point: the target tile's centre of mass (the FP32
+        // coordinates are most precise where the mass is)
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};  // m, m x, m y, m z
 #pragma unroll
-        for (int u = 0; u < kD32Per; u++) tx[u] = ty[u] = tz[u] = 0.f;
-#pragma unroll 8
-        for (int k = 0; k < cnt; k++) {
-            const float4 q = sj[k];
-            float2 sh;
-            if (SHELL) sh = ss[k];
+        for (int u = 0; u < kD32Per; u++) {
+            const int i = t0 + u * kD32Threads + threadIdx.x;
+            if (i < n) {
+                const double4 b = sbody[i];
+                acc[0] += b.w;
+                acc[1] += b.w * b.x;
+                acc[2] += b.w * b.y;
+                acc[3] += b.w * b.z;
+            }
+        }
+        for (int k = 0; k < 4; k++)
+            for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xFFFFFFFFu, acc[k], o);
+        if ((threadIdx.x & 31) == 0)
+            for (int k = 0; k < 4; k++) s_box[k][threadIdx.x >> 5] = acc[k];
+        __syncthreads();
+        double4 ref;
+        {
+            double m = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+            for (int w = 0; w < kD32Threads / 32; w++) {
+                m += s_box[0][w];
+                mx += s_box[1][w];
+                my += s_box[2][w];
+                mz += s_box[3][w];
+            }
+            ref = m > 0.0 ? make_double4(mx / m, my / m, mz / m, 0.0) : sbody[t0];
+        }
+        float bx[kD32Per], by[kD32Per], bz[kD32Per];
+        float sx[kD32Per], sy[kD32Per], sz[kD32Per], cx[kD32Per], cy[kD32Per], cz[kD32Per];
+#pragma unroll
+        for (int u = 0; u < kD32Per; u++) {
+            const int i = t0 + u * kD32Threads + threadIdx.x;
+            const double4 b = sbody[i < n ? i : n - 1];
+            bx[u] = (float)(b.x - ref.x);
+            by[u] = (float)(b.y - ref.y);
+            bz[u] = (float)(b.z - ref.z);
+            sx[u] = sy[u] = sz[u] = cx[u] = cy[u] = cz[u] = 0.f;
+        }
+        for (int base = j0; base < j1; base += kD32Tile) {
+            const int j = base + threadIdx.x;
+            if (j < j1) {
+                const double4 q = sbody[j];
+                sj[threadIdx.x] = make_float4((float)(q.x - ref.x), (float)(q.y - ref.y),
+                                              (float)(q.z - ref.z), (float)q.w);
+                if (SHELL) {
+                    const float R = srad[j];
+                    const float id = rsqrtf(R * R + eps2);
+                    ss[threadIdx.x] = make_float2(R > 0.f ? R * R : 0.f, (float)q.w * id * id * id);
+                }
+            } else {
+                sj[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (SHELL) ss[threadIdx.x] = make_float2(0.f, 0.f);
+            }
+            __syncthreads();
+            const int cnt = min(kD32Tile, j1 - base);
+            float tx[kD32Per], ty[kD32Per], tz[kD32Per];
+#pragma unroll
+            for (int u = 0; u < kD32Per; u++) tx[u] = ty[u] = tz[u] = 0.f;
+#pragma unroll 4
+            for (int k = 0; k < cnt; k++) {
+                const float4 q = sj[k];
+                float2 sh;
+                if (SHELL) sh = ss[k];
+#pragma unroll
+                for (int u = 0; u < kD32Per; u++) {
+                    const float dx = bx[u] - q.x, dy = by[u] - q.y, dz = bz[u] - q.z;
+                    float f;
+                    if (SHELL) {
+                        const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float r2 = raw + eps2;
+                        const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrt_ftz(r2);
+                        f = q.w * (inv * inv * inv);
+                        if (raw < sh.x) f = sh.y;
+                    } else {
+                        // eps^2 folded into the first FMA of r^2
+                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+                        const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrt_ftz(r2);
+                        f = q.w * (inv * inv * inv);
+                    }
+                    tx[u] = fmaf(-f, dx, tx[u]);
+                    ty[u] = fmaf(-f, dy, ty[u]);
+                    tz[u] = fmaf(-f, dz, tz[u]);
+                }
+            }
 #pragma unroll
             for (int u = 0; u < kD32Per; u++) {
-                const float dx = bx[u] - q.x, dy = by[u] - q.y, dz = bz[u] - q.z;
-                const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const float r2 = raw + eps2;
-                const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrtf(r2);
-                float f = q.w * (inv * inv * inv);
-                if (SHELL && raw < sh.x) f = sh.y;
-                tx[u] = fmaf(-f, dx, tx[u]);
-                ty[u] = fmaf(-f, dy, ty[u]);
-                tz[u] = fmaf(-f, dz, tz[u]);
+                kahan32(sx[u], cx[u], tx[u]);
+                kahan32(sy[u], cy[u], ty[u]);
+                kahan32(sz[u], cz[u], tz[u]);
             }
+            __syncthreads();
         }
 #pragma unroll
         for (int u = 0; u < kD32Per; u++) {
-            kahan32(sx[u], cx[u], tx[u]);
-            kahan32(sy[u], cy[u], ty[u]);
-            kahan32(sz[u], cz[u], tz[u]);
+            const int i = t0 + u * kD32Threads + threadIdx.x;
+            if (i < n) {
+                part[(size_t)(chunk * 3 + 0) * n + i] = (double)sx[u] - (double)cx[u];
+                part[(size_t)(chunk * 3 + 1) * n + i] = (double)sy[u] - (double)cy[u];
+                part[(size_t)(chunk * 3 + 2) * n + i] = (double)sz[u] - (double)cz[u];
+            }
         }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int u = 0; u < kD32Per; u++) {
-        const int i = t0 + u * kD32Threads + threadIdx.x;
-        if (i < n) {
-            const uint32_t row = sidx[i];
-            ax[row] = (double)sx[u] - (double)cx[u];
-            ay[row] = (double)sy[u] - (double)cy[u];
-            az[row] = (double)sz[u] - (double)cz[u];
+        if (threadIdx.x == 0 && counter) {
+            const int nt = min(kD32Threads * kD32Per, n - t0);
+            atomicAdd(counter, (unsigned long long)nt * (unsigned long long)(j1 - j0));
         }
     }
-    if (threadIdx.x == 0 && counter) {
-        const int nt = min(kD32Threads * kD32Per, n - t0);
-        atomicAdd(counter, (unsigned long long)nt * (unsigned long long)n);
-    }
+}
+
+// Sum of the chunk partials in chunk order, written by body row.
+__global__ void k_direct_reduce(int n, int chunks, const double* __restrict__ part,
+                                const uint32_t* __restrict__ sidx, double* __restrict__ ax,
+                                double* __restrict__ ay, double* __restrict__ az) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int c = 0; c < chunks; c++)
+        for (int k = 0; k < 3; k++) s[k] += part[(size_t)(c * 3 + k) * n + i];
+    const uint32_t row = sidx[i];
+    ax[row] = s[0];
+    ay[row] = s[1];
+    az[row] = s[2];
 }
 
 // The arithmetic is split in two phases so that the costly per-pair part
@@ -213,17 +285,33 @@ void direct_fp64(cudaStream_t st, int n, const double* px, const double* py, con
 
 void direct_fp32(cudaStream_t st, int n, const double4* sbody, const float* srad,
                  const uint32_t* sidx, double eps, bool shell, double* ax, double* ay,
-                 double* az, unsigned long long* counter) {
+                 double* az, unsigned long long* counter, void* scratch, size_t scratch_bytes,
+                 unsigned* ctr, int sms) {
     if (n <= 0) return;
     const float eps2 = (float)(eps * eps);
-    const int g = ceil_div(n, kD32Threads * kD32Per);
-    if (eps2 > 0.f) {
-        if (shell) k_direct_fp32<true, false><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
-        else k_direct_fp32<false, false><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
-    } else {
-        if (shell) k_direct_fp32<true, true><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
-        else k_direct_fp32<false, true><<<g, kD32Threads, 0, st>>>(n, sbody, srad, sidx, eps2, ax, ay, az, counter);
-    }
+    using K = void (*)(int, const double4*, const float*, float, int, int, int, unsigned*,
+                       double*, unsigned long long*);
+    const K k = eps2 > 0.f ? (shell ? k_direct_fp32<true, false> : k_direct_fp32<false, false>)
+                           : (shell ? k_direct_fp32<true, true> : k_direct_fp32<false, true>);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kD32Threads, 0);
+    const int resident = sms * (per_sm > 0 ? per_sm : 1);
+    const int tiles = ceil_div(n, kD32Threads * kD32Per);
+    // enough items for about 8 waves, chunks of at least kD32MinChunk
+    // sources, partials within the scratch
+    long long chunks = ceil_div(8LL * resident, tiles);
+    chunks = std::min<long long>(chunks, std::max(1, ceil_div(n, kD32MinChunk)));
+    chunks = std::min<long long>(chunks, (long long)(scratch_bytes / (sizeof(double) * 3 * (size_t)n)));
+    if (chunks < 1) chunks = 1;
+    const int chunk_len = ceil_div(n, (int)chunks);
+    const int nchunks = ceil_div(n, chunk_len);
+    const int items = tiles * nchunks;
+    cudaMemsetAsync(ctr, 0, sizeof(unsigned), st);
+    k<<<std::min(items, resident), kD32Threads, 0, st>>>(n, sbody, srad, eps2, items, nchunks,
+                                                         chunk_len, ctr, (double*)scratch,
+                                                         counter);
+    k_direct_reduce<<<ceil_div(n, 256), 256, 0, st>>>(n, nchunks, (const double*)scratch, sidx,
+                                                      ax, ay, az);
 }
 
 }  // namespace nb

@@ -255,8 +255,10 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     record(h, 1);
     if (mode == NB_MODE_DIRECT) {
         record(h, 2);
+        // the walk tree's memory is idle in this mode and holds the chunk partials
         nb::direct_fp32(h->st, na, h->sbody, h->srad, h->vals0, eps, shell, h->s.ax, h->s.ay,
-                        h->s.az, &sc->counters[1]);
+                        h->s.az, &sc->counters[1], h->tree_mem, nb::tree_bytes(h->capacity),
+                        &sc->group_ctr, h->sms);
     } else if (mode == NB_MODE_BARNES_HUT || mode == NB_MODE_BARNES_HUT_REF) {
         const bool ref = mode == NB_MODE_BARNES_HUT_REF;
         nb::tree_build(h->st, h->tree, na, h->keys0, h->sbody, shell ? h->srad : nullptr, sc->cube,

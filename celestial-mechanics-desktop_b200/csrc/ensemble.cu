@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(TPB) k_ens_direct(EnsDirect a) {
                 for (int k = 0; k < TPT; k++) {
                     const float dx = q.x - xi[k], dy = q.y - yi[k], dz = q.z - zi[k];
                     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, a.eps2)));
-                    float inv = rsqrtf(r2);
+                    float inv = rsqrt_ftz(r2);
                     if (GUARD) inv = r2 > 0.f ? inv : 0.f;
                     const float s = q.w * inv * inv * inv;
                     tx[k] = fmaf(dx, s, tx[k]);

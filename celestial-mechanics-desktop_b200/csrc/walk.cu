@@ -148,7 +148,7 @@ k_walk_group(WalkArgs a) {
                 const float4 A = c0[j];
                 const float dx = bx - A.x, dy = by - A.y, dz = bz - A.z;
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-                const float inv = rsqrtf(r2);
+                const float inv = rsqrt_ftz(r2);
                 const float inv2 = inv * inv;
                 const float inv3 = inv * inv2;
                 if (QUAD) {
@@ -190,7 +190,7 @@ k_walk_group(WalkArgs a) {
                 const float dx = bx - P.x, dy = by - P.y, dz = bz - P.z;
                 const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 const float r2 = raw + eps2;
-                const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrtf(r2);
+                const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrt_ftz(r2);
                 float f = P.w * (inv * inv * inv);
                 if (SHELL) {
                     const float2 S = p1[j];
