@@ -24,11 +24,15 @@
 
 namespace nb {
 
-constexpr int kD32Threads = 256;
+#ifndef NB_D32_THREADS
+#define NB_D32_THREADS 256
+#endif
+constexpr int kD32Threads = NB_D32_THREADS;
 #ifndef NB_D32_PER
 #define NB_D32_PER 4
 #endif
-constexpr int kD32Per = NB_D32_PER;  // targets per thread
+constexpr int kD32Per = NB_D32_PER;  // targets per thread (even: packed in pairs)
+static_assert(kD32Per % 2 == 0, "targets are packed two per f32x2 register");
 constexpr int kD32Tile = kD32Threads;
 constexpr int kD32MinChunk = 4096;    // sources per chunk at least
 
@@ -50,6 +54,7 @@ k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict_
               float eps2, int n_items, int chunks, int chunk_len, unsigned* __restrict__ ctr,
               double* __restrict__ part, unsigned long long* __restrict__ counter) {
     __shared__ float4 sj[kD32Tile];
+    __shared__ float4 sj2[kD32Tile];
     __shared__ float2 ss[kD32Tile];
     __shared__ double s_box[4][kD32Threads / 32];
     __shared__ int s_item;
@@ -105,48 +110,88 @@ k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict_
         }
         for (int base = j0; base < j1; base += kD32Tile) {
             const int j = base + threadIdx.x;
+            float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            float R = 0.f;
             if (j < j1) {
                 const double4 q = sbody[j];
-                sj[threadIdx.x] = make_float4((float)(q.x - ref.x), (float)(q.y - ref.y),
-                                              (float)(q.z - ref.z), (float)q.w);
-                if (SHELL) {
-                    const float R = srad[j];
-                    const float id = rsqrtf(R * R + eps2);
-                    ss[threadIdx.x] = make_float2(R > 0.f ? R * R : 0.f, (float)q.w * id * id * id);
-                }
+                q4 = make_float4((float)(q.x - ref.x), (float)(q.y - ref.y), (float)(q.z - ref.z),
+                                 (float)q.w);
+                if (SHELL) R = srad[j];
+            }
+            if constexpr (SHELL) {
+                sj[threadIdx.x] = q4;
+                const float id = rsqrtf(R * R + eps2);
+                ss[threadIdx.x] =
+                    j < j1 ? make_float2(R > 0.f ? R * R : 0.f, q4.w * id * id * id) : make_float2(0.f, 0.f);
             } else {
-                sj[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (SHELL) ss[threadIdx.x] = make_float2(0.f, 0.f);
+                // each source duplicated into both halves of the packed pairs
+                sj[threadIdx.x] = make_float4(q4.x, q4.x, q4.y, q4.y);
+                sj2[threadIdx.x] = make_float4(q4.z, q4.z, q4.w, q4.w);
             }
             __syncthreads();
             const int cnt = min(kD32Tile, j1 - base);
             float tx[kD32Per], ty[kD32Per], tz[kD32Per];
 #pragma unroll
             for (int u = 0; u < kD32Per; u++) tx[u] = ty[u] = tz[u] = 0.f;
+            if constexpr (SHELL) {
 #pragma unroll 4
-            for (int k = 0; k < cnt; k++) {
-                const float4 q = sj[k];
-                float2 sh;
-                if (SHELL) sh = ss[k];
+                for (int k = 0; k < cnt; k++) {
+                    const float4 q = sj[k];
+                    const float2 sh = ss[k];
 #pragma unroll
-                for (int u = 0; u < kD32Per; u++) {
-                    const float dx = bx[u] - q.x, dy = by[u] - q.y, dz = bz[u] - q.z;
-                    float f;
-                    if (SHELL) {
+                    for (int u = 0; u < kD32Per; u++) {
+                        const float dx = bx[u] - q.x, dy = by[u] - q.y, dz = bz[u] - q.z;
                         const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                         const float r2 = raw + eps2;
                         const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrt_ftz(r2);
-                        f = q.w * (inv * inv * inv);
+                        float f = q.w * (inv * inv * inv);
                         if (raw < sh.x) f = sh.y;
-                    } else {
-                        // eps^2 folded into the first FMA of r^2
-                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-                        const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrt_ftz(r2);
-                        f = q.w * (inv * inv * inv);
+                        tx[u] = fmaf(-f, dx, tx[u]);
+                        ty[u] = fmaf(-f, dy, ty[u]);
+                        tz[u] = fmaf(-f, dz, tz[u]);
                     }
-                    tx[u] = fmaf(-f, dx, tx[u]);
-                    ty[u] = fmaf(-f, dy, ty[u]);
-                    tz[u] = fmaf(-f, dz, tz[u]);
+                }
+            } else {
+                // two targets per packed instruction; d = q - b, so each half
+                // rounds exactly as fmaf(-f, b - q, t) and fmaf(b - q, b - q, .)
+                constexpr int P = kD32Per / 2;
+                f32x2 BX[P], BY[P], BZ[P], AX[P], AY[P], AZ[P];
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    BX[p] = pk2(bx[2 * p], bx[2 * p + 1]);
+                    BY[p] = pk2(by[2 * p], by[2 * p + 1]);
+                    BZ[p] = pk2(bz[2 * p], bz[2 * p + 1]);
+                    AX[p] = AY[p] = AZ[p] = 0ull;
+                }
+                const f32x2 E2 = pk2(eps2, eps2);
+#pragma unroll 4
+                for (int k = 0; k < cnt; k++) {
+                    const float4 qa = sj[k], qb = sj2[k];
+                    const f32x2 qx = pk2(qa.x, qa.y), qy = pk2(qa.z, qa.w);
+                    const f32x2 qz = pk2(qb.x, qb.y), qm = pk2(qb.z, qb.w);
+#pragma unroll
+                    for (int p = 0; p < P; p++) {
+                        const f32x2 dx = sub2(qx, BX[p]), dy = sub2(qy, BY[p]), dz = sub2(qz, BZ[p]);
+                        const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+                        float ra, rb;
+                        upk2(r2, ra, rb);
+                        float ia = rsqrt_ftz(ra), ib = rsqrt_ftz(rb);
+                        if (GUARD) {
+                            ia = ra > 0.f ? ia : 0.f;
+                            ib = rb > 0.f ? ib : 0.f;
+                        }
+                        const f32x2 inv = pk2(ia, ib);
+                        const f32x2 f = mul2(mul2(mul2(inv, inv), inv), qm);
+                        AX[p] = fma2(f, dx, AX[p]);
+                        AY[p] = fma2(f, dy, AY[p]);
+                        AZ[p] = fma2(f, dz, AZ[p]);
+                    }
+                }
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    upk2(AX[p], tx[2 * p], tx[2 * p + 1]);
+                    upk2(AY[p], ty[2 * p], ty[2 * p + 1]);
+                    upk2(AZ[p], tz[2 * p], tz[2 * p + 1]);
                 }
             }
 #pragma unroll

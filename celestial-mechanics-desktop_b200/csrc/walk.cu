@@ -66,11 +66,14 @@ k_walk_group(WalkArgs a) {
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* base = s_walk + warp * kWarpFloats;
-    float4* c0 = (float4*)base;                      // rel com xyz, mass
-    float4* c1 = c0 + kCellCap;                      // Qxx, Qyy, Qzz, Qxy
-    float2* c2 = (float2*)(c1 + kCellCap);           // Qxz, Qyz
-    float4* p0 = (float4*)(c2 + kCellCap);           // rel xyz, mass
-    float2* p1 = (float2*)(p0 + kPartCap);           // R^2, m / (R^2 + eps^2)^1.5
+    // Interaction lists in a pair-blocked layout: field f of entry e sits at
+    // [(e / 2) * W + 2 f + e % 2], so one 16-byte load returns two fields of
+    // entries 2m and 2m+1 as register pairs for the packed f32x2 arithmetic.
+    // cells (W = 20): rel x, y, z, -mass, Qxx, Qyy, Qzz, Qxy, Qxz, Qyz
+    // bodies (W = 8): rel x, y, z, -mass
+    float* cbuf = base;
+    float* pbuf = base + kCellCap * 10;
+    float2* p1 = (float2*)(pbuf + kPartCap * 4);     // R^2, m / (R^2 + eps^2)^1.5
     int* p2 = (int*)(p1 + kPartCap);                 // sorted index
     int* fa = a.front + (size_t)(blockIdx.x * kWalkWarps + warp) * a.front_cap;
     const float eps2 = (float)a.eps2;
@@ -143,34 +146,90 @@ k_walk_group(WalkArgs a) {
 
         auto flush_cells = [&]() {
             float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
+            if constexpr (!POT) {
+                // an odd count is padded with a massless, quadrupole-free entry
+                // far away, whose terms are exactly zero
+                if (nc & 1) {
+                    if (lane < 10) cbuf[(nc >> 1) * 20 + lane * 2 + 1] = lane < 3 ? 1e15f : 0.f;
+                    __syncwarp();
+                }
+                const int npair = (nc + 1) >> 1;
+                const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
+                const f32x2 E2 = pk2(eps2, eps2), M25 = pk2(-2.5f, -2.5f);
+                f32x2 TX = 0ull, TY = 0ull, TZ = 0ull;
+#pragma unroll 2
+                for (int m = rep; m < npair; m += nrep) {
+                    const float4* blk = (const float4*)(cbuf + m * 20);
+                    const float4 v0 = blk[0], v1 = blk[1];
+                    const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
+                    const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
+                    const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
+                    const f32x2 nm = pk2(v1.z, v1.w);  // -mass
+                    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+                    float ra, rb;
+                    upk2(r2, ra, rb);
+                    const f32x2 inv = pk2(rsqrt_ftz(ra), rsqrt_ftz(rb));
+                    const f32x2 inv2 = mul2(inv, inv);
+                    const f32x2 inv3 = mul2(inv, inv2);
+                    if constexpr (QUAD) {
+                        const float4 v2 = blk[2], v3 = blk[3], v4 = blk[4];
+                        const f32x2 qxx = pk2(v2.x, v2.y), qyy = pk2(v2.z, v2.w);
+                        const f32x2 qzz = pk2(v3.x, v3.y), qxy = pk2(v3.z, v3.w);
+                        const f32x2 qxz = pk2(v4.x, v4.y), qyz = pk2(v4.z, v4.w);
+                        const f32x2 qx = fma2(qxx, dx, fma2(qxy, dy, mul2(qxz, dz)));
+                        const f32x2 qy = fma2(qxy, dx, fma2(qyy, dy, mul2(qyz, dz)));
+                        const f32x2 qz = fma2(qxz, dx, fma2(qyz, dy, mul2(qzz, dz)));
+                        const f32x2 rqr = fma2(dx, qx, fma2(dy, qy, mul2(dz, qz)));
+                        const f32x2 inv5 = mul2(inv3, inv2);
+                        // a = -M r / r^3 + Q r / r^5 - (5/2) (r.Q.r) r / r^7
+                        const f32x2 f = fma2(mul2(M25, rqr), mul2(inv5, inv2), mul2(nm, inv3));
+                        TX = fma2(f, dx, fma2(qx, inv5, TX));
+                        TY = fma2(f, dy, fma2(qy, inv5, TY));
+                        TZ = fma2(f, dz, fma2(qz, inv5, TZ));
+                    } else {
+                        const f32x2 f = mul2(nm, inv3);
+                        TX = fma2(f, dx, TX);
+                        TY = fma2(f, dy, TY);
+                        TZ = fma2(f, dz, TZ);
+                    }
+                }
+                float a0, a1;
+                upk2(TX, a0, a1);
+                tx = a0 + a1;
+                upk2(TY, a0, a1);
+                ty = a0 + a1;
+                upk2(TZ, a0, a1);
+                tz = a0 + a1;
+            } else {
 #pragma unroll 4
-            for (int j = rep; j < nc; j += nrep) {
-                const float4 A = c0[j];
-                const float dx = bx - A.x, dy = by - A.y, dz = bz - A.z;
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-                const float inv = rsqrt_ftz(r2);
-                const float inv2 = inv * inv;
-                const float inv3 = inv * inv2;
-                if (QUAD) {
-                    const float4 B = c1[j];  // Qxx, Qyy, Qzz, Qxy
-                    const float2 C = c2[j];  // Qxz, Qyz
-                    const float qx = fmaf(B.x, dx, fmaf(B.w, dy, C.x * dz));
-                    const float qy = fmaf(B.w, dx, fmaf(B.y, dy, C.y * dz));
-                    const float qz = fmaf(C.x, dx, fmaf(C.y, dy, B.z * dz));
-                    const float rqr = fmaf(dx, qx, fmaf(dy, qy, dz * qz));
-                    const float inv5 = inv3 * inv2;
-                    // a = -M r / r^3 + Q r / r^5 - (5/2) (r.Q.r) r / r^7
-                    const float f = fmaf(-2.5f * rqr, inv5 * inv2, -A.w * inv3);
-                    tx = fmaf(f, dx, fmaf(qx, inv5, tx));
-                    ty = fmaf(f, dy, fmaf(qy, inv5, ty));
-                    tz = fmaf(f, dz, fmaf(qz, inv5, tz));
-                    if (POT) tp = fmaf(-0.5f * rqr, inv5, fmaf(-A.w, inv, tp));
-                } else {
-                    const float f = -A.w * inv3;
-                    tx = fmaf(f, dx, tx);
-                    ty = fmaf(f, dy, ty);
-                    tz = fmaf(f, dz, tz);
-                    if (POT) tp = fmaf(-A.w, inv, tp);
+                for (int j = rep; j < nc; j += nrep) {
+                    const float* e = cbuf + (j >> 1) * 20 + (j & 1);
+                    const float ax_ = e[0], ay_ = e[2], az_ = e[4], am = -e[6];
+                    const float dx = bx - ax_, dy = by - ay_, dz = bz - az_;
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+                    const float inv = rsqrt_ftz(r2);
+                    const float inv2 = inv * inv;
+                    const float inv3 = inv * inv2;
+                    if (QUAD) {
+                        const float qxx = e[8], qyy = e[10], qzz = e[12], qxy = e[14];
+                        const float qxz = e[16], qyz = e[18];
+                        const float qx = fmaf(qxx, dx, fmaf(qxy, dy, qxz * dz));
+                        const float qy = fmaf(qxy, dx, fmaf(qyy, dy, qyz * dz));
+                        const float qz = fmaf(qxz, dx, fmaf(qyz, dy, qzz * dz));
+                        const float rqr = fmaf(dx, qx, fmaf(dy, qy, dz * qz));
+                        const float inv5 = inv3 * inv2;
+                        const float f = fmaf(-2.5f * rqr, inv5 * inv2, -am * inv3);
+                        tx = fmaf(f, dx, fmaf(qx, inv5, tx));
+                        ty = fmaf(f, dy, fmaf(qy, inv5, ty));
+                        tz = fmaf(f, dz, fmaf(qz, inv5, tz));
+                        tp = fmaf(-0.5f * rqr, inv5, fmaf(-am, inv, tp));
+                    } else {
+                        const float f = -am * inv3;
+                        tx = fmaf(f, dx, tx);
+                        ty = fmaf(f, dy, ty);
+                        tz = fmaf(f, dz, tz);
+                        tp = fmaf(-am, inv, tp);
+                    }
                 }
             }
             kahan(sax, cax, tx);
@@ -184,23 +243,61 @@ k_walk_group(WalkArgs a) {
         };
         auto flush_parts = [&]() {
             float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
-#pragma unroll 4
-            for (int j = rep; j < np; j += nrep) {
-                const float4 P = p0[j];
-                const float dx = bx - P.x, dy = by - P.y, dz = bz - P.z;
-                const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const float r2 = raw + eps2;
-                const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrt_ftz(r2);
-                float f = P.w * (inv * inv * inv);
-                if (SHELL) {
-                    const float2 S = p1[j];
-                    if (raw < S.x) f = S.y;
+            if constexpr (!SHELL && !POT) {
+                if (np & 1) {  // pad: a massless body far away
+                    if (lane < 4) pbuf[(np >> 1) * 8 + lane * 2 + 1] = lane < 3 ? 1e15f : 0.f;
+                    __syncwarp();
                 }
-                tx = fmaf(-f, dx, tx);
-                ty = fmaf(-f, dy, ty);
-                tz = fmaf(-f, dz, tz);
-                if (POT) {
-                    if (p2[j] != s) tp = fmaf(-P.w, inv, tp);
+                const int npair = (np + 1) >> 1;
+                const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
+                const f32x2 E2 = pk2(eps2, eps2);
+                f32x2 TX = 0ull, TY = 0ull, TZ = 0ull;
+#pragma unroll 4
+                for (int m = rep; m < npair; m += nrep) {
+                    const float4* blk = (const float4*)(pbuf + m * 8);
+                    const float4 v0 = blk[0], v1 = blk[1];
+                    const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
+                    const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
+                    const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
+                    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+                    float ra, rb;
+                    upk2(r2, ra, rb);
+                    const float ia = (GUARD && !(ra > 0.f)) ? 0.f : rsqrt_ftz(ra);
+                    const float ib = (GUARD && !(rb > 0.f)) ? 0.f : rsqrt_ftz(rb);
+                    const f32x2 inv = pk2(ia, ib);
+                    // -(m / r^3); the term is -(m/r^3) (b - p), as fmaf(-f, dx, t)
+                    const f32x2 f = mul2(pk2(v1.z, v1.w), mul2(mul2(inv, inv), inv));
+                    TX = fma2(f, dx, TX);
+                    TY = fma2(f, dy, TY);
+                    TZ = fma2(f, dz, TZ);
+                }
+                float a0, a1;
+                upk2(TX, a0, a1);
+                tx = a0 + a1;
+                upk2(TY, a0, a1);
+                ty = a0 + a1;
+                upk2(TZ, a0, a1);
+                tz = a0 + a1;
+            } else {
+#pragma unroll 4
+                for (int j = rep; j < np; j += nrep) {
+                    const float* e = pbuf + (j >> 1) * 8 + (j & 1);
+                    const float px_ = e[0], py_ = e[2], pz_ = e[4], pm = -e[6];
+                    const float dx = bx - px_, dy = by - py_, dz = bz - pz_;
+                    const float raw = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float r2 = raw + eps2;
+                    const float inv = (GUARD && !(r2 > 0.f)) ? 0.f : rsqrt_ftz(r2);
+                    float f = pm * (inv * inv * inv);
+                    if (SHELL) {
+                        const float2 S = p1[j];
+                        if (raw < S.x) f = S.y;
+                    }
+                    tx = fmaf(-f, dx, tx);
+                    ty = fmaf(-f, dy, ty);
+                    tz = fmaf(-f, dz, tz);
+                    if (POT) {
+                        if (p2[j] != s) tp = fmaf(-pm, inv, tp);
+                    }
                 }
             }
             kahan(sax, cax, tx);
@@ -231,11 +328,19 @@ k_walk_group(WalkArgs a) {
                 if (nc + k > kCellCap) flush_cells();
                 if (take_cell) {
                     const int cs = nc + __popc(mcell & lanemask_lt());
-                    c0[cs] = make_float4(rx, ry, rz, mass);
+                    float* e = cbuf + (cs >> 1) * 20 + (cs & 1);
+                    e[0] = rx;
+                    e[2] = ry;
+                    e[4] = rz;
+                    e[6] = -mass;
                     if (QUAD) {
                         const float4 q = a.t.q0[node];  // Qxx, Qyy, Qxy, Qxz
-                        c1[cs] = make_float4(q.x, q.y, -(q.x + q.y), q.z);
-                        c2[cs] = make_float2(q.w, a.t.q1[node].x);
+                        e[8] = q.x;
+                        e[10] = q.y;
+                        e[12] = -(q.x + q.y);
+                        e[14] = q.z;
+                        e[16] = q.w;
+                        e[18] = a.t.q1[node].x;
                     }
                 }
                 nc += k;
@@ -273,8 +378,11 @@ k_walk_group(WalkArgs a) {
                 if (lane < take) {
                     const int bi = ofirst + (t - oexcl);
                     const double4 q = a.sbody[bi];
-                    p0[np + lane] = make_float4((float)(q.x - gcx), (float)(q.y - gcy),
-                                                (float)(q.z - gcz), (float)q.w);
+                    float* e = pbuf + ((np + lane) >> 1) * 8 + ((np + lane) & 1);
+                    e[0] = (float)(q.x - gcx);
+                    e[2] = (float)(q.y - gcy);
+                    e[4] = (float)(q.z - gcz);
+                    e[6] = -(float)q.w;
                     if (SHELL) {
                         const float R = a.srad[bi];
                         const float R2 = R * R;
