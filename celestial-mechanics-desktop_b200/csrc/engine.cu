@@ -73,6 +73,7 @@ struct nb_engine {
     bool mac_ready = false;               // parameters trained or set
     float mac_norm_host[nb::kMacNorm] = {0};
     nb::MacDev* mac_dev = nullptr;        // BF16 fragment image for the walk
+    float2* mac_node = nullptr;           // per-node screen terms (learned walk)
     nb::MacTrainImage* mac_ti = nullptr;  // transposed fragments for training
     float *mac_P = nullptr, *mac_m = nullptr, *mac_v = nullptr, *mac_G = nullptr;
     float *mac_norm = nullptr, *mac_loss = nullptr;
@@ -294,6 +295,8 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
             a.mac_theta_hi2 = (float)(h->mac_theta_hi * h->mac_theta_hi);
             a.samag = h->samag;
             a.mac = h->mac_dev;
+            nb::mac_node_terms(h->st, h->tree, na, h->mac_dev, h->mac_node);
+            a.mac_node = h->mac_node;
             a.mac_budget = (float)((h->mac_budget * 3.321928094887362 - h->mac_norm_host[16]) /
                                    h->mac_norm_host[17]);
             nb::walk_group(h->st, h->wcfg, a, true, false, false, 2);
@@ -441,6 +444,7 @@ NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
         if ((r = dalloc(h, &h->targets, cap)) || (r = dalloc(h, &h->tgt_out, 3 * cap))) break;
         if ((r = dalloc(h, &h->groups, cap))) break;
         if ((r = dalloc(h, &h->samag, cap))) break;
+        if ((r = dalloc(h, &h->mac_node, 2 * cap))) break;
         if ((r = dalloc(h, &h->mac_dev, 1)) || (r = dalloc(h, &h->mac_ti, 1))) break;
         if ((r = dalloc(h, &h->mac_P, nb::kMacParams)) || (r = dalloc(h, &h->mac_m, nb::kMacParams)) ||
             (r = dalloc(h, &h->mac_v, nb::kMacParams)) || (r = dalloc(h, &h->mac_G, nb::kMacParams)))

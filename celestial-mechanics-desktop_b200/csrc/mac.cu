@@ -375,6 +375,31 @@ void mac_adam(cudaStream_t st, float* P, const float* G, float* m, float* v, int
                                                             c2, 1e-8f);
 }
 
+// ---- per-node screen terms (learned walk) --------------------------------------
+
+// For every walk-tree node: the part of the linear screen that depends on the
+// cell only, scr_w0 log2(2h) + scr_w1 f1 + scr_w4 log2(count) (f0 = log2 2h
+// - log2 d and f1, f4 as in mac_features), and log2 of its mass.
+__global__ void k_mac_node_terms(TreeBufs t, const MacDev* __restrict__ w,
+                                 float2* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *t.n_nodes) return;
+    const float mass = (float)t.com[i].w;
+    const float4 q = t.q0[i];
+    const float4 q1 = t.q1[i];
+    const float s = 2.f * q1.y;
+    const float qyz = q1.x, qzz = -(q.x + q.y);
+    const float qn2 = q.x * q.x + q.y * q.y + qzz * qzz + 2.f * (q.z * q.z + q.w * q.w + qyz * qyz);
+    const float f1 = mac_log2(sqrtf(qn2) / (mass * s * s) + 1e-6f);
+    const float cn = w->scr_w[0] * mac_log2(s) + w->scr_w[1] * f1 +
+                     w->scr_w[4] * mac_log2((float)t.link[i].w);
+    out[i] = make_float2(cn, mac_log2(mass));
+}
+
+void mac_node_terms(cudaStream_t st, const TreeBufs& t, int n, const MacDev* w, float2* out) {
+    if (n > 0) k_mac_node_terms<<<ceil_div(2LL * n, 256), 256, 0, st>>>(t, w, out);
+}
+
 // ---- prediction (the walk's inference routine on given feature rows) -------
 
 __global__ void k_mac_predict(const float* __restrict__ X, int n, const MacDev* __restrict__ w,

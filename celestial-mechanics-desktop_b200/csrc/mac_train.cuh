@@ -26,5 +26,7 @@ void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order,
               int sms);
 void mac_adam(cudaStream_t st, float* P, const float* G, float* m, float* v, int step, float lr);
 void mac_predict(cudaStream_t st, const float* X, int n, const MacDev* w, float* out);
+// Per walk-tree node (2n slots, *t.n_nodes used): screen term and log2 mass.
+void mac_node_terms(cudaStream_t st, const TreeBufs& t, int n, const MacDev* w, float2* out);
 
 }  // namespace nb

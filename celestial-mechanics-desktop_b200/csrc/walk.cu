@@ -119,6 +119,7 @@ k_walk_group(WalkArgs a) {
         // smallest / largest |a| of the group's bodies (previous step), and
         // whether this group's candidates are recorded (harvest)
         float a_min = 0.f, a_max = 0.f, r_grp = 0.f;
+        float scr_g = 0.f, scr_w0 = 0.f, scr_w2 = 0.f, scr_w3 = 0.f, scr_mg = 0.f, scr_la = 0.f;
         bool sampled = false;
         if (MAC != kMacGeometric) {
             const float am = a.samag[valid ? s : grp.x];
@@ -130,6 +131,22 @@ k_walk_group(WalkArgs a) {
                 a_max = fmaxf(a_max, __shfl_xor_sync(FULL, a_max, o));
             }
             r_grp = fmaxf(ghx, fmaxf(ghy, ghz));
+            if (MAC == kMacLearned) {
+                // screen terms that depend on the group only, with the budget
+                // moved to this side: y - budget = scr_g + node term
+                // + scr_w0 log2 d^2 + scr_w2 f2 + scr_w3 f3
+                const float f5 = mac_log2((float)nvalid);
+                const float f7 = fminf(mac_log2(a_max / fmaxf(a_min, 1e-30f)), 60.f);
+                const float w6 = mac_ldf(&wmac->scr_w[6]);
+                scr_g = mac_ldf(&wmac->scr_b) + mac_ldf(&wmac->scr_w[5]) * f5 +
+                        mac_ldf(&wmac->scr_w[7]) * f7 -
+                        w6 * mac_log2(fmaxf(sqrtf(eps2), 1e-30f)) - a.mac_budget;
+                scr_w0 = 0.5f * (w6 - mac_ldf(&wmac->scr_w[0]));
+                scr_w2 = mac_ldf(&wmac->scr_w[2]);
+                scr_w3 = mac_ldf(&wmac->scr_w[3]);
+                scr_mg = mac_ldf(&wmac->lin_margin);
+                scr_la = mac_log2(fmaxf(a_min, 1e-30f));
+            }
             if (MAC == kMacHarvest) {
                 unsigned hsh = (unsigned)grp.x * 2654435761u ^ (unsigned)a.mac_seed;
                 hsh ^= hsh >> 15;
@@ -470,22 +487,18 @@ k_walk_group(WalkArgs a) {
                     // linear screen fitted to the network decides the clear
                     // cases; the network decides the rest.
                     bool unsure = false;
-                    float f[kMacIn];
                     if (in_band && lk.w == 1) {
                         take_cell = true;
                     } else if (in_band) {
-                        const float4 q = a.t.q0[node];
-                        const float qyz = a.t.q1[node].x, qzz = -(q.x + q.y);
-                        const float qn2 = q.x * q.x + q.y * q.y + qzz * qzz +
-                                          2.f * (q.z * q.z + q.w * q.w + qyz * qyz);
-                        mac_features(f, d2, half, mass, qn2, lk.w, r_grp, nvalid, a_min, a_max,
-                                     sqrtf(eps2));
-                        float yl = mac_ldf(&wmac->scr_b);
-#pragma unroll
-                        for (int k = 0; k < kMacIn; k++) yl = fmaf(mac_ldf(&wmac->scr_w[k]), f[k], yl);
-                        const float mg = mac_ldf(&wmac->lin_margin);
-                        if (yl < a.mac_budget - mg) take_cell = true;
-                        else if (yl <= a.mac_budget + mg) unsure = true;
+                        // the screen from its per-node and per-group parts:
+                        // only the distance-dependent features are formed here
+                        const float2 nt = a.mac_node[node];
+                        const float l2d2 = mac_log2(d2);
+                        const float f2 = fminf(fmaxf(nt.y - l2d2 - scr_la, -60.f), 60.f);
+                        const float f3 = mac_log2(fmaf(r_grp, rsqrt_ftz(d2), 1e-6f));
+                        const float yl = scr_g + nt.x + fmaf(scr_w0, l2d2, fmaf(scr_w2, f2, scr_w3 * f3));
+                        if (yl < -scr_mg) take_cell = true;
+                        else if (yl <= scr_mg) unsure = true;
                     }
                     const unsigned hard = __ballot_sync(FULL, unsure);
                     if (hard) {
@@ -493,6 +506,13 @@ k_walk_group(WalkArgs a) {
                         if (npend + nh > 32) flush_pending();
                         const int rank = npend + __popc(hard & lanemask_lt());
                         if (unsure) {
+                            float f[kMacIn];
+                            const float4 q = a.t.q0[node];
+                            const float qyz = a.t.q1[node].x, qzz = -(q.x + q.y);
+                            const float qn2 = q.x * q.x + q.y * q.y + qzz * qzz +
+                                              2.f * (q.z * q.z + q.w * q.w + qyz * qyz);
+                            mac_features(f, d2, half, mass, qn2, lk.w, r_grp, nvalid, a_min,
+                                         a_max, sqrtf(eps2));
 #pragma unroll
                             for (int k = 0; k < kMacIn; k += 2)
                                 xs[rank * 4 + k / 2] = pack_bf16(

@@ -26,6 +26,7 @@ struct WalkArgs {
     // learned MAC / harvest
     const float* samag;         // |a| of each sorted body from the previous step
     const MacDev* mac;          // network image (learned mode)
+    const float2* mac_node;     // per walk-tree node: screen term, log2 mass (learned mode)
     float mac_theta_hi2;        // band upper edge, (2h/d)^2
     float mac_budget;           // normalised log2 error budget (learned mode)
     MacRecord* records;         // harvest output
