@@ -873,7 +873,8 @@ def main():
         else:
             line = run_b200(args, ws, rank, local)
             if line is not None:
-                line["gpu_launches"] = launches_per_step() * args.steps
+                # the learned arm adds one kernel per step (per-node screen terms)
+                line["gpu_launches"] = (launches_per_step() + 1) * args.steps
                 print(json.dumps(line))
     finally:
         if ws > 1:

@@ -83,6 +83,22 @@ def test_mixed_systems_stay_isolated(spread):
         assert np.all(rms_dev[np.array(sizes) > 2048] < 1e-3)
 
 
+def test_zero_softening():
+    sizes = [300, 2500]
+    systems = _systems(sizes, seed=9)
+    with Ensemble(sizes, ds_max_n=2048) as ens:
+        ens.set_state(systems)
+        ens.compute_forces(0.0)
+        st = ens.get_state()
+        for s, b in enumerate(systems):
+            o0, o1 = ens.offsets[s], ens.offsets[s + 1]
+            want = oracle.direct_forces(b.px, b.py, b.pz, b.mass, b.active, 0.0)
+            got = [st[k][o0:o1] for k in ("ax", "ay", "az")]
+            assert all(np.all(np.isfinite(g)) for g in got)
+            rms = np.sqrt(np.mean(rel_err(got, want) ** 2))
+            assert rms < (1e-5 if sizes[s] <= 2048 else 1e-3), (s, rms)
+
+
 def test_every_direct_shape_and_autotune():
     sizes = [64, 200, 513, 1024, 2000]
     systems = _systems(sizes, seed=6)

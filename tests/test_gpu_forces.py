@@ -118,6 +118,17 @@ def test_bh_reference_mode_shell(engine, oracle):
     assert e.max() < 1e-9
 
 
+@pytest.mark.parametrize("mode,tol", [(MODE_DIRECT, 1e-5), (MODE_BARNES_HUT, 1e-3)])
+def test_zero_softening(engine, oracle, mode, tol):
+    # eps = 0: the self pair must give 0 (not 0 * inf) in every packed path
+    b = scenarios.plummer(5000, seed=9)
+    got = _forces(engine, b, 0.0, mode)
+    want = oracle.direct_forces(b.px, b.py, b.pz, b.mass, b.active, 0.0)
+    assert all(np.all(np.isfinite(g)) for g in got)
+    e = rel_err(got, want)
+    assert np.sqrt(np.mean(e ** 2)) < tol
+
+
 @pytest.mark.parametrize("n", [20_000, 200_000])
 def test_bh_group_walk_error_budget(engine, oracle, n):
     b = scenarios.plummer(n, seed=1)
