@@ -38,6 +38,7 @@ size_t tree_bytes(int cap) {
     b += 256;                                                          // align slack
     size_t w = 2 * c;
     b += w * 16 + w * 4 + w * 4 + w * 32 + w * 16 + w * 16 + w * 4 + 16;
+    b += 2 * w * 16;                                                   // body boxes
     return b + 16 * 64;
 }
 
@@ -56,6 +57,8 @@ void tree_carve(TreeBufs& t, void* base, int cap) {
     t.link = carve<int4>(p, w);
     t.q0 = carve<float4>(p, w);
     t.q1 = carve<float4>(p, w);
+    t.blo = carve<float4>(p, w);
+    t.bhi = carve<float4>(p, w);
     t.level = carve<int>(p, w);
     t.parent_bin = carve<int>(p, w);
     t.counter = carve<int>(p, w);
@@ -299,6 +302,7 @@ __global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody
         // leaf: moments straight from its bodies
         double M = 0, sx = 0, sy = 0, sz = 0;
         float rmax = 0.f;
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
         for (int b = lk.z; b < lk.z + lk.w; b++) {
             double4 p = sbody[b];
             M += p.w;
@@ -306,7 +310,13 @@ __global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody
             sy += p.w * p.y;
             sz += p.w * p.z;
             if (srad) rmax = fmaxf(rmax, srad[b]);
+            lo[0] = fmin(lo[0], p.x); lo[1] = fmin(lo[1], p.y); lo[2] = fmin(lo[2], p.z);
+            hi[0] = fmax(hi[0], p.x); hi[1] = fmax(hi[1], p.y); hi[2] = fmax(hi[2], p.z);
         }
+        t.blo[w] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
+                               __double2float_rd(lo[2]), 0.f);
+        t.bhi[w] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
+                               __double2float_ru(hi[2]), 0.f);
         double cx, cy, cz;
         if (M > 0) {
             cx = sx / M; cy = sy / M; cz = sz / M;
@@ -351,6 +361,14 @@ __global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody
             double2 b = __ldcg((const double2*)&t.com[pl.x] + 1);
             cx = a.x; cy = a.y; cz = b.x;
         }
+        float4 blo = make_float4(3e38f, 3e38f, 3e38f, 0.f), bhi = make_float4(-3e38f, -3e38f, -3e38f, 0.f);
+        for (int c = pl.x; c < pl.x + pl.y; c++) {
+            const float4 l = __ldcg(&t.blo[c]), h = __ldcg(&t.bhi[c]);
+            blo.x = fminf(blo.x, l.x); blo.y = fminf(blo.y, l.y); blo.z = fminf(blo.z, l.z);
+            bhi.x = fmaxf(bhi.x, h.x); bhi.y = fmaxf(bhi.y, h.y); bhi.z = fmaxf(bhi.z, h.z);
+        }
+        t.blo[p] = blo;
+        t.bhi[p] = bhi;
         double q[6] = {0, 0, 0, 0, 0, 0};
         for (int c = pl.x; c < pl.x + pl.y; c++) {
             double2 a = __ldcg((const double2*)&t.com[c]);

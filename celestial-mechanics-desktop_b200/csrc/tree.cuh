@@ -25,6 +25,8 @@ struct TreeBufs {
     double4* com;       // centre of mass (FP64) and mass
     float4* q0;         // Qxx, Qyy, Qxy, Qxz (traceless, about the COM)
     float4* q1;         // Qyz, cell half-size, max body radius, 0
+    float4* blo;        // bounding box of the node's bodies (xyz, rounded outwards)
+    float4* bhi;
     int* counter;       // bottom-up arrival counters
     int* n_nodes;       // device node count
     int capacity;       // bodies

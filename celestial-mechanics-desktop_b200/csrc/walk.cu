@@ -707,12 +707,28 @@ struct Box {
 };
 
 // Sibling runs are packed only while the packed box stays within `pack`
-// times the larger part's box: siblings that sit far apart in a sparse cell
-// would make one group whose opening test walks most of the tree.  (Measured
-// at N=1M: factor 2-2.5 raises lane fill from 0.30 to 0.57-0.71; from 3 on,
-// a few groups reach into the dense core and serialise ~1e6 list entries.)
-__global__ void k_find_groups(TreeBufs t, const double4* __restrict__ sbody,
-                              int2* __restrict__ groups, int* __restrict__ n_groups, double pack) {
+// times the larger part's box, and only while it does not reach into the
+// body box of a sibling of more than 32 bodies outside the run: siblings
+// that sit far apart in a sparse cell would otherwise make one group whose
+// box encloses a dense sibling (at the top levels, the whole core), and whose
+// opening test then walks the tree down to every body.  (Measured at N=1M: factor 2-2.5 raises
+// lane fill from 0.30 to 0.57-0.71.)
+__device__ __forceinline__ Box node_box(const TreeBufs& t, int c) {
+    const float4 l = t.blo[c], h = t.bhi[c];
+    Box b;
+    b.lo[0] = l.x; b.lo[1] = l.y; b.lo[2] = l.z;
+    b.hi[0] = h.x; b.hi[1] = h.y; b.hi[2] = h.z;
+    return b;
+}
+
+__device__ __forceinline__ bool boxes_meet(const Box& a, const Box& b) {
+    for (int k = 0; k < 3; k++)
+        if (a.hi[k] < b.lo[k] || b.hi[k] < a.lo[k]) return false;
+    return true;
+}
+
+__global__ void k_find_groups(TreeBufs t, int2* __restrict__ groups, int* __restrict__ n_groups,
+                              double pack) {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= *t.n_nodes) return;
     const int4 lk = t.link[w];
@@ -725,7 +741,7 @@ __global__ void k_find_groups(TreeBufs t, const double4* __restrict__ sbody,
             groups[atomicAdd(n_groups, 1)] = make_int2(lk.z + off, min(32, lk.w - off));
         return;
     }
-    int run_first = 0, run_cnt = 0;
+    int run_first = 0, run_cnt = 0, run_c0 = 0;
     Box run;
     run.empty();
     for (int c = lk.x; c < lk.x + lk.y; c++) {
@@ -735,20 +751,15 @@ __global__ void k_find_groups(TreeBufs t, const double4* __restrict__ sbody,
             run_cnt = 0;
             continue;
         }
-        Box cb;
-        cb.empty();
-        if (pack > 0.0)
-            for (int b = cl.z; b < cl.z + cl.w; b++) {
-                const double4 p = sbody[b];
-                cb.lo[0] = fmin(cb.lo[0], p.x); cb.hi[0] = fmax(cb.hi[0], p.x);
-                cb.lo[1] = fmin(cb.lo[1], p.y); cb.hi[1] = fmax(cb.hi[1], p.y);
-                cb.lo[2] = fmin(cb.lo[2], p.z); cb.hi[2] = fmax(cb.hi[2], p.z);
-            }
+        const Box cb = node_box(t, c);
         bool merge = false;
         if (pack > 0.0 && run_cnt > 0 && run_cnt + cl.w <= 32) {
             Box m = run;
             m.add(cb);
             merge = m.ext() <= pack * fmax(run.ext(), cb.ext());
+            for (int k = lk.x; merge && k < lk.x + lk.y; k++)
+                if ((k < run_c0 || k > c) && t.link[k].w > 32 && boxes_meet(m, node_box(t, k)))
+                    merge = false;
         }
         if (merge) {
             run_cnt += cl.w;
@@ -757,6 +768,7 @@ __global__ void k_find_groups(TreeBufs t, const double4* __restrict__ sbody,
             if (run_cnt) groups[atomicAdd(n_groups, 1)] = make_int2(run_first, run_cnt);
             run_first = cl.z;
             run_cnt = cl.w;
+            run_c0 = c;
             run = cb;
         }
     }
@@ -767,7 +779,7 @@ void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n
                  int* n_groups, double pack) {
     cudaMemsetAsync(n_groups, 0, sizeof(int), st);
     if (n > 0)
-        k_find_groups<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, sbody, groups, n_groups, pack);
+        k_find_groups<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, groups, n_groups, pack);
 }
 
 using WalkKernel = void (*)(WalkArgs);
