@@ -129,6 +129,19 @@ def test_zero_softening(engine, oracle, mode, tol):
     assert np.sqrt(np.mean(e ** 2)) < tol
 
 
+def test_group_work_bounded_at_2m(engine):
+    # A walk group packed from sparse siblings must not enclose a dense
+    # sibling: at N = 2^21 (seed 1) such a group once walked to every body.
+    n = 1 << 21
+    b = scenarios.plummer(n, seed=1)
+    engine.set_param(N.PARAM_THETA, 0.5)
+    engine.set_state(b, old_acc=False)
+    engine.step(1, 0.0, 1e-4, MODE_BARNES_HUT)
+    c = engine.counters()
+    assert c[N.C_MAX_GROUP_WORK] < 20_000, c[N.C_MAX_GROUP_WORK]
+    assert c[N.C_GROUPS] < n // 16  # packing still fills the warps
+
+
 @pytest.mark.parametrize("n", [20_000, 200_000])
 def test_bh_group_walk_error_budget(engine, oracle, n):
     b = scenarios.plummer(n, seed=1)
