@@ -320,6 +320,12 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
     w0 = time.time()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    audit = bool(flags & N.FLAG_LEARNED_MAC)
+    if audit:
+        # the sampled FP64 direct sum judges the learned MAC once per timed
+        # block (inside it); a failed audit would switch to the geometric MAC
+        eng.set_param(N.PARAM_MAC_AUDIT_SAMPLES, 1024)
+        eng.set_param(N.PARAM_MAC_AUDIT_INTERVAL, args.steps)
     torch.cuda.nvtx.range_push(label)
     t0.record(stream)
     acc = dict(walk=0.0, build=0.0, sort=0.0, tree=0.0, inter=0, flops=0.0, evals=0)
@@ -341,6 +347,12 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
     barrier(ws)
     clk = clocks.stop((w0, w1))
     ms = max_over_ranks(ws, t0.elapsed_time(t1))
+    audit_state = None
+    if audit:
+        audit_state = eng.mac_audit_state()
+        audit_state["interval_steps"] = args.steps
+        audit_state["samples"] = 1024
+        eng.set_param(N.PARAM_MAC_AUDIT_INTERVAL, 0)
     err = eng.force_error(ERR_SAMPLES, ERR_SEED, EPS)
     k = args.steps
     out = {"steps_per_s": sum_over_ranks(ws, k) / (ms / 1e3), "ms_per_step": ms / k,
@@ -349,7 +361,7 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
            "force_error": {"mean": err[0], "max": err[1], "rms": err[2]},
            "stage_ms": {s: acc[s] / k for s in ("build", "walk", "sort", "tree")},
            "walk_flops_per_step": acc["flops"] / k, "network_rows_per_step": acc["evals"] / k,
-           "clocks": clk}
+           "clocks": clk, "audit": audit_state}
     return out
 
 
@@ -445,6 +457,7 @@ def run_b200(args, ws, rank, local):
                                                         "uniformly sampled bodies, last step"),
             "learned": {"budget_log10": budget, "calibration_rms": rms_l,
                         "network_rows_per_step": arm_l["network_rows_per_step"],
+                        "audit_in_timed_region": arm_l["audit"],
                         "stage_ms": arm_l["stage_ms"], "training": train, "scan": scan_l},
             "geometric_same_error": {k: arm_g[k] for k in ("steps_per_s", "ms_per_step",
                                                            "interactions_per_s",

@@ -69,6 +69,11 @@ struct nb_engine {
     // learned MAC
     double mac_theta_lo = 0.35, mac_theta_hi = 1.0;
     double mac_screen_q = 0.9;             // residual quantile that sets the screen margin
+    // sampled FP64 audit of the learned MAC inside nb_step, geometric fallback
+    int mac_audit_every = 0, mac_audit_samples = 1024, mac_since_audit = 0;
+    double mac_audit_rms_max = 1e-3, mac_audit_last_rms = 0.0, mac_audit_last_max = 0.0;
+    int64_t mac_audits = 0;
+    bool mac_fallback = false;
     float mac_screen[nb::kMacScreen] = {0, 0, 0, 0, 0, 0, 0, 0, 0, INFINITY};
     bool mac_ready = false;               // parameters trained or set
     float mac_norm_host[nb::kMacNorm] = {0};
@@ -502,6 +507,10 @@ NB_API int32_t nb_set_param_f64(nb_engine* h, int32_t p, double v) {
             if (!(v > 0.0 && v < 4.0)) return fail(h, NB_ERR_INVALID_ARG, "theta_hi must be in (0, 4)");
             h->mac_theta_hi = v;
             return NB_OK;
+        case NB_PARAM_MAC_AUDIT_RMS:
+            if (!(v > 0.0)) return fail(h, NB_ERR_INVALID_ARG, "audit rms bound must be > 0");
+            h->mac_audit_rms_max = v;
+            return NB_OK;
         case NB_PARAM_MAC_SCREEN_QUANTILE:
             if (!(v >= 0.0 && v <= 1.0)) return fail(h, NB_ERR_INVALID_ARG, "screen quantile must be in [0, 1]");
             h->mac_screen_q = v;
@@ -525,6 +534,17 @@ NB_API int32_t nb_set_param_i32(nb_engine* h, int32_t p, int32_t v) {
         case NB_PARAM_MAX_MERGES_BODY: h->max_merges_body = v; return NB_OK;
         case NB_PARAM_DENSITY_MERGE: h->density_merge = v; return NB_OK;
         case NB_PARAM_TIMING: h->timing = v; return NB_OK;
+        case NB_PARAM_MAC_AUDIT_INTERVAL:
+            if (v < 0) return fail(h, NB_ERR_INVALID_ARG, "audit interval must be >= 0");
+            h->mac_audit_every = v;
+            h->mac_since_audit = 0;
+            h->mac_audits = 0;
+            h->mac_fallback = false;
+            return NB_OK;
+        case NB_PARAM_MAC_AUDIT_SAMPLES:
+            if (v < 1) return fail(h, NB_ERR_INVALID_ARG, "audit samples must be >= 1");
+            h->mac_audit_samples = v;
+            return NB_OK;
         case NB_PARAM_GROUP_BODIES:
             if (v != 32) return fail(h, NB_ERR_INVALID_ARG, "group size must be 32");
             h->group_bodies = v;
@@ -647,11 +667,13 @@ NB_API int32_t nb_get_state(nb_engine* h, int32_t* n_out, double* px, double* py
     return check_device(h);
 }
 
-NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softening, int32_t flags) {
-    if (!h) return NB_ERR_INVALID_ARG;
-    if (!h->has_state) return fail(h, NB_ERR_STATE, "nb_step before nb_set_state");
-    if (n_steps < 0) return fail(h, NB_ERR_INVALID_ARG, "negative step count");
-    cudaSetDevice(h->device);
+namespace {
+
+int force_error_stats(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
+                      double* out3);
+
+// n_steps Verlet steps with one flag set (no audits).
+int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags) {
     const bool collide = (flags & NB_FLAG_COLLISIONS) != 0;
     int r;
     if (!collide && n_steps > 1) {
@@ -704,6 +726,41 @@ NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softenin
     }
     if ((r = check_device(h))) return r;
     collect_counters(h);
+    return NB_OK;
+}
+
+}  // namespace
+
+NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softening, int32_t flags) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NB_ERR_STATE, "nb_step before nb_set_state");
+    if (n_steps < 0) return fail(h, NB_ERR_INVALID_ARG, "negative step count");
+    cudaSetDevice(h->device);
+    const bool learned = (flags & NB_FLAG_LEARNED_MAC) != 0;
+    const bool audit = learned && h->mac_audit_every > 0;
+    int r, left = n_steps;
+    while (left > 0) {
+        // after a failed audit the learned MAC falls back to the geometric test
+        const int f = (learned && h->mac_fallback) ? (flags & ~NB_FLAG_LEARNED_MAC) : flags;
+        const int k = audit ? std::min(left, h->mac_audit_every - h->mac_since_audit) : left;
+        if ((r = run_steps(h, k, dt, softening, f))) return r;
+        left -= k;
+        if (!audit) continue;
+        h->mac_since_audit += k;
+        if (h->mac_since_audit >= h->mac_audit_every) {
+            h->mac_since_audit = 0;
+            double st[3];
+            if ((r = force_error_stats(h, h->mac_audit_samples, 0x5EEDull + (uint64_t)h->mac_audits,
+                                       softening, st)))
+                return r;
+            h->mac_audits++;
+            h->mac_audit_last_rms = st[2];
+            h->mac_audit_last_max = st[1];
+            if (st[2] > h->mac_audit_rms_max) h->mac_fallback = true;
+        }
+    }
+    h->counters[NB_C_MAC_AUDITS] = h->mac_audits;
+    h->counters[NB_C_MAC_FALLBACK] = h->mac_fallback ? 1 : 0;
     return NB_OK;
 }
 
@@ -760,12 +817,24 @@ NB_API int32_t nb_diagnostics(nb_engine* h, double softening, int32_t pe_mode, d
     return NB_OK;
 }
 
-NB_API int32_t nb_force_error(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
-                              int32_t flags, double* out3) {
-    (void)flags;
-    if (!h || !out3) return NB_ERR_INVALID_ARG;
-    if (!h->has_state && h->n == 0) return fail(h, NB_ERR_STATE, "no bodies on the device");
-    cudaSetDevice(h->device);
+namespace {
+
+// ForceErrorAnalyzer statistics of the handle's current accelerations on
+// n_samples sampled active bodies against the FP64 direct sum: mean, max, rms.
+// out[3 k + axis] = acceleration of row targets[k]
+__global__ void k_gather_acc(int ns, const int32_t* __restrict__ targets,
+                             const double* __restrict__ ax, const double* __restrict__ ay,
+                             const double* __restrict__ az, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ns) return;
+    const int i = targets[k];
+    out[3 * k] = ax[i];
+    out[3 * k + 1] = ay[i];
+    out[3 * k + 2] = az[i];
+}
+
+int force_error_stats(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
+                      double* out3) {
     const int n = h->n;
     std::vector<uint8_t> act((size_t)n);
     int r;
@@ -791,12 +860,25 @@ NB_API int32_t nb_force_error(nb_engine* h, int32_t n_samples, uint64_t seed, do
     cand.resize(ns);
     if ((r = upload(h, h->targets, cand.data(), sizeof(int32_t) * (size_t)ns))) return r;
     nb::direct_targets(h->st, n, h->s, softening, ns, h->targets, h->tgt_out);
-    std::vector<double> ref((size_t)ns * 3), ax((size_t)n), ay((size_t)n), az((size_t)n);
+    std::vector<double> ref((size_t)ns * 3), ax, ay, az;
     if ((r = download(h, ref.data(), h->tgt_out, sizeof(double) * 3 * (size_t)ns))) return r;
-    if ((r = download(h, ax.data(), h->s.ax, sizeof(double) * (size_t)n)) ||
-        (r = download(h, ay.data(), h->s.ay, sizeof(double) * (size_t)n)) ||
-        (r = download(h, az.data(), h->s.az, sizeof(double) * (size_t)n)))
-        return r;
+    const bool gathered = 3 * (size_t)ns <= (size_t)h->capacity;  // fits the key scratch
+    if (gathered) {
+        // only the sampled rows' accelerations cross PCIe
+        double* g = (double*)h->keys1;
+        k_gather_acc<<<nb::ceil_div(ns, 256), 256, 0, h->st>>>(ns, h->targets, h->s.ax, h->s.ay,
+                                                               h->s.az, g);
+        ax.resize(3 * (size_t)ns);
+        if ((r = download(h, ax.data(), g, sizeof(double) * 3 * (size_t)ns))) return r;
+    } else {
+        ax.resize(n);
+        ay.resize(n);
+        az.resize(n);
+        if ((r = download(h, ax.data(), h->s.ax, sizeof(double) * (size_t)n)) ||
+            (r = download(h, ay.data(), h->s.ay, sizeof(double) * (size_t)n)) ||
+            (r = download(h, az.data(), h->s.az, sizeof(double) * (size_t)n)))
+            return r;
+    }
     if ((r = check_device(h))) return r;
     // ForceErrorAnalyzer.CompareForces statistics (ForceErrorAnalyzer.cs:100-134)
     double se = 0, se2 = 0, mx = 0;
@@ -806,7 +888,10 @@ NB_API int32_t nb_force_error(nb_engine* h, int32_t n_samples, uint64_t seed, do
         const double ex = ref[3 * k], ey = ref[3 * k + 1], ez = ref[3 * k + 2];
         const double em = sqrt(ex * ex + ey * ey + ez * ez);
         if (em < 1e-30) continue;
-        const double dx = ax[i] - ex, dy = ay[i] - ey, dz = az[i] - ez;
+        const double gx = gathered ? ax[3 * k] : ax[i];
+        const double gy = gathered ? ax[3 * k + 1] : ay[i];
+        const double gz = gathered ? ax[3 * k + 2] : az[i];
+        const double dx = gx - ex, dy = gy - ey, dz = gz - ez;
         const double e = sqrt(dx * dx + dy * dy + dz * dz) / em;
         se += e;
         se2 += e * e;
@@ -816,6 +901,27 @@ NB_API int32_t nb_force_error(nb_engine* h, int32_t n_samples, uint64_t seed, do
     out3[0] = c ? se / c : 0;
     out3[1] = mx;
     out3[2] = c ? sqrt(se2 / c) : 0;
+    return NB_OK;
+}
+
+}  // namespace
+
+NB_API int32_t nb_force_error(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
+                              int32_t flags, double* out3) {
+    (void)flags;
+    if (!h || !out3) return NB_ERR_INVALID_ARG;
+    if (!h->has_state && h->n == 0) return fail(h, NB_ERR_STATE, "no bodies on the device");
+    cudaSetDevice(h->device);
+    return force_error_stats(h, n_samples, seed, softening, out3);
+}
+
+NB_API int32_t nb_mac_audit_state(nb_engine* h, double* rms, double* max_err, int64_t* audits,
+                                  int32_t* fallback) {
+    if (!h) return NB_ERR_INVALID_ARG;
+    if (rms) *rms = h->mac_audit_last_rms;
+    if (max_err) *max_err = h->mac_audit_last_max;
+    if (audits) *audits = h->mac_audits;
+    if (fallback) *fallback = h->mac_fallback ? 1 : 0;
     return NB_OK;
 }
 
@@ -1238,6 +1344,7 @@ NB_API int32_t nb_mac_set_params(nb_engine* h, const float* params, int32_t n) {
     int r = mac_upload_params(h, params, params + nb::kMacParams);
     if (r) return r;
     h->mac_ready = true;
+    h->mac_fallback = false;
     return NB_OK;
 }
 
@@ -1318,6 +1425,7 @@ NB_API int32_t nb_mac_train(nb_engine* h, int32_t epochs, int32_t batch, double 
     cudaStreamSynchronize(h->st);
     cudaFree(order);
     if (r == NB_OK) r = mac_fit_screen(h);
+    h->mac_fallback = false;
     return r;
 }
 

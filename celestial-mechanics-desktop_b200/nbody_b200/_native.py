@@ -50,11 +50,14 @@ PARAM_MAC_THETA_LO = 11
 PARAM_MAC_THETA_HI = 12
 PARAM_MAC_SCREEN_QUANTILE = 13
 PARAM_ENS_DIRECT_SHAPE = 14
+PARAM_MAC_AUDIT_INTERVAL = 15
+PARAM_MAC_AUDIT_SAMPLES = 16
+PARAM_MAC_AUDIT_RMS = 17
 ENS_SHAPES = [(64, 1), (64, 2), (64, 4), (128, 1), (128, 2), (128, 4), (256, 1), (256, 2), (256, 4)]
 # timings / counters
 T_BUILD, T_TRAVERSAL, T_TOTAL, T_SORT, T_TREE, T_COUNT = range(6)
 (C_CELL_INTERACTIONS, C_BODY_INTERACTIONS, C_NODES, C_ACTIVE, C_PAIRS, C_MERGES, C_OVERFLOWS, C_GROUPS,
- C_MAX_GROUP_WORK, C_MAC_EVALS, C_COUNT) = range(11)
+ C_MAX_GROUP_WORK, C_MAC_EVALS, C_MAC_AUDITS, C_MAC_FALLBACK, C_COUNT) = range(13)
 
 vp = C.c_void_p
 i32 = C.c_int32
@@ -94,6 +97,7 @@ _SIGS = {
     "nb_mac_gradient": (i32, [vp, P, P, i32, P, P]),
     "nb_mac_predict": (i32, [vp, P, i32, P]),
     "nb_mac_fit_screen": (i32, [vp]),
+    "nb_mac_audit_state": (i32, [vp, P, P, P, P]),
     "nb_mac_get_screen": (i32, [vp, P, i32]),
     "nb_mac_set_screen": (i32, [vp, P, i32]),
     "nb_ens_create": (i32, [i32, P, i32, i32, C.POINTER(vp)]),

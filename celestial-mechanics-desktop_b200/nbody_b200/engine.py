@@ -259,6 +259,14 @@ class Engine:
         self._check(N.lib.nb_mac_predict(self._h, N.ptr(X), len(X), N.ptr(y)))
         return y
 
+    def mac_audit_state(self) -> dict:
+        rms, mx = np.zeros(1), np.zeros(1)
+        audits, fb = np.zeros(1, np.int64), np.zeros(1, np.int32)
+        self._check(N.lib.nb_mac_audit_state(self._h, N.ptr(rms), N.ptr(mx), N.ptr(audits),
+                                             N.ptr(fb)))
+        return {"rms": float(rms[0]), "max": float(mx[0]), "audits": int(audits[0]),
+                "fallback": bool(fb[0])}
+
     def mac_fit_screen(self):
         self._check(N.lib.nb_mac_fit_screen(self._h))
 

@@ -87,9 +87,17 @@ enum nb_param {
     NB_PARAM_MAC_SCREEN_QUANTILE = 13, /* f64, learned MAC: quantile of |network - screen| over
                                       the training set that sets the linear screen's margin;
                                       0 = no screen (default 0.9, used by the next fit)       */
-    NB_PARAM_ENS_DIRECT_SHAPE = 14 /* i32, ensembles: direct-sum tile shape 0..8 (threads x
+    NB_PARAM_ENS_DIRECT_SHAPE = 14, /* i32, ensembles: direct-sum tile shape 0..8 (threads x
                                       targets/thread: 64x1 64x2 64x4 128x1 128x2 128x4 256x1
                                       256x2 256x4; default 4), normally set by nb_ens_autotune */
+    NB_PARAM_MAC_AUDIT_INTERVAL = 15, /* i32, learned MAC in nb_step: every this many steps the
+                                      accelerations are audited against the FP64 direct sum on
+                                      sampled bodies; 0 = never (default).  Setting it also
+                                      clears a fallback                                        */
+    NB_PARAM_MAC_AUDIT_SAMPLES = 16, /* i32, bodies per audit (default 1024)                   */
+    NB_PARAM_MAC_AUDIT_RMS = 17    /* f64, an audit whose rms relative error exceeds this
+                                      switches the handle to the geometric MAC at
+                                      NB_PARAM_THETA (default 1e-3)                           */
 };
 
 /* Indices into nb_get_timings() output (milliseconds, CUDA events).
@@ -116,7 +124,9 @@ enum nb_counter {
     NB_C_GROUPS = 7,                /* walk groups (warps' body sets), last evaluation       */
     NB_C_MAX_GROUP_WORK = 8,        /* longest interaction list of one group (load balance)  */
     NB_C_MAC_EVALS = 9,             /* learned MAC: (group, cell) rows the network evaluated */
-    NB_C_COUNT = 10
+    NB_C_MAC_AUDITS = 10,           /* learned MAC: audits run since the interval was set    */
+    NB_C_MAC_FALLBACK = 11,         /* learned MAC: 1 once an audit switched to geometric    */
+    NB_C_COUNT = 12
 };
 
 /* ---- lifetime -------------------------------------------------------- */
@@ -287,6 +297,12 @@ NB_API int32_t nb_mac_gradient(nb_engine* h, const float* X, const float* Y, int
                                float* grad, double* loss);
 /* Predictions (log2 error units) of the walk's inference routine. */
 NB_API int32_t nb_mac_predict(nb_engine* h, const float* X, int32_t n, float* y);
+
+/* The last audit of the learned MAC inside nb_step (NB_PARAM_MAC_AUDIT_*):
+ * its rms and max relative force error against the FP64 direct sum, the
+ * audits run and whether the handle has fallen back to the geometric MAC. */
+NB_API int32_t nb_mac_audit_state(nb_engine* h, double* rms, double* max_err, int64_t* audits,
+                                  int32_t* fallback);
 
 /* Linear screen in front of the network: in the band the walk first forms
  * s = w . x_norm + b (x_norm: features normalised as the network's input,
