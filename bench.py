@@ -546,6 +546,22 @@ def run_theta05(args, ws, rank, local):
                                          if n == N_BODIES and not direct else None)},
                 "gpu_launches": (15 if direct else launches_per_step()) * args.steps,
                 "clocks": arm["clocks"]}
+        if direct and ws == 1 and not args.no_cpu_baseline:
+            # the CpuParallelBackend restatement (FP64, OpenMP over targets) on
+            # a sample of 2048 targets against all n sources, scaled to n
+            import oracle
+
+            threads = os.cpu_count() or 1
+            tsel = np.arange(0, n, max(1, n // 2048))[:2048].astype(np.int32)
+            t = time.perf_counter()
+            oracle.direct_forces_targets(b.px, b.py, b.pz, b.mass, b.active, EPS, tsel,
+                                         nthreads=threads)
+            cs = (time.perf_counter() - t) * n / len(tsel)
+            line["cpu_baseline"] = {"value": 1.0 / cs, "unit": "steps/s", "cores": threads,
+                                    "kind": "port", "pairs_per_s": float(n) * n / cs,
+                                    "sample": f"{len(tsel)} targets x {n} sources with the "
+                                              "CpuParallelBackend restatement, scaled to all "
+                                              "n targets"}
     eng.close()
     return line
 
@@ -890,6 +906,27 @@ def run_disk(args, ws, rank, local):
                 "energy_drift": (p1["e"] - p0["e"]) / abs(p0["e"]),
                 "momentum_drift_abs": dp, "momentum_scale": pn,
                 "mass_drift": (p1["m"] - p0["m"]) / p0["m"], "clocks": clk}
+        if ws == 1 and not args.no_cpu_baseline:
+            # the reference's own Barnes-Hut force evaluation of the initial
+            # disk on all host threads (theta 0.5, monopole); the collision
+            # stage is not counted, so this bounds the CPU step rate from above
+            import oracle
+
+            threads = os.cpu_count() or 1
+            if oracle.ref() is not None:
+                t = time.perf_counter()
+                oracle.ref_bh_forces(d.px, d.py, d.pz, d.mass, d.active, eps, THETA, True, threads)
+                kind = "reference"
+            else:
+                t = time.perf_counter()
+                oracle.bh_forces(d.px, d.py, d.pz, d.mass, d.active, eps, THETA, nthreads=threads)
+                kind = "port"
+            cs = time.perf_counter() - t
+            line["cpu_baseline"] = {"value": 1.0 / cs, "unit": "steps/s", "cores": threads,
+                                    "kind": kind,
+                                    "sample": "one Barnes-Hut force evaluation of the initial "
+                                              "disk (reference BarnesHutSolver, theta 0.5, "
+                                              "monopole), collision stage not counted"}
     eng.close()
     return line
 
