@@ -397,6 +397,38 @@ def run_b200(args, ws, rank, local):
     arm_05 = timed_arm(eng, b, stream, args, ws, dev, geo, N, geo, "theta_0_5")
     eng.set_param(N.PARAM_THETA, theta_g)
 
+    # ---- a long run: learned MAC audited every 100 steps; energy drift of
+    # the learned and the geometric (same-error theta) integrations --------
+    long_run = None
+    if not big and args.long_steps > 0:
+        def drift(flags_run, audit_every):
+            eng.set_state(b, old_acc=False)
+            eng.step(1, 0.0, EPS, geo)
+            e0 = eng.diagnostics(EPS, pe_mode=1)["e"]
+            audits = []
+            if audit_every:
+                eng.set_param(N.PARAM_MAC_AUDIT_SAMPLES, 1024)
+                eng.set_param(N.PARAM_MAC_AUDIT_INTERVAL, audit_every)
+                for _ in range(args.long_steps // audit_every):
+                    eng.step(audit_every, DT, EPS, flags_run)
+                    a = eng.mac_audit_state()
+                    audits.append(round(a["rms"], 7))
+                fb = eng.mac_audit_state()["fallback"]
+                eng.set_param(N.PARAM_MAC_AUDIT_INTERVAL, 0)
+            else:
+                eng.step(args.long_steps, DT, EPS, flags_run)
+                fb = None
+            e1 = eng.diagnostics(EPS, pe_mode=1)["e"]
+            return (e1 - e0) / abs(e0), audits, fb
+
+        d_l, audits_l, fb_l = drift(learned, 100)
+        d_g, _, _ = drift(geo, 0)
+        long_run = {"steps": args.long_steps, "dt": DT,
+                    "learned_audit_rms_every_100_steps": audits_l, "learned_fallback": fb_l,
+                    "energy_drift_learned": d_l, "energy_drift_geometric_same_error": d_g,
+                    "energy": "kinetic + tree potential (theta 0.5), FP64 reductions"}
+        log(f"long run: audits {audits_l}, drift learned {d_l:.3e} geometric {d_g:.3e}")
+
     # ---- end to end through the seam with host buffers (learned MAC) ----
     st, _ = eng.get_state()
     nn = st.n
@@ -465,6 +497,7 @@ def run_b200(args, ws, rank, local):
                                                            "force_error", "stage_ms")}
                                     | {"theta": theta_g, "calibration_rms": rms_g, "scan": scan_g},
             "learned_over_geometric_steps": arm_l["steps_per_s"] / arm_g["steps_per_s"],
+            "long_run": long_run,
             "geometric_theta_0_5": {k: arm_05[k] for k in ("steps_per_s", "ms_per_step",
                                                            "interactions_per_s",
                                                            "force_error", "stage_ms")},
@@ -939,6 +972,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--long-steps", type=int, default=1000,
+                    help="bh1m: steps of the audited long run after the timed arms (0 = skip)")
     ap.add_argument("--n", type=int, default=N_BODIES,
                     help="bodies (default the 1,048,576-body workload; smaller for profiling)")
     ap.add_argument("--workload", default="bh1m",
