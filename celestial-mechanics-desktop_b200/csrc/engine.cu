@@ -88,6 +88,10 @@ struct nb_engine {
     float *mac_X = nullptr, *mac_Y = nullptr;
     int mac_n = 0, mac_cap = 0;
     nb::MacRecord* mac_rec = nullptr;
+    nb::MacRecord* mac_rec2 = nullptr;    // records in a fixed order
+    uint64_t *mac_rk0 = nullptr, *mac_rk1 = nullptr;
+    uint32_t *mac_rv0 = nullptr, *mac_rv1 = nullptr;
+    void* mac_rws = nullptr;
     int mac_rec_cap = 0;
     int* mac_counts = nullptr;            // [0] records, [1] accepted samples
     // device-resident state
@@ -1134,7 +1138,12 @@ NB_API int32_t nb_mac_harvest(nb_engine* h, int32_t max_records, double sample_f
             return r;
     }
     if (h->mac_rec_cap < max_records) {
-        if ((r = dalloc(h, &h->mac_rec, (size_t)max_records))) return r;
+        const size_t m = (size_t)max_records;
+        if ((r = dalloc(h, &h->mac_rec, m)) || (r = dalloc(h, &h->mac_rec2, m)) ||
+            (r = dalloc(h, &h->mac_rk0, m)) || (r = dalloc(h, &h->mac_rk1, m)) ||
+            (r = dalloc(h, &h->mac_rv0, m)) || (r = dalloc(h, &h->mac_rv1, m)) ||
+            (r = dalloc(h, (char**)&h->mac_rws, nb::sort_workspace_bytes(max_records))))
+            return r;
         h->mac_rec_cap = max_records;
     }
     const int n = h->n, na = h->n_active;
@@ -1177,10 +1186,15 @@ NB_API int32_t nb_mac_harvest(nb_engine* h, int32_t max_records, double sample_f
     if ((r = download(h, &nrec, &h->mac_counts[0], sizeof(int)))) return r;
     if ((r = check_device(h))) return r;
     nrec = std::min(nrec, max_records);
-    nb::mac_targets(h->st, nrec, h->mac_rec, h->sbody, h->tree, softening, h->mac_X, h->mac_Y,
-                    &h->mac_counts[1], h->mac_n, h->mac_cap);
+    // a fixed record order (the walk appends them in warp order): the
+    // training set, and so the trained network, do not depend on scheduling
+    nb::mac_sort_records(h->st, nrec, h->mac_rec, h->mac_rec2, h->mac_rk0, h->mac_rv0,
+                         h->mac_rk1, h->mac_rv1, h->mac_rws, &h->mac_counts[1], sc->err, h->sms);
     int got = 0;
     if ((r = download(h, &got, &h->mac_counts[1], sizeof(int)))) return r;
+    if ((r = check_device(h))) return r;
+    nb::mac_targets(h->st, got, h->mac_rec2, h->sbody, h->tree, softening, h->mac_X, h->mac_Y,
+                    &h->mac_counts[2], h->mac_n, h->mac_cap);
     if ((r = check_device(h))) return r;
     got = std::min(got, h->mac_cap - h->mac_n);
     h->mac_n += got;

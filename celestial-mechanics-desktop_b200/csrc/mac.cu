@@ -14,6 +14,7 @@
 //   BF16 fragment image (MacDev) the walk and the training kernel read.
 #include "mac.cuh"
 #include "mac_train.cuh"
+#include "sort.cuh"
 #include "tree.cuh"
 
 namespace nb {
@@ -61,11 +62,43 @@ __global__ void k_mac_targets(int nrec, const MacRecord* __restrict__ rec,
     const double f = -cm.w * inv3 - 2.5 * rqr * inv5 * inv2;
     const double ax = f * dx + qx * inv5, ay = f * dy + qy * inv5, az = f * dz + qz * inv5;
     const double err = sqrt((ax - ex) * (ax - ex) + (ay - ey) * (ay - ey) + (az - ez) * (az - ez));
-    if (!(R.a_min > 0.f)) return;  // no acceleration estimate: not a usable sample
-    const int slot = atomicAdd(n_out, 1);
+    (void)n_out;
+    const int slot = r;  // records come sorted, usable ones first (mac_sort_records)
     if (out_off + slot >= out_cap) return;
     for (int k = 0; k < kMacIn; k++) X[(size_t)(out_off + slot) * kMacIn + k] = R.f[k];
     Y[out_off + slot] = (float)log2(err / (double)R.a_min + 1e-30);
+}
+
+// Harvest records in a fixed order: key = (no |a| estimate) << 63 | body << 32
+// | node, so the training set does not depend on the order in which warps
+// appended records; usable records (a_min > 0) are counted into *n_valid.
+__global__ void k_mac_rec_keys(int nrec, const MacRecord* __restrict__ rec,
+                               uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                               int* __restrict__ n_valid) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrec) return;
+    const MacRecord R = rec[i];
+    const bool ok = R.a_min > 0.f;
+    keys[i] = ((uint64_t)(ok ? 0 : 1) << 63) | ((uint64_t)(uint32_t)R.body << 32) |
+              (uint64_t)(uint32_t)R.node;
+    vals[i] = (uint32_t)i;
+    if (ok) atomicAdd(n_valid, 1);
+}
+
+__global__ void k_mac_rec_gather(int nrec, const MacRecord* __restrict__ rec,
+                                 const uint32_t* __restrict__ order, MacRecord* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nrec) out[i] = rec[order[i]];
+}
+
+void mac_sort_records(cudaStream_t st, int nrec, const MacRecord* rec, MacRecord* sorted,
+                      uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, void* ws,
+                      int* n_valid, int* err, int sms) {
+    cudaMemsetAsync(n_valid, 0, sizeof(int), st);
+    if (nrec <= 0) return;
+    k_mac_rec_keys<<<ceil_div(nrec, 256), 256, 0, st>>>(nrec, rec, k0, v0, n_valid);
+    sort_pairs(st, nrec, k0, v0, k1, v1, ws, false, err, sms);
+    k_mac_rec_gather<<<ceil_div(nrec, 256), 256, 0, st>>>(nrec, rec, v0, sorted);
 }
 
 void mac_targets(cudaStream_t st, int nrec, const MacRecord* rec, const double4* sbody,

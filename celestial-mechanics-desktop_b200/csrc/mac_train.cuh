@@ -14,6 +14,13 @@ struct MacTrainImage {
 // Normalisation block: 8 feature means, 8 feature stds, target mean, target std.
 constexpr int kMacNorm = 2 * kMacIn + 2;
 
+// Sort harvest records by (usable, body, node) into `sorted`; *n_valid = the
+// usable ones, which come first.  Buffers of nrec entries; ws for nrec keys.
+void mac_sort_records(cudaStream_t st, int nrec, const MacRecord* rec, MacRecord* sorted,
+                      uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1, void* ws,
+                      int* n_valid, int* err, int sms);
+// Targets of the first nrec (usable, sorted) records, written to rows
+// out_off + r.
 void mac_targets(cudaStream_t st, int nrec, const MacRecord* rec, const double4* sbody,
                  const TreeBufs& t, double eps, float* X, float* Y, int* n_out, int out_off,
                  int out_cap);

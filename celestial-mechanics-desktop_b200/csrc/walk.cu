@@ -33,16 +33,23 @@ constexpr int kWarpFloats = kCellCap * 10 + kPartCap * 4 + kPartCap * 2 + kPartC
 constexpr int kWalkSmem = kWalkWarps * kWarpFloats * 4;
 constexpr int kMaxWalkRounds = 1 << 22;
 constexpr int kMacGeometric = 0, kMacHarvest = 1, kMacLearned = 2;
-// blocks per SM the learned walk is compiled for (2: 128 registers, no
-// spills; 3: 80 registers)
+// Block shape of the learned walk: warps per block and blocks per SM it is
+// compiled for (its registers, not shared memory, bound the occupancy).
+// 5 x 4 = 20 warps per SM at 96 registers (a few spilled) measured 1.7 %
+// faster than 8 x 2 = 16 warps at 128 registers; 6 x 3 and 8 x 3 slower.
 #ifndef NB_WALK_MAC_BLOCKS
-#define NB_WALK_MAC_BLOCKS 2
+#define NB_WALK_MAC_BLOCKS 4
 #endif
+#ifndef NB_WALK_MAC_WARPS
+#define NB_WALK_MAC_WARPS 5
+#endif
+constexpr int kMacWarps = NB_WALK_MAC_WARPS;
 // learned variant: + per warp 32 staged rows (4 words), 32 outputs and 32
-// pending node ids; three blocks still fit the SM's 228 KB
+// pending node ids
 constexpr int kMacWarpWords = 32 * 4 + 32 + 32;
-constexpr int kWalkSmemMac = kWalkSmem + kWalkWarps * kMacWarpWords * 4;
-static_assert(3 * (kWalkSmemMac + 1024) <= 228 * 1024, "three walk blocks per SM");
+constexpr int kWalkSmemMac = kMacWarps * (kWarpFloats + kMacWarpWords) * 4;
+static_assert(NB_WALK_MAC_BLOCKS * (kWalkSmemMac + 1024) <= 228 * 1024, "learned walk blocks per SM");
+static_assert(kMacWarps <= kWalkWarps, "the stacks are sized for the geometric block shape");
 
 __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     float y = x - c;
@@ -60,8 +67,10 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
 // (geometric below theta, open at or above theta_hi, the network decides in
 // between).
 template <bool QUAD, bool SHELL, bool POT, bool GUARD, int MAC>
-__global__ void __launch_bounds__(kWalkThreads, MAC == kMacLearned ? NB_WALK_MAC_BLOCKS : 3)
+__global__ void __launch_bounds__((MAC == kMacLearned ? kMacWarps : kWalkWarps) * 32,
+                                  MAC == kMacLearned ? NB_WALK_MAC_BLOCKS : 3)
 k_walk_group(WalkArgs a) {
+    constexpr int WARPS = MAC == kMacLearned ? kMacWarps : kWalkWarps;
     extern __shared__ __align__(16) float s_walk[];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -75,7 +84,7 @@ k_walk_group(WalkArgs a) {
     float* pbuf = base + kCellCap * 10;
     float2* p1 = (float2*)(pbuf + kPartCap * 4);     // R^2, m / (R^2 + eps^2)^1.5
     int* p2 = (int*)(p1 + kPartCap);                 // sorted index
-    int* fa = a.front + (size_t)(blockIdx.x * kWalkWarps + warp) * a.front_cap;
+    int* fa = a.front + (size_t)(blockIdx.x * WARPS + warp) * a.front_cap;
     const float eps2 = (float)a.eps2;
     const float theta2 = (float)a.theta2;
     const int ngroups = *a.n_groups;
@@ -87,7 +96,7 @@ k_walk_group(WalkArgs a) {
     float* ys = nullptr;
     int* pend = nullptr;
     if (MAC == kMacLearned) {
-        xs = (uint32_t*)(s_walk + kWalkWarps * kWarpFloats) + warp * kMacWarpWords;
+        xs = (uint32_t*)(s_walk + WARPS * kWarpFloats) + warp * kMacWarpWords;
         ys = (float*)(xs + 32 * 4);
         pend = (int*)(ys + 32);
     }
@@ -819,10 +828,14 @@ void walk_init(int sms, WalkConfig& cfg) {
     cfg.blocks = sms * per_sm;
     int per_sm_mac = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm_mac, k_walk_group<true, false, false, false, kMacLearned>, kWalkThreads,
+        &per_sm_mac, k_walk_group<true, false, false, false, kMacLearned>, kMacWarps * 32,
         kWalkSmemMac);
     if (per_sm_mac < 1) per_sm_mac = 1;
-    cfg.blocks_mac = sms * (per_sm_mac < per_sm ? per_sm_mac : per_sm);
+    // as many resident blocks as fit, within the stacks sized for the
+    // geometric grid (cfg.blocks x kWalkWarps warps)
+    cfg.blocks_mac = sms * per_sm_mac;
+    if (cfg.blocks_mac * kMacWarps > cfg.blocks * kWalkWarps)
+        cfg.blocks_mac = cfg.blocks * kWalkWarps / kMacWarps;
     cfg.front_cap = 16384;
 }
 
@@ -843,7 +856,7 @@ void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, b
     }
     if (mac == kMacLearned) {
         k_walk_group<true, false, false, false, kMacLearned>
-            <<<cfg.blocks_mac, kWalkThreads, kWalkSmemMac, st>>>(a);
+            <<<cfg.blocks_mac, kMacWarps * 32, kWalkSmemMac, st>>>(a);
         return;
     }
     const WalkKernel k = pick_walk(quad, shell, pot, !(a.eps2 > 0.0));
