@@ -346,7 +346,7 @@ k_walk_group(WalkArgs a) {
         // One candidate node per lane, decided: accepted cells -> cell list,
         // children of opened nodes -> stack, bodies of leaves -> particle list.
         auto emit = [&](int node, bool take_cell, bool is_leaf, bool open, int4 lk, float rx,
-                        float ry, float rz, float mass) {
+                        float ry, float rz, float mass, float4 nq0, float nqyz) {
             // 1. accepted cells -> cell list
             const unsigned mcell = __ballot_sync(FULL, take_cell);
             if (mcell) {
@@ -360,13 +360,14 @@ k_walk_group(WalkArgs a) {
                     e[4] = rz;
                     e[6] = -mass;
                     if (QUAD) {
-                        const float4 q = a.t.q0[node];  // Qxx, Qyy, Qxy, Qxz
+                        // Qxx, Qyy, Qxy, Qxz: preloaded by the geometric test
+                        const float4 q = MAC == kMacGeometric ? nq0 : a.t.q0[node];
                         e[8] = q.x;
                         e[10] = q.y;
                         e[12] = -(q.x + q.y);
                         e[14] = q.z;
                         e[16] = q.w;
-                        e[18] = a.t.q1[node].x;
+                        e[18] = MAC == kMacGeometric ? nqyz : a.t.q1[node].x;
                     }
                 }
                 nc += k;
@@ -450,7 +451,7 @@ k_walk_group(WalkArgs a) {
             }
             npend = 0;
             __syncwarp();
-            emit(pn, tc, lf, op, plk, prx, pry, prz, pm);
+            emit(pn, tc, lf, op, plk, prx, pry, prz, pm, make_float4(0.f, 0.f, 0.f, 0.f), 0.f);
         };
         int rounds = 0;
         while (sp > 0 || (MAC == kMacLearned && npend > 0)) {
@@ -470,13 +471,25 @@ k_walk_group(WalkArgs a) {
                 bool take_cell = false, is_leaf = false, open = false, in_band = false;
                 int4 lk = make_int4(0, 0, 0, 0);
                 float rx = 0.f, ry = 0.f, rz = 0.f, mass = 0.f, half = 0.f, d2 = 0.f;
+                float4 nq0 = make_float4(0.f, 0.f, 0.f, 0.f);
+                float nqyz = 0.f;
                 bool live = false;
                 if (node >= 0) {
+                    // geometric test: every word of the node the test and the
+                    // cell list need, loaded together (one memory latency per
+                    // round); the learned variant, short of registers, loads
+                    // the quadrupole only for accepted cells
                     lk = a.t.link[node];
                     const double4 cm = a.t.com[node];
+                    float4 nq1 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (MAC == kMacGeometric) {
+                        nq1 = a.t.q1[node];
+                        if (QUAD) nq0 = a.t.q0[node];
+                        nqyz = nq1.x;
+                    }
                     if (cm.w > 0.0) {
                         live = true;
-                        half = a.t.q1[node].y;
+                        half = MAC == kMacGeometric ? nq1.y : a.t.q1[node].y;
                         rx = (float)(cm.x - gcx);
                         ry = (float)(cm.y - gcy);
                         rz = (float)(cm.z - gcz);
@@ -568,7 +581,7 @@ k_walk_group(WalkArgs a) {
                     if (lk.y == 0) is_leaf = true;
                     else open = true;
                 }
-                emit(node, take_cell, is_leaf, open, lk, rx, ry, rz, mass);
+                emit(node, take_cell, is_leaf, open, lk, rx, ry, rz, mass, nq0, nqyz);
             }
         }
         if (nc) flush_cells();
