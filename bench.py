@@ -243,6 +243,11 @@ RMS_TARGET = 1e-3
 # both arms are calibrated on the initial state to 2 % below the target, so
 # that the force error after the timed steps (the state moves) stays within it
 CALIBRATION_TARGET = 0.98 * RMS_TARGET
+# the in-run audit samples 1024 bodies, whose rms scatters by about 10 %
+# around the 4096-sample figure the target is judged on; its fallback bound
+# sits 20 % above the target so that only a real failure of the criterion
+# (errors several times the target) switches to the geometric MAC
+AUDIT_SAMPLES, AUDIT_RMS_BOUND = 1024, 1.2 * RMS_TARGET
 THETA_GRID = [round(0.5 + 0.0125 * i, 4) for i in range(33)]         # 0.5 .. 0.9
 BUDGET_GRID = [round(-4.5 + 0.05 * i, 2) for i in range(41)]          # log10 budget -4.5 .. -2.5
 ERR_SAMPLES, ERR_SEED = 4096, 12345
@@ -286,10 +291,11 @@ def force_rms(eng, b, flags, mode_geo):
     return eng.force_error(ERR_SAMPLES, ERR_SEED, EPS)[2]
 
 
-def calibrate(eng, b, N, param, grid, flags, mode_geo, log):
+def calibrate(eng, b, N, param, grid, flags, mode_geo, log, refine=4):
     """Largest grid value whose rms error is <= CALIBRATION_TARGET (grid
-    ascending in error); returns (value, rms, scanned)."""
-    best, best_rms, scanned = None, None, []
+    ascending in error), then `refine` evenly spaced values between it and
+    the first grid value above the target; returns (value, rms, scanned)."""
+    best, best_rms, scanned, over = None, None, [], None
     for v in grid:
         eng.set_param(param, v)
         rms = force_rms(eng, b, flags, mode_geo)
@@ -297,38 +303,37 @@ def calibrate(eng, b, N, param, grid, flags, mode_geo, log):
         if rms <= CALIBRATION_TARGET:
             best, best_rms = v, rms
         elif best is not None:
+            over = v
             break
+    if best is not None and over is not None:
+        lo = best
+        for k in range(1, refine + 1):
+            v = lo + (over - lo) * k / (refine + 1)
+            eng.set_param(param, v)
+            rms = force_rms(eng, b, flags, mode_geo)
+            scanned.append([v, rms])
+            if rms > CALIBRATION_TARGET:
+                break
+            best, best_rms = v, rms
     log(f"calibrated param {param}: {best} (rms {best_rms})")
     eng.set_param(param, best if best is not None else grid[0])
     return best, best_rms, scanned
 
 
 def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
-    """Warm-up then K device-resident steps bracketed by barrier +
+    """Warm-up then K device-resident steps in one nb_step call (the step is
+    captured once and replayed as a CUDA graph), bracketed by barrier +
     synchronize and CUDA events on the engine's stream; the timed steps sit
-    in an NVTX range named `label` (ncu --nvtx-include "<label>/")."""
+    in an NVTX range named `label` (ncu --nvtx-include "<label>/").  The
+    per-step interaction counts and stage times come from an untimed replay
+    of the same trajectory, one instrumented step per call (the walk is
+    deterministic, so both passes evaluate identical steps)."""
     import torch
 
-    clocks = Clocks(dev)
-    clocks.start()
+    acc = dict(walk=0.0, build=0.0, sort=0.0, tree=0.0, inter=0, flops=0.0, evals=0)
     eng.set_state(b, old_acc=False)
     eng.step(1, 0.0, EPS, mode_geo)
     eng.step(max(args.warmup, 3), DT, EPS, flags)
-    torch.cuda.synchronize(dev)
-    barrier(ws)
-    torch.cuda.synchronize(dev)
-    w0 = time.time()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    audit = bool(flags & N.FLAG_LEARNED_MAC)
-    if audit:
-        # the sampled FP64 direct sum judges the learned MAC once per timed
-        # block (inside it); a failed audit would switch to the geometric MAC
-        eng.set_param(N.PARAM_MAC_AUDIT_SAMPLES, 1024)
-        eng.set_param(N.PARAM_MAC_AUDIT_INTERVAL, args.steps)
-    torch.cuda.nvtx.range_push(label)
-    t0.record(stream)
-    acc = dict(walk=0.0, build=0.0, sort=0.0, tree=0.0, inter=0, flops=0.0, evals=0)
     for _ in range(args.steps):
         eng.step(1, DT, EPS, flags)
         tm = eng.timings()
@@ -340,6 +345,28 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
         acc["inter"] += int(c[N.C_CELL_INTERACTIONS] + c[N.C_BODY_INTERACTIONS])
         acc["flops"] += FLOPS_CELL_QUAD * c[N.C_CELL_INTERACTIONS] + FLOPS_BODY * c[N.C_BODY_INTERACTIONS]
         acc["evals"] += int(c[N.C_MAC_EVALS])
+
+    clocks = Clocks(dev)
+    clocks.start()
+    eng.set_state(b, old_acc=False)
+    eng.step(1, 0.0, EPS, mode_geo)
+    eng.step(max(args.warmup, 3), DT, EPS, flags)
+    audit = bool(flags & N.FLAG_LEARNED_MAC)
+    if audit:
+        # the sampled FP64 direct sum judges the learned MAC once per timed
+        # block (inside it); a failed audit would switch to the geometric MAC
+        eng.set_param(N.PARAM_MAC_AUDIT_SAMPLES, AUDIT_SAMPLES)
+        eng.set_param(N.PARAM_MAC_AUDIT_RMS, AUDIT_RMS_BOUND)
+        eng.set_param(N.PARAM_MAC_AUDIT_INTERVAL, args.steps)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    w0 = time.time()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push(label)
+    t0.record(stream)
+    eng.step(args.steps, DT, EPS, flags)
     t1.record(stream)
     torch.cuda.synchronize(dev)
     torch.cuda.nvtx.range_pop()
@@ -351,7 +378,8 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
     if audit:
         audit_state = eng.mac_audit_state()
         audit_state["interval_steps"] = args.steps
-        audit_state["samples"] = 1024
+        audit_state["samples"] = AUDIT_SAMPLES
+        audit_state["rms_bound"] = AUDIT_RMS_BOUND
         eng.set_param(N.PARAM_MAC_AUDIT_INTERVAL, 0)
     err = eng.force_error(ERR_SAMPLES, ERR_SEED, EPS)
     k = args.steps
@@ -407,7 +435,8 @@ def run_b200(args, ws, rank, local):
             e0 = eng.diagnostics(EPS, pe_mode=1)["e"]
             audits = []
             if audit_every:
-                eng.set_param(N.PARAM_MAC_AUDIT_SAMPLES, 1024)
+                eng.set_param(N.PARAM_MAC_AUDIT_SAMPLES, AUDIT_SAMPLES)
+                eng.set_param(N.PARAM_MAC_AUDIT_RMS, AUDIT_RMS_BOUND)
                 eng.set_param(N.PARAM_MAC_AUDIT_INTERVAL, audit_every)
                 for _ in range(args.long_steps // audit_every):
                     eng.step(audit_every, DT, EPS, flags_run)

@@ -8,6 +8,8 @@
 // NewtonianGravity.ComputePotentialEnergy (Forces/NewtonianGravity.cs:68-77).
 #include "diag.cuh"
 
+#include <algorithm>
+
 namespace nb {
 
 constexpr int kDiagThreads = 256;
@@ -111,43 +113,138 @@ size_t diag_partial_bytes(int capacity) {
 }
 
 // FP64 direct sum for target rows (ForceErrorAnalyzer's exact reference,
-// CpuSingleThreadBackend arithmetic per pair): one block per target, sources
-// split over the block's threads, fixed-order block reduction.
-__global__ void k_direct_targets(int n, State s, double eps2, const int32_t* __restrict__ targets,
-                                 double* __restrict__ out3) {
-    __shared__ double sh[3][8];
-    const int i = targets[blockIdx.x];
-    const double xi = s.px[i], yi = s.py[i], zi = s.pz[i];
-    double ax = 0, ay = 0, az = 0;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        if (j == i || !s.active[j]) continue;
-        const double dx = xi - s.px[j], dy = yi - s.py[j], dz = zi - s.pz[j];
-        const double inv = 1.0 / sqrt(dx * dx + dy * dy + dz * dz + eps2);
-        const double c = s.mass[j] * inv * inv * inv;
-        ax -= c * dx;
-        ay -= c * dy;
-        az -= c * dz;
+// CpuSingleThreadBackend arithmetic per pair).  Block (tile, chunk) sums
+// kTgtTile targets over one chunk of the sources: each source is loaded once
+// per tile rather than once per target, and the chunks give enough blocks
+// for a few hundred targets.  The block's threads split the chunk, the
+// block reduces in a fixed shuffle-tree order, and the chunk partials are
+// summed in chunk order, so the result is deterministic.
+constexpr int kTgtTile = 8;
+
+// 1/sqrt(x) in FP64 from the FP32 hardware estimate (relative error below
+// 2^-22) and one third-order Householder step, y <- y (1 + e/2 + 3e^2/8)
+// with e = 1 - x y^2, which cubes the relative error (below 2^-64, so the
+// result is within FP64 rounding).  x outside [1e-36, 1e36] (beyond the
+// FP32 normal range after conversion) takes the library routine.
+__device__ __forceinline__ double rsqrt_f64(double x) {
+    if (!(x >= 1e-36 && x <= 1e36)) return rsqrt(x);
+    const double y = (double)rsqrt_ftz((float)x);
+    const double e = fma(-x, y * y, 1.0);
+    return fma(y * e, fma(e, 0.375, 0.5), y);
+}
+constexpr int kTgtThreads = 256;
+constexpr int kTgtUnroll = 4;
+constexpr int kTgtMinChunk = 16384;
+
+__global__ void __launch_bounds__(kTgtThreads)
+k_direct_targets(int n, State s, double eps2, const int32_t* __restrict__ targets, int nt,
+                 int chunk, double* __restrict__ out) {
+    __shared__ double sh[3 * kTgtTile][kTgtThreads / 32];
+    const int t0 = blockIdx.x * kTgtTile;
+    int id[kTgtTile];
+    double xi[kTgtTile], yi[kTgtTile], zi[kTgtTile], ax[kTgtTile], ay[kTgtTile], az[kTgtTile];
+#pragma unroll
+    for (int k = 0; k < kTgtTile; k++) {
+        id[k] = t0 + k < nt ? targets[t0 + k] : -1;
+        const int i = id[k] < 0 ? 0 : id[k];
+        xi[k] = s.px[i];
+        yi[k] = s.py[i];
+        zi[k] = s.pz[i];
+        ax[k] = ay[k] = az[k] = 0.0;
     }
-    ax = warp_sum(ax);
-    ay = warp_sum(ay);
-    az = warp_sum(az);
+    auto pull = [&](int j, double xj, double yj, double zj, double mj) {
+#pragma unroll
+        for (int k = 0; k < kTgtTile; k++) {
+            if (j == id[k]) continue;
+            const double dx = xi[k] - xj, dy = yi[k] - yj, dz = zi[k] - zj;
+            const double inv = rsqrt_f64(fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2))));
+            const double c = mj * inv * inv * inv;
+            ax[k] -= c * dx;
+            ay[k] -= c * dy;
+            az[k] -= c * dz;
+        }
+    };
+    const int j0 = blockIdx.y * chunk, j1 = min(n, j0 + chunk);
+    int j = j0 + threadIdx.x;
+    // kTgtUnroll sources per round, all their words loaded before any use
+    // (one memory latency per round); sources in the same order as one by one
+    for (; j + (kTgtUnroll - 1) * kTgtThreads < j1; j += kTgtUnroll * kTgtThreads) {
+        double xs[kTgtUnroll], ys[kTgtUnroll], zs[kTgtUnroll], ms[kTgtUnroll];
+        uint8_t as[kTgtUnroll];
+#pragma unroll
+        for (int u = 0; u < kTgtUnroll; u++) {
+            const int jj = j + u * kTgtThreads;
+            xs[u] = s.px[jj];
+            ys[u] = s.py[jj];
+            zs[u] = s.pz[jj];
+            ms[u] = s.mass[jj];
+            as[u] = s.active[jj];
+        }
+#pragma unroll
+        for (int u = 0; u < kTgtUnroll; u++)
+            if (as[u]) pull(j + u * kTgtThreads, xs[u], ys[u], zs[u], ms[u]);
+    }
+    for (; j < j1; j += kTgtThreads)
+        if (s.active[j]) pull(j, s.px[j], s.py[j], s.pz[j], s.mass[j]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) {
-        sh[0][warp] = ax;
-        sh[1][warp] = ay;
-        sh[2][warp] = az;
+#pragma unroll
+    for (int k = 0; k < kTgtTile; k++) {
+        const double vx = warp_sum(ax[k]), vy = warp_sum(ay[k]), vz = warp_sum(az[k]);
+        if (lane == 0) {
+            sh[3 * k][warp] = vx;
+            sh[3 * k + 1][warp] = vy;
+            sh[3 * k + 2][warp] = vz;
+        }
     }
     __syncthreads();
-    if (threadIdx.x < 3) {
+    if (threadIdx.x < 3 * kTgtTile && t0 + threadIdx.x / 3 < nt) {
         double t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[threadIdx.x][w];
-        out3[(size_t)blockIdx.x * 3 + threadIdx.x] = t;
+        for (int w = 0; w < kTgtThreads / 32; w++) t += sh[threadIdx.x][w];
+        out[((size_t)blockIdx.y * nt + t0) * 3 + threadIdx.x] = t;
     }
 }
 
+// out3[v] = sum over chunks c of part[c][v], in chunk order.
+__global__ void k_direct_targets_reduce(int nv, int chunks, const double* __restrict__ part,
+                                        double* __restrict__ out3) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    double t = 0;
+    for (int c = 0; c < chunks; c++) t += part[(size_t)c * nv + v];
+    out3[v] = t;
+}
+
+namespace {
+// Chunks per tile: about 8 blocks per SM in all, at least kTgtMinChunk
+// sources per chunk.
+int targets_chunks(int n, int nt, int sms) {
+    const int tiles = ceil_div(nt, kTgtTile);
+    const int want = ceil_div(sms * 8, tiles);
+    return std::max(1, std::min(want, ceil_div(n, kTgtMinChunk)));
+}
+}  // namespace
+
+size_t direct_targets_scratch_bytes(int sms) {
+    // chunks > 1 only when tiles < 8 sms, and then chunks * nt < 2 * 8 sms * kTgtTile
+    return sizeof(double) * 3 * (size_t)(16 * sms * kTgtTile);
+}
+
 void direct_targets(cudaStream_t st, int n, const State& s, double eps, int nt,
-                    const int32_t* targets, double* out3) {
-    if (nt > 0) k_direct_targets<<<nt, 256, 0, st>>>(n, s, eps * eps, targets, out3);
+                    const int32_t* targets, double* out3, double* scratch, int sms) {
+    if (nt <= 0 || n <= 0) {
+        if (nt > 0) cudaMemsetAsync(out3, 0, sizeof(double) * 3 * (size_t)nt, st);
+        return;
+    }
+    const int chunks = targets_chunks(n, nt, sms);
+    const int chunk = ceil_div(ceil_div(n, chunks), kTgtThreads) * kTgtThreads;
+    const int used = ceil_div(n, chunk);
+    const dim3 grid(ceil_div(nt, kTgtTile), used);
+    if (used == 1) {
+        k_direct_targets<<<grid, kTgtThreads, 0, st>>>(n, s, eps * eps, targets, nt, chunk, out3);
+        return;
+    }
+    k_direct_targets<<<grid, kTgtThreads, 0, st>>>(n, s, eps * eps, targets, nt, chunk, scratch);
+    k_direct_targets_reduce<<<ceil_div(3 * nt, 256), 256, 0, st>>>(3 * nt, used, scratch, out3);
 }
 
 }  // namespace nb

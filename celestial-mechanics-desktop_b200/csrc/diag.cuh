@@ -9,7 +9,10 @@ size_t diag_partial_bytes(int capacity);
 // pe_mode 0: exact pair sum; 1: 1/2 sum m_i phi_i from `phi` (by row).
 void diagnostics(cudaStream_t st, int n, const State& s, double eps, int pe_mode,
                  const double* phi, double* rows, double* part, double* out12);
+// FP64 direct-sum accelerations of rows targets[0 .. nt) into out3 (xyz per
+// target); scratch: direct_targets_scratch_bytes(sms).
+size_t direct_targets_scratch_bytes(int sms);
 void direct_targets(cudaStream_t st, int n, const State& s, double eps, int nt,
-                    const int32_t* targets, double* out3);
+                    const int32_t* targets, double* out3, double* scratch, int sms);
 
 }  // namespace nb

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "bodies.cuh"
@@ -82,6 +83,7 @@ struct nb_engine {
     nb::MacTrainImage* mac_ti = nullptr;  // transposed fragments for training
     float *mac_P = nullptr, *mac_m = nullptr, *mac_v = nullptr, *mac_G = nullptr;
     float *mac_norm = nullptr, *mac_loss = nullptr;
+    float* mac_part = nullptr;            // per-block gradient partials (training)
     int mac_adam_step = 0;
     float* samag = nullptr;               // sorted |a| of the previous step
     // training set (allocated by the first harvest)
@@ -116,6 +118,7 @@ struct nb_engine {
     int32_t* targets = nullptr;
     int2* groups = nullptr;
     double* tgt_out = nullptr;
+    double* tgt_part = nullptr;           // FP64 audit chunk partials
     nb::CollideBufs col{};
     Scal* scal = nullptr;
     std::vector<void*> allocs;
@@ -451,6 +454,7 @@ NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
         if ((r = dalloc(h, &h->rows, cap)) || (r = dalloc(h, &h->phi, cap))) break;
         if ((r = dalloc(h, (char**)&h->part, nb::diag_partial_bytes(capacity)))) break;
         if ((r = dalloc(h, &h->targets, cap)) || (r = dalloc(h, &h->tgt_out, 3 * cap))) break;
+        if ((r = dalloc(h, (char**)&h->tgt_part, nb::direct_targets_scratch_bytes(h->sms)))) break;
         if ((r = dalloc(h, &h->groups, cap))) break;
         if ((r = dalloc(h, &h->samag, cap))) break;
         if ((r = dalloc(h, &h->mac_node, 2 * cap))) break;
@@ -460,6 +464,7 @@ NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
             break;
         if ((r = dalloc(h, &h->mac_norm, nb::kMacNorm)) || (r = dalloc(h, &h->mac_loss, 4))) break;
         if ((r = dalloc(h, &h->mac_counts, 4))) break;
+        if ((r = dalloc(h, (char**)&h->mac_part, nb::mac_grad_partial_bytes(h->sms)))) break;
         if ((r = nb::collide_alloc(h->col, capacity, [h](void** p, size_t b) {
                  return dalloc(h, (char**)p, b);
              })))
@@ -840,13 +845,7 @@ __global__ void k_gather_acc(int ns, const int32_t* __restrict__ targets,
 int force_error_stats(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
                       double* out3) {
     const int n = h->n;
-    std::vector<uint8_t> act((size_t)n);
     int r;
-    if ((r = download(h, act.data(), h->s.active, (size_t)n))) return r;
-    if ((r = check_device(h))) return r;
-    std::vector<int32_t> cand;
-    for (int i = 0; i < n; i++)
-        if (act[i]) cand.push_back(i);
     // SplitMix64-driven partial Fisher-Yates: uniform sample without replacement
     uint64_t x = seed;
     auto next = [&x]() {
@@ -855,15 +854,43 @@ int force_error_stats(nb_engine* h, int32_t n_samples, uint64_t seed, double sof
         z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
         return z ^ (z >> 31);
     };
-    int ns = (n_samples <= 0 || n_samples >= (int)cand.size()) ? (int)cand.size() : n_samples;
-    if (ns < (int)cand.size())
+    std::vector<int32_t> cand;
+    int ns;
+    if (h->n_active == n && n_samples > 0 && n_samples < n) {
+        // every row active: the candidates are 0 .. n-1, so the shuffle only
+        // records the positions it touched (the same draws and the same
+        // sample as on the full list, without reading the active flags)
+        ns = n_samples;
+        std::unordered_map<int32_t, int32_t> moved;
+        moved.reserve(2 * (size_t)ns);
+        auto at = [&moved](int32_t k) {
+            auto it = moved.find(k);
+            return it == moved.end() ? k : it->second;
+        };
+        cand.resize(ns);
         for (int k = 0; k < ns; k++) {
-            uint64_t j = k + next() % (uint64_t)(cand.size() - k);
-            std::swap(cand[k], cand[j]);
+            const int32_t j = (int32_t)(k + next() % (uint64_t)(n - k));
+            const int32_t vk = at(k), vj = at(j);
+            moved[j] = vk;
+            cand[k] = vj;
         }
-    cand.resize(ns);
+    } else {
+        std::vector<uint8_t> act((size_t)n);
+        if ((r = download(h, act.data(), h->s.active, (size_t)n))) return r;
+        if ((r = check_device(h))) return r;
+        cand.reserve((size_t)n);
+        for (int i = 0; i < n; i++)
+            if (act[i]) cand.push_back(i);
+        ns = (n_samples <= 0 || n_samples >= (int)cand.size()) ? (int)cand.size() : n_samples;
+        if (ns < (int)cand.size())
+            for (int k = 0; k < ns; k++) {
+                uint64_t j = k + next() % (uint64_t)(cand.size() - k);
+                std::swap(cand[k], cand[j]);
+            }
+        cand.resize(ns);
+    }
     if ((r = upload(h, h->targets, cand.data(), sizeof(int32_t) * (size_t)ns))) return r;
-    nb::direct_targets(h->st, n, h->s, softening, ns, h->targets, h->tgt_out);
+    nb::direct_targets(h->st, n, h->s, softening, ns, h->targets, h->tgt_out, h->tgt_part, h->sms);
     std::vector<double> ref((size_t)ns * 3), ax, ay, az;
     if ((r = download(h, ref.data(), h->tgt_out, sizeof(double) * 3 * (size_t)ns))) return r;
     const bool gathered = 3 * (size_t)ns <= (size_t)h->capacity;  // fits the key scratch
@@ -1427,7 +1454,7 @@ NB_API int32_t nb_mac_train(nb_engine* h, int32_t epochs, int32_t batch, double 
         for (int row0 = 0; row0 < n; row0 += batch) {
             const int rows = std::min(batch, n - row0);
             nb::mac_grad(h->st, h->mac_X, h->mac_Y, order, row0, rows, h->mac_dev, h->mac_ti,
-                         h->mac_G, h->mac_loss, h->sms);
+                         h->mac_G, h->mac_loss, h->sms, h->mac_part);
             nb::mac_adam(h->st, h->mac_P, h->mac_G, h->mac_m, h->mac_v, ++h->mac_adam_step, (float)lr);
             nb::mac_image(h->st, h->mac_P, h->mac_norm, h->mac_dev, h->mac_ti);
         }
@@ -1486,7 +1513,8 @@ NB_API int32_t nb_mac_gradient(nb_engine* h, const float* X, const float* Y, int
         !(r = upload(h, dY, Y, sizeof(float) * (size_t)n)) &&
         !(r = upload(h, dO, ord.data(), sizeof(int) * (size_t)n))) {
         cudaMemsetAsync(h->mac_loss, 0, sizeof(float), h->st);
-        nb::mac_grad(h->st, dX, dY, dO, 0, n, h->mac_dev, h->mac_ti, h->mac_G, h->mac_loss, h->sms);
+        nb::mac_grad(h->st, dX, dY, dO, 0, n, h->mac_dev, h->mac_ti, h->mac_G, h->mac_loss, h->sms,
+                     h->mac_part);
         float l = 0.f;
         if (!(r = download(h, grad, h->mac_G, sizeof(float) * nb::kMacParams)) &&
             !(r = download(h, &l, h->mac_loss, sizeof(float))) && !(r = check_device(h)) && loss)

@@ -154,18 +154,20 @@ void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w, Ma
 // ---- training --------------------------------------------------------------
 
 constexpr int kTrainWarps = 4;
-
-struct TrainSmem {
-    float dW1[kMacIn][kMacHid];
-    float dW2[kMacHid][kMacHid];
-    float db1[kMacHid], db2[kMacHid], dw3[kMacHid];
-    float db3, loss;
-    // per warp staging of one 16-row tile
-    __nv_bfloat16 xs[kTrainWarps][16][16];
-    __nv_bfloat16 h1[kTrainWarps][16][kMacHid];
-    __nv_bfloat16 g2[kTrainWarps][16][kMacHid];
-    __nv_bfloat16 g1[kTrainWarps][16][kMacHid];
+// Per-warp gradient accumulator, laid out like the parameter vector plus the
+// loss: each warp adds only its own tiles' contributions (no two lanes of an
+// mma tile write the same entry), and the warps' and blocks' accumulators
+// are summed in a fixed order, so a gradient is bitwise reproducible.
+constexpr int kAccLoss = kMacParams;
+constexpr int kAccFloats = (kMacParams + 1 + 3) / 4 * 4;
+// per warp staging of one 16-row tile
+struct TrainStage {
+    __nv_bfloat16 xs[16][16];
+    __nv_bfloat16 h1[16][kMacHid];
+    __nv_bfloat16 g2[16][kMacHid];
+    __nv_bfloat16 g1[16][kMacHid];
 };
+constexpr int kTrainSmem = kTrainWarps * (kAccFloats * 4 + (int)sizeof(TrainStage));
 
 __device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16* p) {
     return *reinterpret_cast<const uint32_t*>(p);
@@ -179,14 +181,12 @@ __device__ __forceinline__ uint32_t pair_of(__nv_bfloat16 lo, __nv_bfloat16 hi) 
 __global__ void __launch_bounds__(kTrainWarps * 32)
 k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
             const int* __restrict__ order, int row0, int nrows, const MacDev* __restrict__ w,
-            const MacTrainImage* __restrict__ ti, float inv_batch, float* __restrict__ grad,
-            float* __restrict__ loss) {
-    __shared__ TrainSmem S;
+            const MacTrainImage* __restrict__ ti, float inv_batch, float* __restrict__ part) {
+    extern __shared__ __align__(16) float s_train[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t4 = lane & 3;
-    for (int e = threadIdx.x; e < kMacIn * kMacHid; e += blockDim.x) (&S.dW1[0][0])[e] = 0.f;
-    for (int e = threadIdx.x; e < kMacHid * kMacHid; e += blockDim.x) (&S.dW2[0][0])[e] = 0.f;
-    for (int e = threadIdx.x; e < kMacHid; e += blockDim.x) S.db1[e] = S.db2[e] = S.dw3[e] = 0.f;
-    if (threadIdx.x == 0) S.db3 = S.loss = 0.f;
+    for (int e = threadIdx.x; e < kTrainWarps * kAccFloats; e += blockDim.x) s_train[e] = 0.f;
+    float* A = s_train + warp * kAccFloats;  // this warp's accumulator
+    TrainStage& ST = reinterpret_cast<TrainStage*>(s_train + kTrainWarps * kAccFloats)[warp];
     __syncthreads();
     const int tiles = (nrows + 15) / 16;
     for (int tile = blockIdx.x * kTrainWarps + warp; tile < tiles; tile += gridDim.x * kTrainWarps) {
@@ -199,21 +199,21 @@ k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
                 const int row = order[row0 + r_lo + r];
                 v = (X[(size_t)row * kMacIn + k] - w->mean[k]) * w->inv_std[k];
             }
-            S.xs[warp][r][k] = __float2bfloat16_rn(v);
+            ST.xs[r][k] = __float2bfloat16_rn(v);
         }
         __syncwarp();
         // 2. layer 1 -> h1 (bf16, row-major in smem)
-        const uint32_t a0 = ld_pair(&S.xs[warp][g][2 * t4]), a1 = ld_pair(&S.xs[warp][g + 8][2 * t4]);
+        const uint32_t a0 = ld_pair(&ST.xs[g][2 * t4]), a1 = ld_pair(&ST.xs[g + 8][2 * t4]);
 #pragma unroll
         for (int nt = 0; nt < 8; nt++) {
             const float bl = w->b1[nt * 8 + 2 * t4], bh = w->b1[nt * 8 + 2 * t4 + 1];
             float c[4] = {bl, bh, bl, bh};
             mma_bf16(c, a0, a1, 0u, 0u, w->w1f[nt][lane]);
             const int col = nt * 8 + 2 * t4;
-            S.h1[warp][g][col] = __float2bfloat16_rn(fmaxf(c[0], 0.f));
-            S.h1[warp][g][col + 1] = __float2bfloat16_rn(fmaxf(c[1], 0.f));
-            S.h1[warp][g + 8][col] = __float2bfloat16_rn(fmaxf(c[2], 0.f));
-            S.h1[warp][g + 8][col + 1] = __float2bfloat16_rn(fmaxf(c[3], 0.f));
+            ST.h1[g][col] = __float2bfloat16_rn(fmaxf(c[0], 0.f));
+            ST.h1[g][col + 1] = __float2bfloat16_rn(fmaxf(c[1], 0.f));
+            ST.h1[g + 8][col] = __float2bfloat16_rn(fmaxf(c[2], 0.f));
+            ST.h1[g + 8][col + 1] = __float2bfloat16_rn(fmaxf(c[3], 0.f));
         }
         __syncwarp();
         // 3. layer 2 (pre-activations kept in registers) and output
@@ -226,8 +226,8 @@ k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
 #pragma unroll
             for (int kt = 0; kt < 4; kt++) {
                 const int k0 = kt * 16 + 2 * t4;
-                mma_bf16(z2[nt], ld_pair(&S.h1[warp][g][k0]), ld_pair(&S.h1[warp][g + 8][k0]),
-                         ld_pair(&S.h1[warp][g][k0 + 8]), ld_pair(&S.h1[warp][g + 8][k0 + 8]),
+                mma_bf16(z2[nt], ld_pair(&ST.h1[g][k0]), ld_pair(&ST.h1[g + 8][k0]),
+                         ld_pair(&ST.h1[g][k0 + 8]), ld_pair(&ST.h1[g + 8][k0 + 8]),
                          w->w2f[kt][nt][lane]);
             }
             const float wl = w->w3[nt * 8 + 2 * t4], wh = w->w3[nt * 8 + 2 * t4 + 1];
@@ -241,17 +241,20 @@ k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
         y0 += w->b3;
         y1 += w->b3;
         // 4. loss and dL/dy for rows g and g + 8 (mean squared error)
-        float d0 = 0.f, d1 = 0.f;
+        float d0 = 0.f, d1 = 0.f, lsq = 0.f;
         if (r_lo + g < nrows) {
             const float tg = (Y[order[row0 + r_lo + g]] - w->y_mean) / w->y_std;
             d0 = 2.f * (y0 - tg) * inv_batch;
-            if (t4 == 0) atomicAdd(&S.loss, (y0 - tg) * (y0 - tg));
+            if (t4 == 0) lsq += (y0 - tg) * (y0 - tg);
         }
         if (r_lo + g + 8 < nrows) {
             const float tg = (Y[order[row0 + r_lo + g + 8]] - w->y_mean) / w->y_std;
             d1 = 2.f * (y1 - tg) * inv_batch;
-            if (t4 == 0) atomicAdd(&S.loss, (y1 - tg) * (y1 - tg));
+            if (t4 == 0) lsq += (y1 - tg) * (y1 - tg);
         }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) lsq += __shfl_xor_sync(0xFFFFFFFFu, lsq, o);
+        if (lane == 0) A[kAccLoss] += lsq;
         // 5. g2 = dy w3 [z2 > 0]; dw3, db2 partials; db3
         float pdb3 = (t4 == 0) ? d0 + d1 : 0.f;
 #pragma unroll
@@ -260,10 +263,10 @@ k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
             const float wl = w->w3[col], wh = w->w3[col + 1];
             const float g00 = z2[nt][0] > 0.f ? d0 * wl : 0.f, g01 = z2[nt][1] > 0.f ? d0 * wh : 0.f;
             const float g10 = z2[nt][2] > 0.f ? d1 * wl : 0.f, g11 = z2[nt][3] > 0.f ? d1 * wh : 0.f;
-            S.g2[warp][g][col] = __float2bfloat16_rn(g00);
-            S.g2[warp][g][col + 1] = __float2bfloat16_rn(g01);
-            S.g2[warp][g + 8][col] = __float2bfloat16_rn(g10);
-            S.g2[warp][g + 8][col + 1] = __float2bfloat16_rn(g11);
+            ST.g2[g][col] = __float2bfloat16_rn(g00);
+            ST.g2[g][col + 1] = __float2bfloat16_rn(g01);
+            ST.g2[g + 8][col] = __float2bfloat16_rn(g10);
+            ST.g2[g + 8][col + 1] = __float2bfloat16_rn(g11);
             float w3l = fmaxf(z2[nt][0], 0.f) * d0 + fmaxf(z2[nt][2], 0.f) * d1;
             float w3h = fmaxf(z2[nt][1], 0.f) * d0 + fmaxf(z2[nt][3], 0.f) * d1;
             float b2l = g00 + g10, b2h = g01 + g11;
@@ -275,36 +278,36 @@ k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
                 b2h += __shfl_xor_sync(0xFFFFFFFFu, b2h, o);
             }
             if (g == 0) {
-                atomicAdd(&S.dw3[col], w3l);
-                atomicAdd(&S.dw3[col + 1], w3h);
-                atomicAdd(&S.db2[col], b2l);
-                atomicAdd(&S.db2[col + 1], b2h);
+                A[kMacW3 + col] += w3l;
+                A[kMacW3 + col + 1] += w3h;
+                A[kMacB2 + col] += b2l;
+                A[kMacB2 + col + 1] += b2h;
             }
         }
 #pragma unroll
         for (int o = 4; o < 32; o <<= 1) pdb3 += __shfl_xor_sync(0xFFFFFFFFu, pdb3, o);
-        if (lane == 0) atomicAdd(&S.db3, pdb3);
+        if (lane == 0) A[kMacB3] += pdb3;
         __syncwarp();
         // 6. dW2 += H1^T G2: M = 64 inputs (4 m-tiles), N = 64 outputs, K = 16 rows
 #pragma unroll
         for (int mt = 0; mt < 4; mt++) {
             const int i0 = mt * 16 + g;
-            const uint32_t b_a0 = pair_of(S.h1[warp][2 * t4][i0], S.h1[warp][2 * t4 + 1][i0]);
-            const uint32_t b_a1 = pair_of(S.h1[warp][2 * t4][i0 + 8], S.h1[warp][2 * t4 + 1][i0 + 8]);
-            const uint32_t b_a2 = pair_of(S.h1[warp][2 * t4 + 8][i0], S.h1[warp][2 * t4 + 9][i0]);
-            const uint32_t b_a3 = pair_of(S.h1[warp][2 * t4 + 8][i0 + 8], S.h1[warp][2 * t4 + 9][i0 + 8]);
+            const uint32_t b_a0 = pair_of(ST.h1[2 * t4][i0], ST.h1[2 * t4 + 1][i0]);
+            const uint32_t b_a1 = pair_of(ST.h1[2 * t4][i0 + 8], ST.h1[2 * t4 + 1][i0 + 8]);
+            const uint32_t b_a2 = pair_of(ST.h1[2 * t4 + 8][i0], ST.h1[2 * t4 + 9][i0]);
+            const uint32_t b_a3 = pair_of(ST.h1[2 * t4 + 8][i0 + 8], ST.h1[2 * t4 + 9][i0 + 8]);
 #pragma unroll
             for (int nt = 0; nt < 8; nt++) {
                 const int j = nt * 8 + g;
-                const uint2 bb = make_uint2(pair_of(S.g2[warp][2 * t4][j], S.g2[warp][2 * t4 + 1][j]),
-                                            pair_of(S.g2[warp][2 * t4 + 8][j], S.g2[warp][2 * t4 + 9][j]));
+                const uint2 bb = make_uint2(pair_of(ST.g2[2 * t4][j], ST.g2[2 * t4 + 1][j]),
+                                            pair_of(ST.g2[2 * t4 + 8][j], ST.g2[2 * t4 + 9][j]));
                 float c[4] = {0.f, 0.f, 0.f, 0.f};
                 mma_bf16(c, b_a0, b_a1, b_a2, b_a3, bb);
                 const int col = nt * 8 + 2 * t4;
-                atomicAdd(&S.dW2[i0][col], c[0]);
-                atomicAdd(&S.dW2[i0][col + 1], c[1]);
-                atomicAdd(&S.dW2[i0 + 8][col], c[2]);
-                atomicAdd(&S.dW2[i0 + 8][col + 1], c[3]);
+                A[kMacW2 + i0 * kMacHid + col] += c[0];
+                A[kMacW2 + i0 * kMacHid + col + 1] += c[1];
+                A[kMacW2 + (i0 + 8) * kMacHid + col] += c[2];
+                A[kMacW2 + (i0 + 8) * kMacHid + col + 1] += c[3];
             }
         }
         // 7. dH1 = G2 W2^T, g1 = dH1 [h1 > 0]; db1
@@ -314,19 +317,19 @@ k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
 #pragma unroll
             for (int kt = 0; kt < 4; kt++) {
                 const int k0 = kt * 16 + 2 * t4;
-                mma_bf16(c, ld_pair(&S.g2[warp][g][k0]), ld_pair(&S.g2[warp][g + 8][k0]),
-                         ld_pair(&S.g2[warp][g][k0 + 8]), ld_pair(&S.g2[warp][g + 8][k0 + 8]),
+                mma_bf16(c, ld_pair(&ST.g2[g][k0]), ld_pair(&ST.g2[g + 8][k0]),
+                         ld_pair(&ST.g2[g][k0 + 8]), ld_pair(&ST.g2[g + 8][k0 + 8]),
                          ti->w2tf[kt][nt][lane]);
             }
             const int col = nt * 8 + 2 * t4;
-            const float m00 = __bfloat162float(S.h1[warp][g][col]) > 0.f ? c[0] : 0.f;
-            const float m01 = __bfloat162float(S.h1[warp][g][col + 1]) > 0.f ? c[1] : 0.f;
-            const float m10 = __bfloat162float(S.h1[warp][g + 8][col]) > 0.f ? c[2] : 0.f;
-            const float m11 = __bfloat162float(S.h1[warp][g + 8][col + 1]) > 0.f ? c[3] : 0.f;
-            S.g1[warp][g][col] = __float2bfloat16_rn(m00);
-            S.g1[warp][g][col + 1] = __float2bfloat16_rn(m01);
-            S.g1[warp][g + 8][col] = __float2bfloat16_rn(m10);
-            S.g1[warp][g + 8][col + 1] = __float2bfloat16_rn(m11);
+            const float m00 = __bfloat162float(ST.h1[g][col]) > 0.f ? c[0] : 0.f;
+            const float m01 = __bfloat162float(ST.h1[g][col + 1]) > 0.f ? c[1] : 0.f;
+            const float m10 = __bfloat162float(ST.h1[g + 8][col]) > 0.f ? c[2] : 0.f;
+            const float m11 = __bfloat162float(ST.h1[g + 8][col + 1]) > 0.f ? c[3] : 0.f;
+            ST.g1[g][col] = __float2bfloat16_rn(m00);
+            ST.g1[g][col + 1] = __float2bfloat16_rn(m01);
+            ST.g1[g + 8][col] = __float2bfloat16_rn(m10);
+            ST.g1[g + 8][col + 1] = __float2bfloat16_rn(m11);
             float bl = m00 + m10, bh = m01 + m11;
 #pragma unroll
             for (int o = 4; o < 32; o <<= 1) {
@@ -334,47 +337,53 @@ k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
                 bh += __shfl_xor_sync(0xFFFFFFFFu, bh, o);
             }
             if (g == 0) {
-                atomicAdd(&S.db1[col], bl);
-                atomicAdd(&S.db1[col + 1], bh);
+                A[kMacB1 + col] += bl;
+                A[kMacB1 + col + 1] += bh;
             }
         }
         __syncwarp();
         // 8. dW1 += X^T G1: M = 16 features (8 used), N = 64, K = 16 rows
         {
-            const uint32_t x_a0 = pair_of(S.xs[warp][2 * t4][g], S.xs[warp][2 * t4 + 1][g]);
-            const uint32_t x_a1 = pair_of(S.xs[warp][2 * t4][g + 8], S.xs[warp][2 * t4 + 1][g + 8]);
-            const uint32_t x_a2 = pair_of(S.xs[warp][2 * t4 + 8][g], S.xs[warp][2 * t4 + 9][g]);
-            const uint32_t x_a3 = pair_of(S.xs[warp][2 * t4 + 8][g + 8], S.xs[warp][2 * t4 + 9][g + 8]);
+            const uint32_t x_a0 = pair_of(ST.xs[2 * t4][g], ST.xs[2 * t4 + 1][g]);
+            const uint32_t x_a1 = pair_of(ST.xs[2 * t4][g + 8], ST.xs[2 * t4 + 1][g + 8]);
+            const uint32_t x_a2 = pair_of(ST.xs[2 * t4 + 8][g], ST.xs[2 * t4 + 9][g]);
+            const uint32_t x_a3 = pair_of(ST.xs[2 * t4 + 8][g + 8], ST.xs[2 * t4 + 9][g + 8]);
 #pragma unroll
             for (int nt = 0; nt < 8; nt++) {
                 const int j = nt * 8 + g;
-                const uint2 bb = make_uint2(pair_of(S.g1[warp][2 * t4][j], S.g1[warp][2 * t4 + 1][j]),
-                                            pair_of(S.g1[warp][2 * t4 + 8][j], S.g1[warp][2 * t4 + 9][j]));
+                const uint2 bb = make_uint2(pair_of(ST.g1[2 * t4][j], ST.g1[2 * t4 + 1][j]),
+                                            pair_of(ST.g1[2 * t4 + 8][j], ST.g1[2 * t4 + 9][j]));
                 float c[4] = {0.f, 0.f, 0.f, 0.f};
                 mma_bf16(c, x_a0, x_a1, x_a2, x_a3, bb);
                 const int col = nt * 8 + 2 * t4;
                 if (g < kMacIn) {  // rows g + 8 are padding features
-                    atomicAdd(&S.dW1[g][col], c[0]);
-                    atomicAdd(&S.dW1[g][col + 1], c[1]);
+                    A[kMacW1 + g * kMacHid + col] += c[0];
+                    A[kMacW1 + g * kMacHid + col + 1] += c[1];
                 }
             }
         }
         __syncwarp();
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < kMacIn * kMacHid; e += blockDim.x)
-        atomicAdd(&grad[kMacW1 + e], (&S.dW1[0][0])[e]);
-    for (int e = threadIdx.x; e < kMacHid * kMacHid; e += blockDim.x)
-        atomicAdd(&grad[kMacW2 + e], (&S.dW2[0][0])[e]);
-    for (int e = threadIdx.x; e < kMacHid; e += blockDim.x) {
-        atomicAdd(&grad[kMacB1 + e], S.db1[e]);
-        atomicAdd(&grad[kMacB2 + e], S.db2[e]);
-        atomicAdd(&grad[kMacW3 + e], S.dw3[e]);
+    // this block's partial: its warps' accumulators in warp order
+    for (int e = threadIdx.x; e < kAccFloats; e += blockDim.x) {
+        float sum = 0.f;
+        for (int wi = 0; wi < kTrainWarps; wi++) sum += s_train[wi * kAccFloats + e];
+        part[(size_t)blockIdx.x * kAccFloats + e] = sum;
     }
-    if (threadIdx.x == 0) {
-        atomicAdd(&grad[kMacB3], S.db3);
-        atomicAdd(loss, S.loss);
-    }
+}
+
+// grad = the blocks' partials summed in block order; the loss is added to
+// *loss (it accumulates over the batches of an epoch).
+__global__ void k_mac_grad_reduce(int nblocks, const float* __restrict__ part,
+                                  float* __restrict__ grad, float* __restrict__ loss) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e > kMacParams) return;
+    float sum = 0.f;
+#pragma unroll 8
+    for (int b = 0; b < nblocks; b++) sum += part[(size_t)b * kAccFloats + e];
+    if (e < kMacParams) grad[e] = sum;
+    else *loss += sum;
 }
 
 __global__ void k_mac_adam(float* __restrict__ P, const float* __restrict__ G, float* __restrict__ m,
@@ -390,15 +399,26 @@ __global__ void k_mac_adam(float* __restrict__ P, const float* __restrict__ G, f
     P[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
+size_t mac_grad_partial_bytes(int sms) { return sizeof(float) * (size_t)kAccFloats * sms * 4; }
+
 void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order, int row0,
               int nrows, const MacDev* w, const MacTrainImage* ti, float* grad, float* loss,
-              int sms) {
-    cudaMemsetAsync(grad, 0, sizeof(float) * kMacParams, st);
-    if (nrows <= 0) return;
+              int sms, float* part) {
+    if (nrows <= 0) {
+        cudaMemsetAsync(grad, 0, sizeof(float) * kMacParams, st);
+        return;
+    }
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute((const void*)k_mac_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kTrainSmem);
+        attr = true;
+    }
     const int tiles = (nrows + 15) / 16;
     const int blocks = min(ceil_div(tiles, kTrainWarps), sms * 4);
-    k_mac_train<<<blocks, kTrainWarps * 32, 0, st>>>(X, Y, order, row0, nrows, w, ti,
-                                                      1.f / (float)nrows, grad, loss);
+    k_mac_train<<<blocks, kTrainWarps * 32, kTrainSmem, st>>>(X, Y, order, row0, nrows, w, ti,
+                                                               1.f / (float)nrows, part);
+    k_mac_grad_reduce<<<ceil_div(kMacParams + 1, 256), 256, 0, st>>>(blocks, part, grad, loss);
 }
 
 void mac_adam(cudaStream_t st, float* P, const float* G, float* m, float* v, int step, float lr) {

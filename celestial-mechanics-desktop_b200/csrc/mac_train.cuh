@@ -27,10 +27,12 @@ void mac_targets(cudaStream_t st, int nrec, const MacRecord* rec, const double4*
 void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w, MacTrainImage* ti);
 // Gradient of the mean squared error of rows order[row0 .. row0+nrows) into
 // grad (kMacParams floats, overwritten); the sum of squared errors is added
-// to *loss.
+// to *loss.  part: mac_grad_partial_bytes(sms) of scratch.  The result is
+// bitwise reproducible (no floating-point atomics).
+size_t mac_grad_partial_bytes(int sms);
 void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order, int row0,
               int nrows, const MacDev* w, const MacTrainImage* ti, float* grad, float* loss,
-              int sms);
+              int sms, float* part);
 void mac_adam(cudaStream_t st, float* P, const float* G, float* m, float* v, int step, float lr);
 void mac_predict(cudaStream_t st, const float* X, int n, const MacDev* w, float* out);
 // Per walk-tree node (2n slots, *t.n_nodes used): screen term and log2 mass.

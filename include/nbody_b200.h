@@ -292,7 +292,9 @@ NB_API int32_t nb_mac_train(nb_engine* h, int32_t epochs, int32_t batch, double 
 NB_API int32_t nb_mac_set_params(nb_engine* h, const float* params, int32_t n);
 NB_API int32_t nb_mac_get_params(nb_engine* h, float* params, int32_t n);
 /* Gradient (NB_MAC_PARAMS floats) of the mean squared error over the given
- * rows with the current parameters, computed by the training kernel. */
+ * rows with the current parameters, computed by the training kernel.  The
+ * kernel sums its partials in a fixed order, so gradients and trainings are
+ * bitwise reproducible on one device. */
 NB_API int32_t nb_mac_gradient(nb_engine* h, const float* X, const float* Y, int32_t n,
                                float* grad, double* loss);
 /* Predictions (log2 error units) of the walk's inference routine. */

@@ -72,6 +72,44 @@ def test_force_error_audit_matches_oracle(engine, oracle):
     assert rms < 1e-3
 
 
+def _sample_rows(active, ns, seed):
+    """The audit's sample: a SplitMix64-driven partial Fisher-Yates shuffle
+    of the active rows in index order (the first ns of the shuffled list)."""
+    m = (1 << 64) - 1
+    x = seed
+    cand = [int(i) for i in np.flatnonzero(active)]
+    for k in range(ns):
+        x = (x + 0x9E3779B97F4A7C15) & m
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+        z ^= z >> 31
+        j = k + z % (len(cand) - k)
+        cand[k], cand[j] = cand[j], cand[k]
+    return np.array(cand[:ns])
+
+
+@pytest.mark.parametrize("inactive", [False, True])
+def test_sampled_force_error_matches_oracle(engine, oracle, inactive):
+    """A sampled audit (all rows active, and with inactive rows) draws the
+    same bodies as the shuffle restated here and reports the oracle's
+    statistics over them against the FP64 direct sum."""
+    b = scenarios.plummer(30_000, seed=8)
+    if inactive:
+        b.active[::7] = 0
+    engine.set_param(N.PARAM_THETA, 0.6)
+    engine.set_state(b, old_acc=False)
+    engine.step(1, 0.0, 1e-4, MODE_BARNES_HUT)
+    got, _ = engine.get_state()
+    for ns, seed in ((700, 3), (2500, 0x5EED)):
+        mean, mx, rms = engine.force_error(ns, seed, 1e-4)
+        t = _sample_rows(b.active, ns, seed)
+        want = oracle.direct_forces_targets(b.px, b.py, b.pz, b.mass, b.active, 1e-4, t)
+        wm, wx, wr = oracle.force_error((got.ax[t], got.ay[t], got.az[t]), want)
+        assert mean == pytest.approx(wm, rel=1e-9) and rms == pytest.approx(wr, rel=1e-9)
+        assert mx == pytest.approx(wx, rel=1e-9)
+
+
 def test_merge_and_compaction_step_bit_exact(engine, oracle):
     """dt = 0 step with collisions: pairs, merges (sequential CPU-resolver
     semantics) and compaction equal the oracle's."""
