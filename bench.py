@@ -1044,7 +1044,8 @@ def main():
             line = run_b200(args, ws, rank, local)
             if line is not None:
                 # the learned arm adds one kernel per step (per-node screen terms)
-                line["gpu_launches"] = (launches_per_step() + 1) * args.steps
+                # and its audit three (FP64 targets, chunk reduction, gather)
+                line["gpu_launches"] = (launches_per_step() + 1) * args.steps + 3
                 print(json.dumps(line))
     finally:
         if ws > 1:
