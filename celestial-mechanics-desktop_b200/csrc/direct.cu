@@ -35,6 +35,10 @@ constexpr int kD32Per = NB_D32_PER;  // targets per thread (even: packed in pair
 static_assert(kD32Per % 2 == 0, "targets are packed two per f32x2 register");
 constexpr int kD32Tile = kD32Threads;
 constexpr int kD32MinChunk = 4096;    // sources per chunk at least
+#ifndef NB_D32_UNROLL
+#define NB_D32_UNROLL 8
+#endif
+constexpr int kD32Unroll = NB_D32_UNROLL;  // source loop unroll
 
 __device__ __forceinline__ void kahan32(float& s, float& c, float x) {
     float y = x - c;
@@ -108,16 +112,20 @@ k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict_
             bz[u] = (float)(b.z - ref.z);
             sx[u] = sy[u] = sz[u] = cx[u] = cy[u] = cz[u] = 0.f;
         }
+        // the next j-tile's source is loaded while the current one is evaluated
+        double4 qn = make_double4(0.0, 0.0, 0.0, 0.0);
+        float Rn = 0.f;
+        if (j0 + (int)threadIdx.x < j1) {
+            qn = sbody[j0 + threadIdx.x];
+            if (SHELL) Rn = srad[j0 + threadIdx.x];
+        }
         for (int base = j0; base < j1; base += kD32Tile) {
             const int j = base + threadIdx.x;
             float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            float R = 0.f;
-            if (j < j1) {
-                const double4 q = sbody[j];
-                q4 = make_float4((float)(q.x - ref.x), (float)(q.y - ref.y), (float)(q.z - ref.z),
-                                 (float)q.w);
-                if (SHELL) R = srad[j];
-            }
+            const float R = Rn;
+            if (j < j1)
+                q4 = make_float4((float)(qn.x - ref.x), (float)(qn.y - ref.y), (float)(qn.z - ref.z),
+                                 (float)qn.w);
             if constexpr (SHELL) {
                 sj[threadIdx.x] = q4;
                 const float id = rsqrtf(R * R + eps2);
@@ -129,6 +137,10 @@ k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict_
                 sj2[threadIdx.x] = make_float4(q4.z, q4.z, q4.w, q4.w);
             }
             __syncthreads();
+            if (j + kD32Tile < j1) {
+                qn = sbody[j + kD32Tile];
+                if (SHELL) Rn = srad[j + kD32Tile];
+            }
             const int cnt = min(kD32Tile, j1 - base);
             float tx[kD32Per], ty[kD32Per], tz[kD32Per];
 #pragma unroll
@@ -164,7 +176,7 @@ k_direct_fp32(int n, const double4* __restrict__ sbody, const float* __restrict_
                     AX[p] = AY[p] = AZ[p] = 0ull;
                 }
                 const f32x2 E2 = pk2(eps2, eps2);
-#pragma unroll 4
+#pragma unroll kD32Unroll
                 for (int k = 0; k < cnt; k++) {
                     const float4 qa = sj[k], qb = sj2[k];
                     const f32x2 qx = pk2(qa.x, qa.y), qy = pk2(qa.z, qa.w);

@@ -26,8 +26,14 @@ namespace nb {
 
 constexpr int kWalkWarps = 8;
 constexpr int kWalkThreads = kWalkWarps * 32;
-constexpr int kCellCap = 128;
-constexpr int kPartCap = 128;
+#ifndef NB_WALK_CELL_CAP
+#define NB_WALK_CELL_CAP 128
+#endif
+#ifndef NB_WALK_PART_CAP
+#define NB_WALK_PART_CAP 128
+#endif
+constexpr int kCellCap = NB_WALK_CELL_CAP;
+constexpr int kPartCap = NB_WALK_PART_CAP;
 // per-warp shared memory, in floats
 constexpr int kWarpFloats = kCellCap * 10 + kPartCap * 4 + kPartCap * 2 + kPartCap;
 constexpr int kWalkSmem = kWalkWarps * kWarpFloats * 4;
