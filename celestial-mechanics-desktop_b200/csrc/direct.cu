@@ -354,12 +354,24 @@ void direct_fp32(cudaStream_t st, int n, const double4* sbody, const float* srad
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kD32Threads, 0);
     const int resident = sms * (per_sm > 0 ? per_sm : 1);
     const int tiles = ceil_div(n, kD32Threads * kD32Per);
-    // enough items for about 8 waves, chunks of at least kD32MinChunk
-    // sources, partials within the scratch
-    long long chunks = ceil_div(8LL * resident, tiles);
-    chunks = std::min<long long>(chunks, std::max(1, ceil_div(n, kD32MinChunk)));
-    chunks = std::min<long long>(chunks, (long long)(scratch_bytes / (sizeof(double) * 3 * (size_t)n)));
-    if (chunks < 1) chunks = 1;
+    // Chunks per tile: at least 4 waves of items where the scratch and the
+    // kD32MinChunk floor allow, and among those the count whose last wave is
+    // fullest (every item costs the same, so a part-filled last wave idles
+    // the rest of the GPU: 3 chunks of 1024 tiles on 296 resident blocks
+    // leave 62 % of the 11th wave empty, 2 or 4 chunks about 8 %).
+    const long long cmax = std::max<long long>(
+        1, std::min<long long>(std::max(1, ceil_div(n, kD32MinChunk)),
+                               (long long)(scratch_bytes / (sizeof(double) * 3 * (size_t)n))));
+    const long long cmin = std::min<long long>(cmax, std::max(1, ceil_div(4LL * resident, tiles)));
+    auto fill = [&](long long c) {
+        const long long nc = ceil_div(n, ceil_div(n, (int)c));  // chunks actually formed
+        const long long it = (long long)tiles * nc;
+        return (double)it / (double)(((it + resident - 1) / resident) * resident);
+    };
+    double best = 0.0;
+    for (long long c = cmin; c <= cmax; c++) best = std::max(best, fill(c));
+    long long chunks = cmin;  // the fewest chunks within 0.5 % of the best fill
+    while (chunks < cmax && fill(chunks) < best - 0.005) chunks++;
     const int chunk_len = ceil_div(n, (int)chunks);
     const int nchunks = ceil_div(n, chunk_len);
     const int items = tiles * nchunks;
