@@ -29,7 +29,7 @@ namespace nb {
 #endif
 constexpr int kD32Threads = NB_D32_THREADS;
 #ifndef NB_D32_PER
-#define NB_D32_PER 4
+#define NB_D32_PER 10
 #endif
 constexpr int kD32Per = NB_D32_PER;  // targets per thread (even: packed in pairs)
 static_assert(kD32Per % 2 == 0, "targets are packed two per f32x2 register");
