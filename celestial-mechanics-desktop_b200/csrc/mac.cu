@@ -408,12 +408,10 @@ void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order,
         cudaMemsetAsync(grad, 0, sizeof(float) * kMacParams, st);
         return;
     }
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute((const void*)k_mac_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kTrainSmem);
-        attr = true;
-    }
+    // per call: the attribute belongs to the current device, and handles on
+    // several devices share this function (a host-side call of a microsecond)
+    cudaFuncSetAttribute((const void*)k_mac_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kTrainSmem);
     const int tiles = (nrows + 15) / 16;
     const int blocks = min(ceil_div(tiles, kTrainWarps), sms * 4);
     k_mac_train<<<blocks, kTrainWarps * 32, kTrainSmem, st>>>(X, Y, order, row0, nrows, w, ti,
