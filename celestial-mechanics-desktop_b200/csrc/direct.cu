@@ -31,7 +31,11 @@ constexpr int kD32Threads = NB_D32_THREADS;
 #ifndef NB_D32_PER
 #define NB_D32_PER 10
 #endif
-constexpr int kD32Per = NB_D32_PER;  // targets per thread (even: packed in pairs)
+// targets per thread (even: packed in pairs).  10 keeps five independent
+// packed chains per source in flight at 240 registers (one block of 8 warps
+// per SM); measured against 4 (2 blocks per SM), 6 and 8 it feeds the FMA
+// pipe best.
+constexpr int kD32Per = NB_D32_PER;
 static_assert(kD32Per % 2 == 0, "targets are packed two per f32x2 register");
 constexpr int kD32Tile = kD32Threads;
 constexpr int kD32MinChunk = 4096;    // sources per chunk at least

@@ -26,6 +26,9 @@ namespace nb {
 
 constexpr int kWalkWarps = 8;
 constexpr int kWalkThreads = kWalkWarps * 32;
+// Interaction-list capacities per warp (entries before a flush).  128 / 128
+// measured within 1 % of 96 / 96 and 64 / 64 on both walks: a smaller list
+// gives L1 more of the shared-memory carve-out but flushes more often.
 #ifndef NB_WALK_CELL_CAP
 #define NB_WALK_CELL_CAP 128
 #endif
