@@ -110,7 +110,11 @@ __device__ __forceinline__ uint64_t quant_cube(double p, double lo, double inv2h
 }
 
 constexpr int kKeyThreads = 256;
+constexpr int kKeyItems = 8;  // keys per thread: one block's histograms cover 2048 keys
 
+// Cube-mode keys of kKeyItems keys per thread, plus the digit histograms of
+// all 8 sort passes; a block folds its 2048 keys into shared bins and adds
+// the non-zero bins to the global counts (fewer global atomics per key).
 __global__ void __launch_bounds__(kKeyThreads)
 k_keys_cube(int n, State s, const double* __restrict__ cube, uint64_t* __restrict__ keys,
             uint32_t* __restrict__ vals, uint32_t* __restrict__ hist) {
@@ -120,25 +124,27 @@ k_keys_cube(int n, State s, const double* __restrict__ cube, uint64_t* __restric
     const double h = cube[3];
     const double inv2h = 1.0 / __dmul_rn(2.0, h);
     const double lx = __dsub_rn(cube[0], h), ly = __dsub_rn(cube[1], h), lz = __dsub_rn(cube[2], h);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t key = kInactiveKey;
-    if (i < n) {
-        if (s.active[i])
-            key = (spread21(quant_cube(s.px[i], lx, inv2h)) << 2) |
-                  (spread21(quant_cube(s.py[i], ly, inv2h)) << 1) |
-                  spread21(quant_cube(s.pz[i], lz, inv2h));
-        keys[i] = key;
-        vals[i] = (uint32_t)i;
-    }
-    // digit histograms of all 8 passes, warp-aggregated (Morton digits of a
-    // clustered system pile up in a few bins)
+    for (int k = 0; k < kKeyItems; k++) {
+        const int i = (blockIdx.x * kKeyItems + k) * kKeyThreads + threadIdx.x;
+        uint64_t key = kInactiveKey;
+        if (i < n) {
+            if (s.active[i])
+                key = (spread21(quant_cube(s.px[i], lx, inv2h)) << 2) |
+                      (spread21(quant_cube(s.py[i], ly, inv2h)) << 1) |
+                      spread21(quant_cube(s.pz[i], lz, inv2h));
+            keys[i] = key;
+            vals[i] = (uint32_t)i;
+        }
+        // warp-aggregated (Morton digits of a clustered system pile up in a
+        // few bins)
 #pragma unroll
-    for (int p = 0; p < 8; p++) {
-        const uint32_t d = (uint32_t)(key >> (8 * p)) & 0xFF;
-        const bool live = i < n;
-        const unsigned lm = __ballot_sync(0xFFFFFFFFu, live);
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, live ? d : 0x100u) & lm;
-        if (live && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][d], (uint32_t)__popc(peers));
+        for (int p = 0; p < 8; p++) {
+            const uint32_t d = (uint32_t)(key >> (8 * p)) & 0xFF;
+            const bool live = i < n;
+            const unsigned lm = __ballot_sync(0xFFFFFFFFu, live);
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, live ? d : 0x100u) & lm;
+            if (live && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][d], (uint32_t)__popc(peers));
+        }
     }
     __syncthreads();
     for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) {
@@ -219,7 +225,9 @@ void launch_cube(cudaStream_t st, const unsigned long long* bbox_ord, const doub
 void launch_keys_cube(cudaStream_t st, int n, const State& s, const double* cube,
                       uint64_t* keys, uint32_t* vals, uint32_t* hist) {
     cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, st);
-    if (n > 0) k_keys_cube<<<ceil_div(n, kKeyThreads), kKeyThreads, 0, st>>>(n, s, cube, keys, vals, hist);
+    if (n > 0)
+        k_keys_cube<<<ceil_div(n, kKeyThreads * kKeyItems), kKeyThreads, 0, st>>>(n, s, cube, keys,
+                                                                                  vals, hist);
 }
 
 void launch_keys_aabb(cudaStream_t st, int n, const State& s,

@@ -236,33 +236,37 @@ __device__ __forceinline__ uint64_t quant17(double p, double lo, double inv2h) {
 }
 
 // Keys (system | 17-bit Morton in the system's cube) and the 8 digit
-// histograms of the radix sort (hist zeroed before).
+// histograms of the radix sort (hist zeroed before); kEnsKeyItems keys per
+// thread, so a block's shared bins cover 2048 keys before the global adds.
+constexpr int kEnsKeyItems = 8;
 __global__ void k_ens_keys(int n, State s, const int* __restrict__ sys_of,
                            const double4* __restrict__ cubes, uint64_t* __restrict__ keys,
                            uint32_t* __restrict__ vals, uint32_t* __restrict__ hist) {
     __shared__ uint32_t sh[8][256];
     for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) (&sh[0][0])[t] = 0;
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t key = 0;
-    if (i < n) {
-        const int sys = sys_of[i];
-        const double4 c = cubes[sys];
-        const double inv2h = 1.0 / __dmul_rn(2.0, c.w);
-        const double lx = __dsub_rn(c.x, c.w), ly = __dsub_rn(c.y, c.w), lz = __dsub_rn(c.z, c.w);
-        key = ((uint64_t)sys << kEnsSysShift) |
-              (spread21(quant17(s.px[i], lx, inv2h)) << 2) |
-              (spread21(quant17(s.py[i], ly, inv2h)) << 1) | spread21(quant17(s.pz[i], lz, inv2h));
-        keys[i] = key;
-        vals[i] = (uint32_t)i;
-    }
+    for (int k = 0; k < kEnsKeyItems; k++) {
+        const int i = (blockIdx.x * kEnsKeyItems + k) * blockDim.x + threadIdx.x;
+        uint64_t key = 0;
+        if (i < n) {
+            const int sys = sys_of[i];
+            const double4 c = cubes[sys];
+            const double inv2h = 1.0 / __dmul_rn(2.0, c.w);
+            const double lx = __dsub_rn(c.x, c.w), ly = __dsub_rn(c.y, c.w), lz = __dsub_rn(c.z, c.w);
+            key = ((uint64_t)sys << kEnsSysShift) |
+                  (spread21(quant17(s.px[i], lx, inv2h)) << 2) |
+                  (spread21(quant17(s.py[i], ly, inv2h)) << 1) | spread21(quant17(s.pz[i], lz, inv2h));
+            keys[i] = key;
+            vals[i] = (uint32_t)i;
+        }
 #pragma unroll
-    for (int p = 0; p < 8; p++) {
-        const uint32_t d = (uint32_t)(key >> (8 * p)) & 0xFF;
-        const bool live = i < n;
-        const unsigned lm = __ballot_sync(0xFFFFFFFFu, live);
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, live ? d : 0x100u) & lm;
-        if (live && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][d], (uint32_t)__popc(peers));
+        for (int p = 0; p < 8; p++) {
+            const uint32_t d = (uint32_t)(key >> (8 * p)) & 0xFF;
+            const bool live = i < n;
+            const unsigned lm = __ballot_sync(0xFFFFFFFFu, live);
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, live ? d : 0x100u) & lm;
+            if (live && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][d], (uint32_t)__popc(peers));
+        }
     }
     __syncthreads();
     for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) {
@@ -541,8 +545,8 @@ void enqueue_forces(nb_ensemble* h, double eps) {
         const double* half16 = h->d_half16 + h->nds;
         uint32_t* hist = (uint32_t*)h->sort_ws;
         cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, st);
-        nb::k_ens_keys<<<nb::ceil_div(n, 256), 256, 0, st>>>(n, h->sbh, h->d_sys_of_bh, cubes,
-                                                            h->keys0, h->vals0, hist);
+        nb::k_ens_keys<<<nb::ceil_div(n, 256 * nb::kEnsKeyItems), 256, 0, st>>>(
+            n, h->sbh, h->d_sys_of_bh, cubes, h->keys0, h->vals0, hist);
         nb::sort_pairs(st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err,
                        h->sms);
         nb::launch_gather(st, n, h->sbh, h->vals0, h->sbody, nullptr, nullptr);
