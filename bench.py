@@ -48,8 +48,11 @@ FLOPS_BODY, FLOPS_CELL_QUAD = 20, 51
 # key+row) + 8 radix passes x 24 (read and write key+row) + gather 68 (read
 # row, pos, mass; write double4) = 450; tree stage = radix tree 29 (read key,
 # write children/range/prefix/parent) + mark 35 + scan/base 8 + emit 40 +
-# multipoles 32 + 0.45 nodes/body x 100 = 189.
-SORT_BYTES_PER_BODY, TREE_BYTES_PER_BODY = 450, 189
+# multipoles 32 + 100 per walk-tree node.
+SORT_BYTES_PER_BODY = 450
+# tree stage without the per-node part: 29 + 35 + 8 + 40 + 32 = 144 B/body,
+# plus 100 B per walk-tree node (the node count is read from the engine)
+TREE_BYTES_PER_BODY_FIXED, TREE_BYTES_PER_NODE = 144, 100
 DISK_RADIUS_SCALE = 30.0
 
 
@@ -496,6 +499,9 @@ def run_b200(args, ws, rank, local):
                              "theta 0.5, monopole)"}
         sort_s = arm_l["stage_ms"]["sort"] / 1e3
         tree_s = arm_l["stage_ms"]["tree"] / 1e3
+        # walk-tree nodes of the last evaluation (same bodies, same tree shape)
+        nodes_per_body = int(eng.counters()[N.C_NODES]) / n
+        tree_bpb = TREE_BYTES_PER_BODY_FIXED + TREE_BYTES_PER_NODE * nodes_per_body
         line = {
             "metric": METRIC, "value": arm_l["steps_per_s"], "unit": "steps/s", "n_gpus": ws,
             "steps": args.steps, "warmup": max(args.warmup, 3),
@@ -532,9 +538,10 @@ def run_b200(args, ws, rank, local):
                                                            "force_error", "stage_ms")},
             "stage_gbs": {
                 "sort": SORT_BYTES_PER_BODY * n / sort_s / 1e9,
-                "tree": TREE_BYTES_PER_BODY * n / tree_s / 1e9,
+                "tree": tree_bpb * n / tree_s / 1e9,
                 "hbm_peak": pk.get("hbm_gbs", 6458.1),
-                "bytes_per_body": {"sort": SORT_BYTES_PER_BODY, "tree": TREE_BYTES_PER_BODY},
+                "bytes_per_body": {"sort": SORT_BYTES_PER_BODY, "tree": round(tree_bpb, 1)},
+                "nodes_per_body": nodes_per_body,
                 "note": "sort = kick-drift+bbox, keys+histograms, 8 radix passes, gather; "
                         "tree = radix tree, octree mark/scan/emit, multipoles"},
             "gpu_launches": None,

@@ -68,7 +68,8 @@ enum nb_mode {
 /* Parameter ids for nb_set_param_f64 / nb_set_param_i32. */
 enum nb_param {
     NB_PARAM_THETA = 1,            /* f64, opening angle, default 0.5                         */
-    NB_PARAM_LEAF_CAPACITY = 2,    /* i32, bodies per leaf bucket of the walk tree, default 8  */
+    NB_PARAM_LEAF_CAPACITY = 2,    /* i32, bodies per leaf bucket of the walk tree, 1..64,
+                                      default 24                                              */
     NB_PARAM_MAX_MERGES_FRAME = 3, /* i32, default 64 (simulation_config.hpp:57)               */
     NB_PARAM_MAX_MERGES_BODY = 4,  /* i32, default 2  (simulation_config.hpp:58)               */
     NB_PARAM_MIN_RADIUS = 5,       /* f64, density-model floor for merged radii, default 1e-6
