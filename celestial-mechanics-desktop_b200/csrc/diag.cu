@@ -112,8 +112,10 @@ size_t diag_partial_bytes(int capacity) {
     return sizeof(double) * kDiagVals * (size_t)ceil_div(capacity > 0 ? capacity : 1, kDiagThreads);
 }
 
-// FP64 direct sum for target rows (ForceErrorAnalyzer's exact reference,
-// CpuSingleThreadBackend arithmetic per pair).  Block (tile, chunk) sums
+// FP64 direct sum for target rows (ForceErrorAnalyzer's exact reference:
+// the softened Newtonian pair term of CpuSingleThreadBackend, evaluated in
+// FP64 with FMA contraction and the 1/sqrt below, so it agrees with the CPU
+// sum to a few FP64 ulps per pair, not bit for bit).  Block (tile, chunk) sums
 // kTgtTile targets over one chunk of the sources: each source is loaded once
 // per tile rather than once per target, and the chunks give enough blocks
 // for a few hundred targets.  The block's threads split the chunk, the
