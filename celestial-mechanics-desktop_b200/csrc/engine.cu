@@ -327,6 +327,23 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
 // Capture one device step (forces + second half kick) as a CUDA graph, or
 // reuse the captured one when nothing it depends on changed.  Per-stage
 // timing events are not recorded inside the graph.
+// Yoshida 4th-order sub-step multipliers, computed as the reference computes
+// them (YoshidaCoefficients, engine/include/celestial/sim/yoshida.hpp:19-24)
+constexpr double kCbrt2 = 1.2599210498948732;
+constexpr double kYoshidaW1 = 1.0 / (2.0 - kCbrt2);
+constexpr double kYoshidaW0 = -kCbrt2 / (2.0 - kCbrt2);
+constexpr double kYoshidaSub[3] = {kYoshidaW1, kYoshidaW0, kYoshidaW1};
+
+// The sub-step time steps of one step: dt itself, or Yoshida's three.
+int sub_steps(int flags, double dt, double* sub) {
+    if (!(flags & NB_FLAG_YOSHIDA4)) {
+        sub[0] = dt;
+        return 1;
+    }
+    for (int s = 0; s < 3; s++) sub[s] = kYoshidaSub[s] * dt;
+    return 3;
+}
+
 int step_graph(nb_engine* h, int flags, double dt, double eps) {
     const nb_engine::GraphKey key{flags,           h->n,           h->n_active,
                                   h->leaf_cap,     dt,             eps,
@@ -342,8 +359,13 @@ int step_graph(nb_engine* h, int flags, double dt, double eps) {
     h->timing = 0;
     cudaGraph_t g = nullptr;
     NB_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-    int r = force_pipeline(h, flags, eps, true, dt);
-    if (r == NB_OK) nb::launch_kick(h->st, h->n, h->s, dt);
+    double sub[3];
+    const int ns = sub_steps(flags, dt, sub);
+    int r = NB_OK;
+    for (int k = 0; k < ns && r == NB_OK; k++) {
+        r = force_pipeline(h, flags, eps, true, sub[k]);
+        if (r == NB_OK) nb::launch_kick(h->st, h->n, h->s, sub[k]);
+    }
     const cudaError_t e = cudaStreamEndCapture(h->st, &g);
     h->timing = timing;
     if (r != NB_OK) {
@@ -695,9 +717,12 @@ int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags)
         collect_counters(h);
         return NB_OK;
     }
-    for (int k = 0; k < n_steps; k++) {
-        if ((r = force_pipeline(h, flags, softening, true, dt))) return r;
-        nb::launch_kick(h->st, h->n, h->s, dt);
+    double sub[3];
+    const int ns = sub_steps(flags, dt, sub);
+    for (int k = 0; k < n_steps * ns; k++) {
+        const double sdt = sub[k % ns];
+        if ((r = force_pipeline(h, flags, softening, true, sdt))) return r;
+        nb::launch_kick(h->st, h->n, h->s, sdt);
         if (collide) {
             nb::CollideArgs c{};
             c.n = h->n;

@@ -35,6 +35,7 @@ FLAG_SHELL_THEOREM = 0x10
 FLAG_NO_QUADRUPOLE = 0x20
 FLAG_COLLISIONS = 0x40
 FLAG_LEARNED_MAC = 0x80
+FLAG_YOSHIDA4 = 0x100
 # parameters
 PARAM_THETA = 1
 PARAM_LEAF_CAPACITY = 2

@@ -64,6 +64,12 @@ enum nb_mode {
 #define NB_FLAG_NO_QUADRUPOLE 0x20  /* monopole only in NB_MODE_BARNES_HUT                   */
 #define NB_FLAG_COLLISIONS 0x40     /* nb_step: broad phase + merge + compaction per step    */
 #define NB_FLAG_LEARNED_MAC 0x80    /* NB_MODE_BARNES_HUT: MLP opening criterion              */
+/* nb_step: each step is Yoshida's 4th-order composition of three KDK
+ * sub-steps of w1 dt, w0 dt, w1 dt, w1 = 1 / (2 - 2^(1/3)), w0 = -2^(1/3) w1
+ * (IntegratorType::Yoshida4: engine/include/celestial/sim/yoshida.hpp:8-27,
+ * Engine::cpu_yoshida_substep, engine/src/sim/engine.cpp:685-746), three
+ * force evaluations per step. */
+#define NB_FLAG_YOSHIDA4 0x100
 
 /* Parameter ids for nb_set_param_f64 / nb_set_param_i32. */
 enum nb_param {

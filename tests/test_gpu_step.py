@@ -6,8 +6,9 @@ import numpy as np
 import pytest
 
 from conftest import bodies_dict
-from nbody_b200 import (FLAG_COLLISIONS, FLAG_SHELL_THEOREM, MODE_BARNES_HUT, MODE_DIRECT_FP64,
-                        NBodyError, scenarios)
+from nbody_b200 import (FLAG_COLLISIONS, FLAG_SHELL_THEOREM, FLAG_YOSHIDA4, MODE_BARNES_HUT,
+                        MODE_DIRECT_FP64, NBodyError, scenarios)
+from nbody_b200.scenarios import Bodies
 from nbody_b200 import _native as N
 
 pytestmark = pytest.mark.gpu
@@ -25,6 +26,61 @@ def test_verlet_fp64_trajectory_bit_exact(engine, oracle):
     np.testing.assert_array_equal(ids, np.arange(300))
     for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az"):
         np.testing.assert_array_equal(getattr(got, k), want[k], err_msg=k)
+
+
+YOSHIDA_W1 = 1.0 / (2.0 - 1.2599210498948732)
+YOSHIDA_W0 = -1.2599210498948732 / (2.0 - 1.2599210498948732)
+
+
+def test_yoshida4_fp64_trajectory_bit_exact(engine, oracle):
+    """Yoshida4 steps (three KDK sub-steps of w1 dt, w0 dt, w1 dt, as the
+    reference's Engine::cpu_yoshida_substep composes them) with the FP64
+    direct sum equal the oracle's Verlet sub-steps chained the same way, bit
+    for bit, through the captured-graph path and the step-by-step path."""
+    b = scenarios.plummer(300, seed=0)
+    b.active[::17] = 0
+    want = bodies_dict(b)
+    for _ in range(20):
+        for w in (YOSHIDA_W1, YOSHIDA_W0, YOSHIDA_W1):
+            want = dict(oracle.verlet_direct(want | {"active": b.active}, 1e-4, w * 1e-3, 1),
+                        active=b.active)
+    for one_by_one in (False, True):
+        engine.set_state(b)
+        if one_by_one:
+            for _ in range(20):
+                engine.step(1, 1e-3, 1e-4, MODE_DIRECT_FP64 | FLAG_YOSHIDA4)
+        else:
+            engine.step(20, 1e-3, 1e-4, MODE_DIRECT_FP64 | FLAG_YOSHIDA4)
+        got, _ = engine.get_state()
+        for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az"):
+            np.testing.assert_array_equal(getattr(got, k), want[k], err_msg=(k, one_by_one))
+
+
+def test_yoshida4_energy_error_is_fourth_order(engine):
+    """Two bodies on an eccentric orbit (G = 1, total mass 1, separation 1 at
+    apocentre, speeds 0.8 of circular): over 2 pi time units the energy error
+    of Yoshida4 is far below Verlet's at the same dt, and shrinks about
+    16-fold when dt halves (4th order; Verlet's shrinks 4-fold)."""
+    def run(flags, dt):
+        v = 0.4  # circular would be 0.5: v^2 / 0.5 = 0.5 / 1^2
+        b = Bodies(px=np.array([0.5, -0.5]), py=np.zeros(2), pz=np.zeros(2),
+                   vx=np.zeros(2), vy=np.array([v, -v]), vz=np.zeros(2),
+                   mass=np.array([0.5, 0.5]), radius=np.zeros(2), active=np.ones(2, np.uint8))
+        engine.set_state(b, old_acc=False)
+        engine.step(1, 0.0, 1e-6, MODE_DIRECT_FP64)  # accelerations at the start
+        e0 = engine.diagnostics(1e-6)["e"]
+        steps = int(round(2 * np.pi / dt))
+        errs = []
+        for _ in range(steps):
+            engine.step(1, dt, 1e-6, MODE_DIRECT_FP64 | flags)
+            errs.append(abs(engine.diagnostics(1e-6)["e"] - e0) / abs(e0))
+        return max(errs)
+
+    ev = run(0, 0.02)
+    ey = run(FLAG_YOSHIDA4, 0.02)
+    ey2 = run(FLAG_YOSHIDA4, 0.01)
+    assert ey < 0.05 * ev, (ey, ev)
+    assert 8.0 < ey / ey2 < 32.0, (ey, ey2)
 
 
 def test_energy_drift_10k_steps_plummer_1000(engine, oracle):
