@@ -206,6 +206,33 @@ k_direct_targets(int n, State s, double eps2, const int32_t* __restrict__ target
     }
 }
 
+// Largest |a|^2 over the active rows, a2 = ax*ax + ay*ay + az*az rounded as
+// Engine::compute_max_acceleration's CPU loop rounds it (engine/src/sim/
+// engine.cpp:491-501), which also skips NaN.  a2 >= 0, so its bit pattern
+// orders like an unsigned integer and atomicMax on the bits is exact.
+__global__ void k_max_acc2(int n, State s, unsigned long long* __restrict__ out) {
+    unsigned long long m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!s.active[i]) continue;
+        const double a2 = __dadd_rn(__dadd_rn(__dmul_rn(s.ax[i], s.ax[i]), __dmul_rn(s.ay[i], s.ay[i])),
+                                    __dmul_rn(s.az[i], s.az[i]));
+        if (!(a2 > 0.0)) continue;
+        const unsigned long long b = (unsigned long long)__double_as_longlong(a2);
+        m = b > m ? b : m;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xFFFFFFFFu, m, o);
+        m = v > m ? v : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+void max_acc2(cudaStream_t st, int n, const State& s, unsigned long long* out, int sms) {
+    cudaMemsetAsync(out, 0, sizeof(unsigned long long), st);
+    if (n > 0) k_max_acc2<<<std::min(ceil_div(n, 256), sms * 4), 256, 0, st>>>(n, s, out);
+}
+
 // out3[v] = sum over chunks c of part[c][v], in chunk order.
 __global__ void k_direct_targets_reduce(int nv, int chunks, const double* __restrict__ part,
                                         double* __restrict__ out3) {

@@ -12,6 +12,8 @@ void diagnostics(cudaStream_t st, int n, const State& s, double eps, int pe_mode
 // FP64 direct-sum accelerations of rows targets[0 .. nt) into out3 (xyz per
 // target); scratch: direct_targets_scratch_bytes(sms).
 size_t direct_targets_scratch_bytes(int sms);
+// *out = bits of the largest |a|^2 over the active rows (0 when none > 0).
+void max_acc2(cudaStream_t st, int n, const State& s, unsigned long long* out, int sms);
 void direct_targets(cudaStream_t st, int n, const State& s, double eps, int nt,
                     const int32_t* targets, double* out3, double* scratch, int sms);
 

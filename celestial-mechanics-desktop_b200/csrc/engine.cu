@@ -46,6 +46,7 @@ struct Scal {
     int n_kept;
     int n_merges;
     int pad;
+    unsigned long long amax2;  // bits of the largest |a|^2 (adaptive dt)
 };
 
 }  // namespace
@@ -67,6 +68,9 @@ struct nb_engine {
     double mac_budget = -3.0;
     int group_bodies = 32;
     double group_pack = 2.25;
+    // adaptive time step (AdaptiveTimestepConfig defaults)
+    double adapt_eta = 0.01, adapt_dt_min = 1e-8, adapt_dt_max = 0.01;
+    double adapt_dt = 0.0;  // the next adaptive step's dt; 0 = take nb_step's dt
     // learned MAC
     double mac_theta_lo = 0.35, mac_theta_hi = 1.0;
     double mac_screen_q = 0.9;             // residual quantile that sets the screen margin
@@ -542,6 +546,21 @@ NB_API int32_t nb_set_param_f64(nb_engine* h, int32_t p, double v) {
             if (!(v > 0.0)) return fail(h, NB_ERR_INVALID_ARG, "audit rms bound must be > 0");
             h->mac_audit_rms_max = v;
             return NB_OK;
+        case NB_PARAM_ADAPTIVE_ETA:
+            if (!(v > 0.0)) return fail(h, NB_ERR_INVALID_ARG, "eta must be > 0");
+            h->adapt_eta = v;
+            h->adapt_dt = 0.0;
+            return NB_OK;
+        case NB_PARAM_ADAPTIVE_DT_MIN:
+        case NB_PARAM_ADAPTIVE_DT_MAX: {
+            const double lo = p == NB_PARAM_ADAPTIVE_DT_MIN ? v : h->adapt_dt_min;
+            const double hi = p == NB_PARAM_ADAPTIVE_DT_MAX ? v : h->adapt_dt_max;
+            if (!(lo > 0.0 && lo <= hi)) return fail(h, NB_ERR_INVALID_ARG, "need 0 < dt_min <= dt_max");
+            h->adapt_dt_min = lo;
+            h->adapt_dt_max = hi;
+            h->adapt_dt = 0.0;
+            return NB_OK;
+        }
         case NB_PARAM_MAC_SCREEN_QUANTILE:
             if (!(v >= 0.0 && v <= 1.0)) return fail(h, NB_ERR_INVALID_ARG, "screen quantile must be in [0, 1]");
             h->mac_screen_q = v;
@@ -610,6 +629,12 @@ NB_API int32_t nb_get_counters(const nb_engine* h, int64_t* out, int32_t n) {
     return NB_OK;
 }
 
+NB_API int32_t nb_get_adaptive_dt(const nb_engine* h, double* dt) {
+    if (!h || !dt) return NB_ERR_INVALID_ARG;
+    *dt = h->adapt_dt;
+    return NB_OK;
+}
+
 NB_API int32_t nb_compute_forces(nb_engine* h, int32_t n, const double* px, const double* py,
                                  const double* pz, const double* mass, const double* radius,
                                  const uint8_t* active, double softening, int32_t flags,
@@ -672,6 +697,7 @@ NB_API int32_t nb_set_state(nb_engine* h, int32_t n, const double* px, const dou
     if ((r = upload(h, h->s.ids, ids.data(), sizeof(int32_t) * (size_t)n))) return r;
     if ((r = check_device(h))) return r;
     h->has_state = true;
+    h->adapt_dt = 0.0;
     return NB_OK;
 }
 
@@ -765,6 +791,29 @@ int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags)
 
 }  // namespace
 
+namespace {
+
+// AdaptiveTimestep::update after a step (engine/src/sim/adaptive_timestep.cpp:
+// 12-23): a_max = sqrt of the largest |a|^2 over the active rows.
+int adaptive_update(nb_engine* h, double softening) {
+    nb::max_acc2(h->st, h->n, h->s, &h->scal->amax2, h->sms);
+    unsigned long long bits = 0;
+    int r;
+    if ((r = download(h, &bits, &h->scal->amax2, sizeof(bits))) || (r = check_device(h))) return r;
+    double a2;
+    std::memcpy(&a2, &bits, sizeof(a2));
+    const double a_max = std::sqrt(a2);
+    if (a_max <= 0.0 || softening <= 0.0) {
+        h->adapt_dt = h->adapt_dt_max;
+    } else {
+        const double dt_new = h->adapt_eta * std::sqrt(softening / a_max);
+        h->adapt_dt = std::clamp(dt_new, h->adapt_dt_min, h->adapt_dt_max);
+    }
+    return NB_OK;
+}
+
+}  // namespace
+
 NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softening, int32_t flags) {
     if (!h) return NB_ERR_INVALID_ARG;
     if (!h->has_state) return fail(h, NB_ERR_STATE, "nb_step before nb_set_state");
@@ -772,12 +821,16 @@ NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softenin
     cudaSetDevice(h->device);
     const bool learned = (flags & NB_FLAG_LEARNED_MAC) != 0;
     const bool audit = learned && h->mac_audit_every > 0;
+    const bool adaptive = (flags & NB_FLAG_ADAPTIVE_DT) != 0;
     int r, left = n_steps;
     while (left > 0) {
         // after a failed audit the learned MAC falls back to the geometric test
         const int f = (learned && h->mac_fallback) ? (flags & ~NB_FLAG_LEARNED_MAC) : flags;
-        const int k = audit ? std::min(left, h->mac_audit_every - h->mac_since_audit) : left;
-        if ((r = run_steps(h, k, dt, softening, f))) return r;
+        int k = audit ? std::min(left, h->mac_audit_every - h->mac_since_audit) : left;
+        if (adaptive) k = 1;  // dt changes after every step
+        const double dstep = (adaptive && h->adapt_dt > 0.0) ? h->adapt_dt : dt;
+        if ((r = run_steps(h, k, dstep, softening, f))) return r;
+        if (adaptive && (r = adaptive_update(h, softening))) return r;
         left -= k;
         if (!audit) continue;
         h->mac_since_audit += k;

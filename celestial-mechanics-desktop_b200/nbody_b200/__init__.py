@@ -5,7 +5,8 @@ package only binds it.  Importing it loads the library and raises if it is
 missing: there is no CPU fallback.
 """
 from . import _native as native  # noqa: F401  (loads the library)
-from ._native import (FLAG_COLLISIONS, FLAG_LEARNED_MAC, FLAG_NO_QUADRUPOLE, FLAG_YOSHIDA4,  # noqa: F401,E501
+from ._native import (FLAG_ADAPTIVE_DT, FLAG_COLLISIONS, FLAG_LEARNED_MAC,  # noqa: F401
+                      FLAG_NO_QUADRUPOLE, FLAG_YOSHIDA4,
                       FLAG_SHELL_THEOREM, MODE_BARNES_HUT, MODE_BARNES_HUT_REF, MODE_DIRECT,
                       MODE_DIRECT_FP64)
 from .engine import B200PhysicsBackend, B200SoAIntegrator, Engine, NBodyError  # noqa: F401

@@ -36,6 +36,7 @@ FLAG_NO_QUADRUPOLE = 0x20
 FLAG_COLLISIONS = 0x40
 FLAG_LEARNED_MAC = 0x80
 FLAG_YOSHIDA4 = 0x100
+FLAG_ADAPTIVE_DT = 0x200
 # parameters
 PARAM_THETA = 1
 PARAM_LEAF_CAPACITY = 2
@@ -54,6 +55,9 @@ PARAM_ENS_DIRECT_SHAPE = 14
 PARAM_MAC_AUDIT_INTERVAL = 15
 PARAM_MAC_AUDIT_SAMPLES = 16
 PARAM_MAC_AUDIT_RMS = 17
+PARAM_ADAPTIVE_ETA = 18
+PARAM_ADAPTIVE_DT_MIN = 19
+PARAM_ADAPTIVE_DT_MAX = 20
 ENS_SHAPES = [(64, 1), (64, 2), (64, 4), (128, 1), (128, 2), (128, 4), (256, 1), (256, 2), (256, 4)]
 # timings / counters
 T_BUILD, T_TRAVERSAL, T_TOTAL, T_SORT, T_TREE, T_COUNT = range(6)
@@ -74,6 +78,7 @@ _SIGS = {
     "nb_set_param_i32": (i32, [vp, i32, i32]),
     "nb_get_timings": (i32, [vp, P, i32]),
     "nb_get_counters": (i32, [vp, P, i32]),
+    "nb_get_adaptive_dt": (i32, [vp, P]),
     "nb_stream": (vp, [vp]),
     "nb_version": (C.c_char_p, []),
     "nb_compute_forces": (i32, [vp, i32, P, P, P, P, P, P, f64, i32, P, P, P]),

@@ -81,6 +81,12 @@ class Engine:
         self._check(N.lib.nb_get_counters(self._h, N.ptr(out), N.C_COUNT))
         return out
 
+    def adaptive_dt(self) -> float:
+        """dt of the next FLAG_ADAPTIVE_DT step (0 before the first)."""
+        out = np.zeros(1)
+        self._check(N.lib.nb_get_adaptive_dt(self._h, N.ptr(out)))
+        return float(out[0])
+
     # -- the seam -----------------------------------------------------------
     def compute_forces(self, px, py, pz, mass, active, softening: float, flags: int,
                        radius=None, out=None):

@@ -70,6 +70,15 @@ enum nb_mode {
  * Engine::cpu_yoshida_substep, engine/src/sim/engine.cpp:685-746), three
  * force evaluations per step. */
 #define NB_FLAG_YOSHIDA4 0x100
+/* nb_step: adaptive time step (AdaptiveTimestep::compute_dt, engine/src/sim/
+ * adaptive_timestep.cpp:12-17, applied after every step as Engine::step does,
+ * engine/src/sim/engine.cpp:268-272): after each step dt becomes
+ * clamp(eta sqrt(softening / a_max), dt_min, dt_max), a_max the largest |a|
+ * over active bodies (dt_max when a_max or softening is 0).  The first step
+ * after nb_set_state or a NB_PARAM_ADAPTIVE_* change uses nb_step's dt; the
+ * current dt is read with nb_get_adaptive_dt.  Steps run one by one (no
+ * captured graph: dt changes every step). */
+#define NB_FLAG_ADAPTIVE_DT 0x200
 
 /* Parameter ids for nb_set_param_f64 / nb_set_param_i32. */
 enum nb_param {
@@ -102,9 +111,14 @@ enum nb_param {
                                       sampled bodies; 0 = never (default).  Setting it also
                                       clears a fallback                                        */
     NB_PARAM_MAC_AUDIT_SAMPLES = 16, /* i32, bodies per audit (default 1024)                   */
-    NB_PARAM_MAC_AUDIT_RMS = 17    /* f64, an audit whose rms relative error exceeds this
+    NB_PARAM_MAC_AUDIT_RMS = 17,   /* f64, an audit whose rms relative error exceeds this
                                       switches the handle to the geometric MAC at
                                       NB_PARAM_THETA (default 1e-3)                           */
+    /* NB_FLAG_ADAPTIVE_DT (AdaptiveTimestepConfig, engine/include/celestial/sim/
+     * simulation_config.hpp:73-79); setting one restarts from nb_step's dt */
+    NB_PARAM_ADAPTIVE_ETA = 18,    /* f64, safety factor eta (default 0.01)                  */
+    NB_PARAM_ADAPTIVE_DT_MIN = 19, /* f64, floor (default 1e-8)                               */
+    NB_PARAM_ADAPTIVE_DT_MAX = 20  /* f64, ceiling (default 0.01)                             */
 };
 
 /* Indices into nb_get_timings() output (milliseconds, CUDA events).
@@ -150,6 +164,10 @@ NB_API int32_t nb_set_param_f64(nb_engine* h, int32_t param, double value);
 NB_API int32_t nb_set_param_i32(nb_engine* h, int32_t param, int32_t value);
 NB_API int32_t nb_get_timings(const nb_engine* h, double* out, int32_t n);
 NB_API int32_t nb_get_counters(const nb_engine* h, int64_t* out, int32_t n);
+/* The time step the next NB_FLAG_ADAPTIVE_DT step will take (0 before the
+ * first adaptive step; AdaptiveTimestep::current_dt,
+ * engine/include/celestial/sim/adaptive_timestep.hpp:26). */
+NB_API int32_t nb_get_adaptive_dt(const nb_engine* h, double* dt);
 /* cudaStream_t of the handle, for callers that time with CUDA events. */
 NB_API void* nb_stream(nb_engine* h);
 NB_API const char* nb_version(void);

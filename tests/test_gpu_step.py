@@ -6,8 +6,8 @@ import numpy as np
 import pytest
 
 from conftest import bodies_dict
-from nbody_b200 import (FLAG_COLLISIONS, FLAG_SHELL_THEOREM, FLAG_YOSHIDA4, MODE_BARNES_HUT,
-                        MODE_DIRECT_FP64, NBodyError, scenarios)
+from nbody_b200 import (FLAG_ADAPTIVE_DT, FLAG_COLLISIONS, FLAG_SHELL_THEOREM, FLAG_YOSHIDA4,
+                        MODE_BARNES_HUT, MODE_DIRECT_FP64, NBodyError, scenarios)
 from nbody_b200.scenarios import Bodies
 from nbody_b200 import _native as N
 
@@ -81,6 +81,56 @@ def test_yoshida4_energy_error_is_fourth_order(engine):
     ey2 = run(FLAG_YOSHIDA4, 0.01)
     assert ey < 0.05 * ev, (ey, ev)
     assert 8.0 < ey / ey2 < 32.0, (ey, ey2)
+
+
+def _adaptive_dt_rule(st, active, eps, eta, lo, hi):
+    """AdaptiveTimestep::compute_dt after a step: a_max over the active rows
+    (NaN and zero rows skipped, as the reference's max loop skips them)."""
+    a2 = st["ax"] * st["ax"] + st["ay"] * st["ay"] + st["az"] * st["az"]
+    a2 = a2[active.astype(bool) & (a2 > 0)]
+    amax = float(np.sqrt(a2.max())) if a2.size else 0.0
+    if amax <= 0.0 or eps <= 0.0:
+        return hi
+    return min(max(eta * float(np.sqrt(eps / amax)), lo), hi)
+
+
+def test_adaptive_dt_fp64_trajectory_bit_exact(engine, oracle):
+    """FLAG_ADAPTIVE_DT: after every step dt becomes clamp(eta sqrt(eps /
+    a_max), dt_min, dt_max); the dt sequence and the trajectory equal the
+    oracle's Verlet steps under the same rule, bit for bit, whether the steps
+    come one call at a time or in one call."""
+    eps, eta, lo, hi = 1e-4, 0.02, 1e-6, 1e-3
+    b = scenarios.plummer(300, seed=3)
+    b.active[::13] = 0
+    want, dt, dts = bodies_dict(b), 1e-4, []
+    for _ in range(15):
+        want = dict(oracle.verlet_direct(want | {"active": b.active}, eps, dt, 1), active=b.active)
+        dt = _adaptive_dt_rule(want, b.active, eps, eta, lo, hi)
+        dts.append(dt)
+    assert len(set(dts)) > 1  # the rule moves dt
+    engine.set_param(N.PARAM_ADAPTIVE_ETA, eta)
+    engine.set_param(N.PARAM_ADAPTIVE_DT_MIN, lo)
+    engine.set_param(N.PARAM_ADAPTIVE_DT_MAX, hi)
+    try:
+        for one_call in (False, True):
+            engine.set_state(b)
+            assert engine.adaptive_dt() == 0.0
+            if one_call:
+                engine.step(15, 1e-4, eps, MODE_DIRECT_FP64 | FLAG_ADAPTIVE_DT)
+                assert engine.adaptive_dt() == dts[-1]
+            else:
+                got = []
+                for _ in range(15):
+                    engine.step(1, 1e-4, eps, MODE_DIRECT_FP64 | FLAG_ADAPTIVE_DT)
+                    got.append(engine.adaptive_dt())
+                assert got == dts
+            st, _ = engine.get_state()
+            for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az"):
+                np.testing.assert_array_equal(getattr(st, k), want[k], err_msg=(k, one_call))
+    finally:
+        engine.set_param(N.PARAM_ADAPTIVE_ETA, 0.01)
+        engine.set_param(N.PARAM_ADAPTIVE_DT_MIN, 1e-8)
+        engine.set_param(N.PARAM_ADAPTIVE_DT_MAX, 0.01)
 
 
 def test_energy_drift_10k_steps_plummer_1000(engine, oracle):
