@@ -15,7 +15,7 @@ CSRC = HERE / "csrc"
 LIB = HERE / "libnbody_b200.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = ["engine.cu", "bodies.cu", "sort.cu", "tree.cu", "walk.cu", "direct.cu", "diag.cu",
-           "collide.cu", "noalloc.cu", "mac.cu", "ensemble.cu"]
+           "collide.cu", "noalloc.cu", "mac.cu", "ensemble.cu", "celestial_compat.cu"]
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "--extended-lambda", "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared",
          "-cudart", "shared"]
@@ -25,7 +25,8 @@ def needs_build() -> bool:
     if not LIB.exists():
         return True
     t = LIB.stat().st_mtime
-    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "nbody_b200.h"]
+    deps = (list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) +
+            list((HERE.parent / "include").glob("*.h")))
     return any(p.stat().st_mtime > t for p in deps)
 
 

@@ -635,6 +635,13 @@ NB_API int32_t nb_get_adaptive_dt(const nb_engine* h, double* dt) {
     return NB_OK;
 }
 
+NB_API int32_t nb_get_body_count(const nb_engine* h, int32_t* n, int32_t* n_active) {
+    if (!h || !n || !n_active) return NB_ERR_INVALID_ARG;
+    *n = h->n;
+    *n_active = h->n_active;
+    return NB_OK;
+}
+
 NB_API int32_t nb_compute_forces(nb_engine* h, int32_t n, const double* px, const double* py,
                                  const double* pz, const double* mass, const double* radius,
                                  const uint8_t* active, double softening, int32_t flags,
@@ -848,6 +855,20 @@ NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softenin
     }
     h->counters[NB_C_MAC_AUDITS] = h->mac_audits;
     h->counters[NB_C_MAC_FALLBACK] = h->mac_fallback ? 1 : 0;
+    return NB_OK;
+}
+
+NB_API int32_t nb_max_acceleration(nb_engine* h, double* a_max) {
+    if (!h || !a_max) return NB_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NB_ERR_STATE, "no device-resident state");
+    cudaSetDevice(h->device);
+    nb::max_acc2(h->st, h->n, h->s, &h->scal->amax2, h->sms);
+    unsigned long long bits = 0;
+    int r;
+    if ((r = download(h, &bits, &h->scal->amax2, sizeof(bits))) || (r = check_device(h))) return r;
+    double a2;
+    std::memcpy(&a2, &bits, sizeof(a2));
+    *a_max = std::sqrt(a2);
     return NB_OK;
 }
 

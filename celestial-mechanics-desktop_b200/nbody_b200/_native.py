@@ -79,6 +79,8 @@ _SIGS = {
     "nb_get_timings": (i32, [vp, P, i32]),
     "nb_get_counters": (i32, [vp, P, i32]),
     "nb_get_adaptive_dt": (i32, [vp, P]),
+    "nb_max_acceleration": (i32, [vp, P]),
+    "nb_get_body_count": (i32, [vp, P, P]),
     "nb_stream": (vp, [vp]),
     "nb_version": (C.c_char_p, []),
     "nb_compute_forces": (i32, [vp, i32, P, P, P, P, P, P, f64, i32, P, P, P]),

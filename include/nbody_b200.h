@@ -168,6 +168,12 @@ NB_API int32_t nb_get_counters(const nb_engine* h, int64_t* out, int32_t n);
  * first adaptive step; AdaptiveTimestep::current_dt,
  * engine/include/celestial/sim/adaptive_timestep.hpp:26). */
 NB_API int32_t nb_get_adaptive_dt(const nb_engine* h, double* dt);
+/* Largest |a| over the active bodies of the device state
+ * (Engine::compute_max_acceleration, engine/src/sim/engine.cpp:468-501). */
+NB_API int32_t nb_max_acceleration(nb_engine* h, double* a_max);
+/* Rows of the device state and how many are active (ParticleSystem::count
+ * and the active count, engine/src/interop/native_api.cpp:217-220,393-396). */
+NB_API int32_t nb_get_body_count(const nb_engine* h, int32_t* n, int32_t* n_active);
 /* cudaStream_t of the handle, for callers that time with CUDA events. */
 NB_API void* nb_stream(nb_engine* h);
 NB_API const char* nb_version(void);
