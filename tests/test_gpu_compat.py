@@ -25,6 +25,12 @@ def lib():
 
     lib = A.bind(N.lib)
     assert lib.celestial_init(512) == 0, lib.celestial_get_last_error_message()
+    # settings outlive shutdown/init, as the reference's global config does:
+    # start every test from the defaults
+    lib.celestial_set_integrator(0)
+    lib.celestial_set_compute_mode(2)
+    lib.celestial_set_collision_mode(0)
+    lib.celestial_set_adaptive_timestep(0, 0.01, 1e-8, 0.01, 0.001)
     yield lib
     lib.celestial_shutdown()
 
