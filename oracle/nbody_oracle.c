@@ -550,6 +550,44 @@ void or_verlet_direct(int32_t n, double* px, double* py, double* pz, double* vx,
     free(nx);
 }
 
+/* Engine::step_yoshida4_cpu_brute_force (engine/src/sim/engine.cpp:1057-1066):
+ * per step, three Engine::cpu_yoshida_substep calls (engine.cpp:685-746:
+ * half kick with the previous acceleration, drift, forces, half kick,
+ * rotate) with sub_dt = SUB_DT[s] * dt, SUB_DT = {w1, w0, w1} of
+ * YoshidaCoefficients (engine/include/celestial/sim/yoshida.hpp:19-24);
+ * each sub-step is the Verlet step above, with the direct sum as forces. */
+void or_yoshida_direct(int32_t n, double* px, double* py, double* pz, double* vx, double* vy,
+                       double* vz, double* ax, double* ay, double* az, const double* m,
+                       const uint8_t* active, double eps, double dt, int32_t steps,
+                       int32_t threads) {
+    const double cbrt2 = 1.2599210498948732;
+    const double w1 = 1.0 / (2.0 - cbrt2);
+    const double w0 = -cbrt2 / (2.0 - cbrt2);
+    const double sub[3] = {w1, w0, w1};
+    for (int32_t s = 0; s < steps; s++)
+        for (int k = 0; k < 3; k++)
+            or_verlet_direct(n, px, py, pz, vx, vy, vz, ax, ay, az, m, active, eps, sub[k] * dt, 1,
+                             threads);
+}
+
+/* AdaptiveTimestep::compute_dt (engine/src/sim/adaptive_timestep.cpp:12-17)
+ * from Engine::compute_max_acceleration's CPU loop (engine/src/sim/
+ * engine.cpp:491-501): the next dt after a step. */
+double or_adaptive_dt(int32_t n, const double* ax, const double* ay, const double* az,
+                      const uint8_t* active, double eps, double eta, double dt_min,
+                      double dt_max) {
+    double max_a2 = 0.0;
+    for (int32_t i = 0; i < n; i++) {
+        if (!active[i]) continue;
+        const double a2 = ax[i] * ax[i] + ay[i] * ay[i] + az[i] * az[i];
+        if (a2 > max_a2) max_a2 = a2;
+    }
+    const double a_max = sqrt(max_a2);
+    if (a_max <= 0.0 || eps <= 0.0) return dt_max;
+    const double v = eta * sqrt(eps / a_max);
+    return v < dt_min ? dt_min : (v > dt_max ? dt_max : v);
+}
+
 /* EnergyCalculator.ComputeKE/ComputePE/ComputeMomentum/ComputeAngularMomentum
  * (EnergyCalculator.cs:16-78); pair PE of NewtonianGravity.cs:68-77. */
 void or_energy(int32_t n, const double* px, const double* py, const double* pz,

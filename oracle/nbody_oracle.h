@@ -80,6 +80,16 @@ void or_verlet_direct(int32_t n, double* px, double* py, double* pz, double* vx,
                       double* vz, double* ax, double* ay, double* az, const double* m,
                       const uint8_t* active, double eps, double dt, int32_t steps,
                       int32_t threads);
+/* Yoshida4 steps: three Verlet sub-steps of w1 dt, w0 dt, w1 dt
+ * (engine/src/sim/engine.cpp:685-746,1057-1066; yoshida.hpp:19-24). */
+void or_yoshida_direct(int32_t n, double* px, double* py, double* pz, double* vx, double* vy,
+                       double* vz, double* ax, double* ay, double* az, const double* m,
+                       const uint8_t* active, double eps, double dt, int32_t steps,
+                       int32_t threads);
+/* The adaptive dt after a step (adaptive_timestep.cpp:12-17, engine.cpp:491-501). */
+double or_adaptive_dt(int32_t n, const double* ax, const double* ay, const double* az,
+                      const uint8_t* active, double eps, double eta, double dt_min,
+                      double dt_max);
 /* KE, PE, E, P[3], L[3], COM[3], M (EnergyCalculator.cs:16-78,
  * NewtonianGravity.cs:68-77). */
 void or_energy(int32_t n, const double* px, const double* py, const double* pz,

@@ -58,6 +58,8 @@ _OR_SIGS = {
     "or_resolve_merges": (i32, [i32, P, P, P, P, P, P, P, P, P, P, i32, P, P, i32, i32, i32, f64]),
     "or_verlet_direct": (None, [i32, P, P, P, P, P, P, P, P, P, P, P, f64, f64, i32, i32]),
     "or_energy": (None, [i32, P, P, P, P, P, P, P, P, f64, P, i32]),
+    "or_yoshida_direct": (None, [i32, P, P, P, P, P, P, P, P, P, P, P, f64, f64, i32, i32]),
+    "or_adaptive_dt": (f64, [i32, P, P, P, P, f64, f64, f64, f64]),
     "or_force_error": (i32, [i32, P, P, P, P, P, P, P, P]),
 }
 _REF_SIGS = {
@@ -267,6 +269,22 @@ def verlet_direct(b: dict, eps, dt, steps, nthreads=None):
                                                            "ax", "ay", "az", "mass")), _p(act),
                            eps, dt, steps, nthreads or threads())
     return a
+
+
+def yoshida_direct(b: dict, eps, dt, steps, nthreads=None):
+    a = {k: _f(b[k]).copy() for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az", "mass")}
+    act = _u8(b["active"])
+    lib().or_yoshida_direct(len(act), *(_p(a[k]) for k in ("px", "py", "pz", "vx", "vy", "vz",
+                                                            "ax", "ay", "az", "mass")), _p(act),
+                            eps, dt, steps, nthreads or threads())
+    return a
+
+
+def adaptive_dt(b: dict, eps, eta, dt_min, dt_max):
+    ax, ay, az = (_f(b[k]) for k in ("ax", "ay", "az"))
+    act = _u8(b["active"])  # held: the library reads it during the call
+    return lib().or_adaptive_dt(len(ax), _p(ax), _p(ay), _p(az), _p(act), eps, eta, dt_min,
+                                dt_max)
 
 
 def energy(b: dict, eps, nthreads=None):

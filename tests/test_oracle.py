@@ -229,6 +229,32 @@ def test_yoshida4_composition_is_fourth_order(oracle):
     assert 3.0 < v1 / v2 < 5.0 and 8.0 < y1 / y2 < 32.0, (v1 / v2, y1 / y2)
 
 
+def test_yoshida_and_adaptive_restatements(oracle):
+    """or_yoshida_direct (Engine::cpu_yoshida_substep x 3) equals three
+    chained Verlet sub-steps bit for bit, and or_adaptive_dt applies the
+    AdaptiveTimestep rule to the largest active |a| (clamped both ways)."""
+    b = scenarios.plummer(120, seed=4)
+    b.active[::9] = 0
+    d = {k: v for k, v in b.__dict__.items()}
+    w1 = 1.0 / (2.0 - 1.2599210498948732)
+    w0 = -1.2599210498948732 / (2.0 - 1.2599210498948732)
+    want = d
+    for _ in range(4):
+        for w in (w1, w0, w1):
+            want = dict(oracle.verlet_direct(want, 1e-4, w * 1e-3, 1), active=b.active)
+    got = oracle.yoshida_direct(d, 1e-4, 1e-3, 4)
+    for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az"):
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+    s = dict(got, active=b.active)
+    act = b.active.astype(bool)
+    a2 = s["ax"] * s["ax"] + s["ay"] * s["ay"] + s["az"] * s["az"]
+    amax = np.sqrt(a2[act].max())
+    assert oracle.adaptive_dt(s, 1e-4, 0.02, 1e-9, 1.0) == 0.02 * np.sqrt(1e-4 / amax)
+    assert oracle.adaptive_dt(s, 1e-4, 0.02, 1e-9, 1e-7) == 1e-7     # ceiling
+    assert oracle.adaptive_dt(s, 1e-4, 0.02, 1.0, 2.0) == 1.0        # floor
+    assert oracle.adaptive_dt(s, 0.0, 0.02, 1e-9, 3e-3) == 3e-3      # no softening: dt_max
+
+
 def test_stable_sort_semantics(oracle):
     rng = np.random.Generator(np.random.PCG64(1))
     keys = rng.integers(0, 50, 20000).astype(np.uint64) << np.uint64(40)
