@@ -20,7 +20,11 @@
  *     are refused (the last error says so) and leave the mode unchanged;
  *   - functions outside this subset (post-Newtonian terms, softening modes,
  *     GPU validation, telemetry, snapshots, JSON config, deterministic mode
- *     switches) are not provided. */
+ *     switches) are not provided.
+ * Like the reference's, these functions share one global engine and are not
+ * safe to call from several threads at once; settings made through them
+ * (mode, integrator, adaptive dt, collisions) outlive shutdown and apply to
+ * the next init, as the reference's global configuration does. */
 #ifndef CELESTIAL_COMPAT_H
 #define CELESTIAL_COMPAT_H
 
