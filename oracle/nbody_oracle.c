@@ -107,6 +107,130 @@ void or_direct_forces_targets(int32_t n, const double* px, const double* py, con
     }
 }
 
+/* SimdSingleThreadBackend.ComputeForces (SimdSingleThreadBackend.cs:43-165):
+ * sources in chunks of Vector<double>.Count lanes (4: 256-bit vectors), per
+ * lane dist2 = ((dx*dx + dy*dy) + dz*dz) + eps2, invDist = 1 / sqrt(dist2),
+ * invDist3 = (invDist*invDist)*invDist, factor = m_j * invDist3 (not the
+ * ((m*inv)*inv)*inv of GravityKernel); the lanes are then subtracted from
+ * the scalar sums in lane order (self and inactive lanes skipped), the tail
+ * runs the same arithmetic in scalar code.  The lane width therefore does
+ * not change a single bit.  The same arithmetic and order are the native
+ * engine's CPU brute force (Engine::compute_cpu_brute_forces, global
+ * softening, engine/src/sim/engine.cpp:649-674).  With the shell theorem the
+ * backend runs CpuSingleThreadBackend's shell loop, whose arithmetic is
+ * CpuParallelBackend's. */
+#define OR_SIMD_LANES 4
+void or_direct_forces_simd(int32_t n, const double* px, const double* py, const double* pz,
+                           const double* m, const double* radius, const uint8_t* active,
+                           double eps, int32_t shell, double* ax, double* ay, double* az,
+                           int32_t threads) {
+    if (shell) {
+        or_direct_forces(n, px, py, pz, m, radius, active, eps, 1, ax, ay, az, threads);
+        return;
+    }
+    const double eps2 = eps * eps;
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int32_t i = 0; i < n; i++) {
+        ax[i] = ay[i] = az[i] = 0.0;
+        if (!active[i]) continue;
+        const double xi = px[i], yi = py[i], zi = pz[i];
+        double axi = 0.0, ayi = 0.0, azi = 0.0;
+        int32_t j = 0;
+        const int32_t vec_limit = n - (n % OR_SIMD_LANES);
+        for (; j < vec_limit; j += OR_SIMD_LANES) {
+            double fx[OR_SIMD_LANES], fdx[OR_SIMD_LANES], fdy[OR_SIMD_LANES], fdz[OR_SIMD_LANES];
+            for (int k = 0; k < OR_SIMD_LANES; k++) {
+                const double dx = xi - px[j + k], dy = yi - py[j + k], dz = zi - pz[j + k];
+                const double dist2 = dx * dx + dy * dy + dz * dz + eps2;
+                const double inv = 1.0 / sqrt(dist2);
+                const double inv3 = inv * inv * inv;
+                fx[k] = m[j + k] * inv3;
+                fdx[k] = dx;
+                fdy[k] = dy;
+                fdz[k] = dz;
+            }
+            for (int k = 0; k < OR_SIMD_LANES; k++) {
+                const int32_t jk = j + k;
+                if (jk == i || !active[jk]) continue;
+                axi -= fx[k] * fdx[k];
+                ayi -= fx[k] * fdy[k];
+                azi -= fx[k] * fdz[k];
+            }
+        }
+        for (; j < n; j++) {
+            if (j == i || !active[j]) continue;
+            const double dx = xi - px[j], dy = yi - py[j], dz = zi - pz[j];
+            const double dist2 = dx * dx + dy * dy + dz * dz + eps2;
+            const double inv = 1.0 / sqrt(dist2);
+            const double inv3 = inv * inv * inv;
+            const double f = m[j] * inv3;
+            axi -= f * dx;
+            ayi -= f * dy;
+            azi -= f * dz;
+        }
+        ax[i] = axi;
+        ay[i] = ayi;
+        az[i] = azi;
+    }
+}
+
+/* CpuSingleThreadBackend.ComputeForces (CpuSingleThreadBackend.cs:50-159).
+ * Without the shell theorem: the O(n^2/2) Newton's-third-law loop - for
+ * each active i and each active j > i one factor pair m_j*invDist3,
+ * m_i*invDist3 (invDist3 = (inv*inv)*inv); i's sum over j > i is kept in a
+ * register and added to ax[i] at the end of row i, while j receives
+ * +m_i*invDist3*dx directly in ax[j] during earlier rows.  So a body's
+ * acceleration is (sum over lower partners, in order) + (sum over higher
+ * partners, in order): a different summation order from CpuParallel's single
+ * running sum.  With the shell theorem: the CpuParallel loop. Serial. */
+void or_direct_forces_pairwise(int32_t n, const double* px, const double* py, const double* pz,
+                               const double* m, const double* radius, const uint8_t* active,
+                               double eps, int32_t shell, double* ax, double* ay, double* az) {
+    if (shell) {
+        or_direct_forces(n, px, py, pz, m, radius, active, eps, 1, ax, ay, az, 1);
+        return;
+    }
+    const double eps2 = eps * eps;
+    for (int32_t i = 0; i < n; i++) ax[i] = ay[i] = az[i] = 0.0;
+    for (int32_t i = 0; i < n; i++) {
+        if (!active[i]) continue;
+        const double xi = px[i], yi = py[i], zi = pz[i], mi = m[i];
+        double axi = 0.0, ayi = 0.0, azi = 0.0;
+        for (int32_t j = i + 1; j < n; j++) {
+            if (!active[j]) continue;
+            const double dx = xi - px[j], dy = yi - py[j], dz = zi - pz[j];
+            const double dist2 = dx * dx + dy * dy + dz * dz + eps2;
+            const double inv = 1.0 / sqrt(dist2);
+            const double inv3 = inv * inv * inv;
+            const double f_ij = m[j] * inv3, f_ji = mi * inv3;
+            axi -= f_ij * dx;
+            ayi -= f_ij * dy;
+            azi -= f_ij * dz;
+            ax[j] += f_ji * dx;
+            ay[j] += f_ji * dy;
+            az[j] += f_ji * dz;
+        }
+        ax[i] += axi;
+        ay[i] += ayi;
+        az[i] += azi;
+    }
+}
+
+/* One of the three direct-sum orders: 0 CpuParallelBackend, 1 the SIMD
+ * backend / native engine, 2 CpuSingleThreadBackend. */
+void or_direct_forces_order(int32_t n, const double* px, const double* py, const double* pz,
+                            const double* m, const double* radius, const uint8_t* active,
+                            double eps, int32_t shell, int32_t order, double* ax, double* ay,
+                            double* az, int32_t threads) {
+    if (order == 1)
+        or_direct_forces_simd(n, px, py, pz, m, radius, active, eps, shell, ax, ay, az, threads);
+    else if (order == 2)
+        or_direct_forces_pairwise(n, px, py, pz, m, radius, active, eps, shell, ax, ay, az);
+    else
+        or_direct_forces(n, px, py, pz, m, radius, active, eps, shell, ax, ay, az, threads);
+}
+
 /* Bounding box over active bodies (BarnesHutBackend.cs:150-170). */
 void or_bbox(int32_t n, const double* px, const double* py, const double* pz,
              const uint8_t* active, double* out6) {
@@ -451,6 +575,53 @@ int32_t or_broad_phase(int32_t n, const double* px, const double* py, const doub
     return cnt;
 }
 
+/* The same pair list as or_broad_phase (the all-pairs test of
+ * collision_kernel.cu:40-52, pairs in (lo, hi) lexicographic order), with the
+ * rows split over OpenMP threads: a counting pass, an exclusive scan of the
+ * row counts, then a filling pass.  For config-size inputs. */
+int32_t or_broad_phase_parallel(int32_t n, const double* px, const double* py, const double* pz,
+                                const double* radius, const uint8_t* active,
+                                const uint8_t* collidable, int32_t max_pairs, int32_t* lo,
+                                int32_t* hi, int32_t threads) {
+    int64_t* start = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int32_t i = 0; i < n; i++) {
+        if (!active[i] || (collidable && !collidable[i])) continue;
+        int64_t c = 0;
+        for (int32_t j = i + 1; j < n; j++) {
+            if (!active[j] || (collidable && !collidable[j])) continue;
+            double dx = px[i] - px[j], dy = py[i] - py[j], dz = pz[i] - pz[j];
+            double d2 = dx * dx + dy * dy + dz * dz;
+            double sr = radius[i] + radius[j];
+            if (d2 < sr * sr) c++;
+        }
+        start[i + 1] = c;
+    }
+    for (int32_t i = 0; i < n; i++) start[i + 1] += start[i];
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int32_t i = 0; i < n; i++) {
+        int64_t k = start[i];
+        if (k == start[i + 1]) continue;
+        for (int32_t j = i + 1; j < n; j++) {
+            if (!active[j] || (collidable && !collidable[j])) continue;
+            double dx = px[i] - px[j], dy = py[i] - py[j], dz = pz[i] - pz[j];
+            double d2 = dx * dx + dy * dy + dz * dz;
+            double sr = radius[i] + radius[j];
+            if (d2 < sr * sr) {
+                if (k < max_pairs) {
+                    lo[k] = i;
+                    hi[k] = j;
+                }
+                k++;
+            }
+        }
+    }
+    const int64_t total = start[n];
+    free(start);
+    return total > 2147483647 ? 2147483647 : (int32_t)total;
+}
+
 /* DensityModel (density_model.cpp:10-22). */
 static double dm_density(double mass, double radius, double min_radius) {
     double r = (radius > min_radius) ? radius : min_radius;
@@ -513,12 +684,15 @@ int32_t or_resolve_merges(int32_t n, double* px, double* py, double* pz, double*
     return total;
 }
 
-/* SoAVerletIntegrator.Step (SoAVerletIntegrator.cs:48-116) with the
- * CpuParallelBackend direct sum as the backend. */
-void or_verlet_direct(int32_t n, double* px, double* py, double* pz, double* vx, double* vy,
-                      double* vz, double* ax, double* ay, double* az, const double* m,
-                      const uint8_t* active, double eps, double dt, int32_t steps,
-                      int32_t threads) {
+/* SoAVerletIntegrator.Step (SoAVerletIntegrator.cs:48-116) with a direct
+ * sum of the given order (or_direct_forces_order) as the backend.  With
+ * order 1 this is also the native engine's CPU brute-force Leapfrog step
+ * (Engine::step_cpu_brute_force, engine/src/sim/engine.cpp:753-800: half
+ * kick with the previous acceleration, drift, forces, half kick, rotate). */
+void or_verlet_direct_order(int32_t n, double* px, double* py, double* pz, double* vx,
+                            double* vy, double* vz, double* ax, double* ay, double* az,
+                            const double* m, const uint8_t* active, double eps, double dt,
+                            int32_t steps, int32_t order, int32_t threads) {
     double half = 0.5 * dt;
     double* nx = (double*)malloc(sizeof(double) * (size_t)n * 3);
     double* ny = nx + n;
@@ -536,7 +710,8 @@ void or_verlet_direct(int32_t n, double* px, double* py, double* pz, double* vx,
             py[i] += dt * vy[i];
             pz[i] += dt * vz[i];
         }
-        or_direct_forces(n, px, py, pz, m, NULL, active, eps, 0, nx, ny, nz, threads);
+        or_direct_forces_order(n, px, py, pz, m, NULL, active, eps, 0, order, nx, ny, nz,
+                               threads);
         for (int32_t i = 0; i < n; i++) {
             if (!active[i]) continue;
             vx[i] += half * nx[i];
@@ -550,24 +725,41 @@ void or_verlet_direct(int32_t n, double* px, double* py, double* pz, double* vx,
     free(nx);
 }
 
+/* SoAVerletIntegrator.Step with the CpuParallelBackend direct sum. */
+void or_verlet_direct(int32_t n, double* px, double* py, double* pz, double* vx, double* vy,
+                      double* vz, double* ax, double* ay, double* az, const double* m,
+                      const uint8_t* active, double eps, double dt, int32_t steps,
+                      int32_t threads) {
+    or_verlet_direct_order(n, px, py, pz, vx, vy, vz, ax, ay, az, m, active, eps, dt, steps, 0,
+                           threads);
+}
+
 /* Engine::step_yoshida4_cpu_brute_force (engine/src/sim/engine.cpp:1057-1066):
  * per step, three Engine::cpu_yoshida_substep calls (engine.cpp:685-746:
  * half kick with the previous acceleration, drift, forces, half kick,
  * rotate) with sub_dt = SUB_DT[s] * dt, SUB_DT = {w1, w0, w1} of
  * YoshidaCoefficients (engine/include/celestial/sim/yoshida.hpp:19-24);
  * each sub-step is the Verlet step above, with the direct sum as forces. */
-void or_yoshida_direct(int32_t n, double* px, double* py, double* pz, double* vx, double* vy,
-                       double* vz, double* ax, double* ay, double* az, const double* m,
-                       const uint8_t* active, double eps, double dt, int32_t steps,
-                       int32_t threads) {
+void or_yoshida_direct_order(int32_t n, double* px, double* py, double* pz, double* vx,
+                             double* vy, double* vz, double* ax, double* ay, double* az,
+                             const double* m, const uint8_t* active, double eps, double dt,
+                             int32_t steps, int32_t order, int32_t threads) {
     const double cbrt2 = 1.2599210498948732;
     const double w1 = 1.0 / (2.0 - cbrt2);
     const double w0 = -cbrt2 / (2.0 - cbrt2);
     const double sub[3] = {w1, w0, w1};
     for (int32_t s = 0; s < steps; s++)
         for (int k = 0; k < 3; k++)
-            or_verlet_direct(n, px, py, pz, vx, vy, vz, ax, ay, az, m, active, eps, sub[k] * dt, 1,
-                             threads);
+            or_verlet_direct_order(n, px, py, pz, vx, vy, vz, ax, ay, az, m, active, eps,
+                                   sub[k] * dt, 1, order, threads);
+}
+
+void or_yoshida_direct(int32_t n, double* px, double* py, double* pz, double* vx, double* vy,
+                       double* vz, double* ax, double* ay, double* az, const double* m,
+                       const uint8_t* active, double eps, double dt, int32_t steps,
+                       int32_t threads) {
+    or_yoshida_direct_order(n, px, py, pz, vx, vy, vz, ax, ay, az, m, active, eps, dt, steps, 0,
+                            threads);
 }
 
 /* AdaptiveTimestep::compute_dt (engine/src/sim/adaptive_timestep.cpp:12-17)
@@ -624,6 +816,52 @@ void or_energy(int32_t n, const double* px, const double* py, const double* pz,
     double pe = 0.0;
     for (int32_t i = 0; i < n; i++) pe += row[i];
     free(row);
+    o[0] = ke; o[1] = pe; o[2] = ke + pe;
+    o[3] = P[0]; o[4] = P[1]; o[5] = P[2];
+    o[6] = L[0]; o[7] = L[1]; o[8] = L[2];
+    o[9] = M > 0 ? C[0] / M : 0; o[10] = M > 0 ? C[1] / M : 0; o[11] = M > 0 ? C[2] / M : 0;
+    o[12] = M;
+}
+
+/* The native engine's EnergyTracker::compute (engine/src/profile/
+ * energy_tracker.cpp:8-90): one pass over the active bodies for KE
+ * (0.5*m*v2), momentum m*v, angular momentum m*(r x v), total mass and the
+ * mass-weighted position sums, then the pair potential -m_i*m_j/sqrt(r2+eps2)
+ * subtracted from one running total in (i, j > i) order.  out13 as
+ * or_energy's. */
+void or_energy_tracker(int32_t n, const double* px, const double* py, const double* pz,
+                       const double* vx, const double* vy, const double* vz, const double* m,
+                       const uint8_t* active, double eps, double* o) {
+    const double eps2 = eps * eps;
+    double ke = 0, P[3] = {0, 0, 0}, L[3] = {0, 0, 0}, C[3] = {0, 0, 0}, M = 0;
+    for (int32_t i = 0; i < n; i++) {
+        if (!active[i]) continue;
+        const double mi = m[i];
+        const double vxi = vx[i], vyi = vy[i], vzi = vz[i];
+        const double pxi = px[i], pyi = py[i], pzi = pz[i];
+        const double v2 = vxi * vxi + vyi * vyi + vzi * vzi;
+        ke += 0.5 * mi * v2;
+        P[0] += mi * vxi;
+        P[1] += mi * vyi;
+        P[2] += mi * vzi;
+        L[0] += mi * (pyi * vzi - pzi * vyi);
+        L[1] += mi * (pzi * vxi - pxi * vzi);
+        L[2] += mi * (pxi * vyi - pyi * vxi);
+        M += mi;
+        C[0] += mi * pxi;
+        C[1] += mi * pyi;
+        C[2] += mi * pzi;
+    }
+    double pe = 0.0;
+    for (int32_t i = 0; i < n; i++) {
+        if (!active[i]) continue;
+        for (int32_t j = i + 1; j < n; j++) {
+            if (!active[j]) continue;
+            const double dx = px[i] - px[j], dy = py[i] - py[j], dz = pz[i] - pz[j];
+            const double dist2 = dx * dx + dy * dy + dz * dz + eps2;
+            pe -= m[i] * m[j] / sqrt(dist2);
+        }
+    }
     o[0] = ke; o[1] = pe; o[2] = ke + pe;
     o[3] = P[0]; o[4] = P[1]; o[5] = P[2];
     o[6] = L[0]; o[7] = L[1]; o[8] = L[2];

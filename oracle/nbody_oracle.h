@@ -64,6 +64,10 @@ int32_t or_compact_indices(int32_t n, const uint8_t* active, const double* mass,
 /* All overlapping pairs (lo, hi), lo < hi, sorted (collision_kernel.cu:40-52
  * overlap test; CollisionResolver::sort_pairs order).  Returns the count
  * (pairs beyond max_pairs are counted, not written). */
+int32_t or_broad_phase_parallel(int32_t n, const double* px, const double* py, const double* pz,
+                                const double* radius, const uint8_t* active,
+                                const uint8_t* collidable, int32_t max_pairs, int32_t* lo,
+                                int32_t* hi, int32_t threads);
 int32_t or_broad_phase(int32_t n, const double* px, const double* py, const double* pz,
                        const double* radius, const uint8_t* active, const uint8_t* collidable,
                        int32_t max_pairs, int32_t* lo, int32_t* hi);
@@ -76,6 +80,31 @@ int32_t or_resolve_merges(int32_t n, double* px, double* py, double* pz, double*
                           double min_radius);
 
 /* Velocity Verlet with direct-sum forces (SoAVerletIntegrator.cs:48-116). */
+/* Direct sums in the other reference backends' orders (see nbody_oracle.c):
+ * order 0 CpuParallelBackend, 1 SimdSingleThreadBackend (= the native
+ * engine's CPU brute force), 2 CpuSingleThreadBackend. */
+void or_direct_forces_simd(int32_t n, const double* px, const double* py, const double* pz,
+                           const double* m, const double* radius, const uint8_t* active,
+                           double eps, int32_t shell, double* ax, double* ay, double* az,
+                           int32_t threads);
+void or_direct_forces_pairwise(int32_t n, const double* px, const double* py, const double* pz,
+                               const double* m, const double* radius, const uint8_t* active,
+                               double eps, int32_t shell, double* ax, double* ay, double* az);
+void or_direct_forces_order(int32_t n, const double* px, const double* py, const double* pz,
+                            const double* m, const double* radius, const uint8_t* active,
+                            double eps, int32_t shell, int32_t order, double* ax, double* ay,
+                            double* az, int32_t threads);
+void or_verlet_direct_order(int32_t n, double* px, double* py, double* pz, double* vx,
+                            double* vy, double* vz, double* ax, double* ay, double* az,
+                            const double* m, const uint8_t* active, double eps, double dt,
+                            int32_t steps, int32_t order, int32_t threads);
+void or_yoshida_direct_order(int32_t n, double* px, double* py, double* pz, double* vx,
+                             double* vy, double* vz, double* ax, double* ay, double* az,
+                             const double* m, const uint8_t* active, double eps, double dt,
+                             int32_t steps, int32_t order, int32_t threads);
+void or_energy_tracker(int32_t n, const double* px, const double* py, const double* pz,
+                       const double* vx, const double* vy, const double* vz, const double* m,
+                       const uint8_t* active, double eps, double* o);
 void or_verlet_direct(int32_t n, double* px, double* py, double* pz, double* vx, double* vy,
                       double* vz, double* ax, double* ay, double* az, const double* m,
                       const uint8_t* active, double eps, double dt, int32_t steps,

@@ -18,15 +18,19 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libcelestial_ref.so"
-REF_TREE = Path("/root/reference/engine")
+# root of the reference repository (only needed to build _ref)
+REF_ENV = "CELESTIAL_REF"
 
 P = C.c_void_p
 i32, f64, u8 = C.c_int32, C.c_double, C.c_uint8
 
 
 def build(ref: bool = True) -> None:
-    """Compile liboracle.so (and _ref when the reference tree exists)."""
-    targets = ["all"] + (["ref"] if ref and REF_TREE.exists() else [])
+    """Compile liboracle.so, and _ref when $CELESTIAL_REF names the
+    reference repository root and its engine sources are there."""
+    root = os.environ.get(REF_ENV, "")
+    with_ref = ref and root and (Path(root) / "engine" / "src").is_dir()
+    targets = ["all"] + (["ref", f"CELESTIAL_REF={root}"] if with_ref else [])
     subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
 
 
@@ -61,6 +65,13 @@ _OR_SIGS = {
     "or_yoshida_direct": (None, [i32, P, P, P, P, P, P, P, P, P, P, P, f64, f64, i32, i32]),
     "or_adaptive_dt": (f64, [i32, P, P, P, P, f64, f64, f64, f64]),
     "or_force_error": (i32, [i32, P, P, P, P, P, P, P, P]),
+    "or_direct_forces_order": (None, [i32, P, P, P, P, P, P, f64, i32, i32, P, P, P, i32]),
+    "or_verlet_direct_order": (None, [i32, P, P, P, P, P, P, P, P, P, P, P, f64, f64, i32, i32,
+                                      i32]),
+    "or_yoshida_direct_order": (None, [i32, P, P, P, P, P, P, P, P, P, P, P, f64, f64, i32, i32,
+                                       i32]),
+    "or_energy_tracker": (None, [i32, P, P, P, P, P, P, P, P, f64, P]),
+    "or_broad_phase_parallel": (i32, [i32, P, P, P, P, P, P, i32, P, P, i32]),
 }
 _REF_SIGS = {
     "ref_morton_from_unit": (C.c_uint64, [f64, f64, f64]),
@@ -68,6 +79,11 @@ _REF_SIGS = {
     "ref_bh_forces": (f64, [i32, P, P, P, P, P, f64, f64, i32, i32, P, P, P, P]),
     "ref_compact": (i32, [i32, P, P, P, P, P, P, P, P]),
     "ref_resolve_merges": (i32, [i32, P, P, P, P, P, P, P, P, P, P, i32, P, P, i32, i32, i32, f64]),
+    "ref_engine_steps": (i32, [i32, P, P, P, P, P, P, P, P, P, P, P, P, i32, i32, f64, f64, f64,
+                               i32]),
+    "ref_engine_update": (i32, [i32, P, P, P, P, P, P, P, P, P, P, P, i32, i32, f64, f64, f64,
+                                i32, f64, f64, f64, f64, f64, i32, P, P]),
+    "ref_energy_tracker": (None, [i32, P, P, P, P, P, P, P, P, f64, P]),
 }
 
 _lib = None
@@ -230,13 +246,21 @@ def compact_indices(active, mass):
     return dest, int(k)
 
 
-def broad_phase(px, py, pz, radius, active, collidable=None, max_pairs=1 << 22):
+def broad_phase(px, py, pz, radius, active, collidable=None, max_pairs=1 << 22,
+                nthreads=None):
+    """All pairs with |xi - xj|^2 < (ri + rj)^2 in (lo, hi) order; the rows
+    are split over `nthreads` threads when given (same list)."""
     lo = np.empty(max_pairs, np.int32)
     hi = np.empty(max_pairs, np.int32)
     px, py, pz, radius = map(_f, (px, py, pz, radius))
+    act = _u8(active)
     col = None if collidable is None else _u8(collidable)
-    k = lib().or_broad_phase(len(px), _p(px), _p(py), _p(pz), _p(radius), _p(_u8(active)),
-                             _p(col), max_pairs, _p(lo), _p(hi))
+    if nthreads:
+        k = lib().or_broad_phase_parallel(len(px), _p(px), _p(py), _p(pz), _p(radius), _p(act),
+                                          _p(col), max_pairs, _p(lo), _p(hi), int(nthreads))
+    else:
+        k = lib().or_broad_phase(len(px), _p(px), _p(py), _p(pz), _p(radius), _p(act),
+                                 _p(col), max_pairs, _p(lo), _p(hi))
     k = min(k, max_pairs)
     return lo[:k].copy(), hi[:k].copy()
 
@@ -262,22 +286,96 @@ def ref_resolve_merges(b, lo, hi, **kw):
     return _merge(ref().ref_resolve_merges, b, lo, hi, **kw)
 
 
-def verlet_direct(b: dict, eps, dt, steps, nthreads=None):
-    a = {k: _f(b[k]).copy() for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az", "mass")}
+# direct-sum orders of the reference backends (or_direct_forces_order)
+ORDER_PARALLEL, ORDER_SIMD, ORDER_PAIRWISE = 0, 1, 2
+_STATE = ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az", "mass")
+
+
+def direct_forces_order(px, py, pz, m, active, eps, order, radius=None, shell=False,
+                        nthreads=None):
+    """Direct sum in the order of CpuParallelBackend (0), the SIMD backend /
+    native engine (1) or CpuSingleThreadBackend (2)."""
+    n = len(px)
+    px, py, pz, m = map(_f, (px, py, pz, m))
+    active = _u8(active)
+    radius = None if radius is None else _f(radius)
+    ax, ay, az = np.empty(n), np.empty(n), np.empty(n)
+    lib().or_direct_forces_order(n, _p(px), _p(py), _p(pz), _p(m), _p(radius), _p(active), eps,
+                                 int(shell), int(order), _p(ax), _p(ay), _p(az),
+                                 nthreads or threads())
+    return ax, ay, az
+
+
+def verlet_direct(b: dict, eps, dt, steps, nthreads=None, order=ORDER_PARALLEL):
+    a = {k: _f(b[k]).copy() for k in _STATE}
     act = _u8(b["active"])
-    lib().or_verlet_direct(len(act), *(_p(a[k]) for k in ("px", "py", "pz", "vx", "vy", "vz",
-                                                           "ax", "ay", "az", "mass")), _p(act),
-                           eps, dt, steps, nthreads or threads())
+    lib().or_verlet_direct_order(len(act), *(_p(a[k]) for k in _STATE), _p(act), eps, dt, steps,
+                                 int(order), nthreads or threads())
     return a
 
 
-def yoshida_direct(b: dict, eps, dt, steps, nthreads=None):
-    a = {k: _f(b[k]).copy() for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az", "mass")}
+def yoshida_direct(b: dict, eps, dt, steps, nthreads=None, order=ORDER_PARALLEL):
+    a = {k: _f(b[k]).copy() for k in _STATE}
     act = _u8(b["active"])
-    lib().or_yoshida_direct(len(act), *(_p(a[k]) for k in ("px", "py", "pz", "vx", "vy", "vz",
-                                                            "ax", "ay", "az", "mass")), _p(act),
-                            eps, dt, steps, nthreads or threads())
+    lib().or_yoshida_direct_order(len(act), *(_p(a[k]) for k in _STATE), _p(act), eps, dt, steps,
+                                  int(order), nthreads or threads())
     return a
+
+
+def ref_engine_steps(b: dict, eps, dt, steps, compute_mode=0, integrator=0, theta=0.5):
+    """The reference's own Engine (CPU_BruteForce = 0 / CPU_BarnesHut = 1,
+    Leapfrog_KDK = 0 / Yoshida4 = 1): set_particles, then `steps` steps."""
+    a = {k: _f(b[k]).copy() for k in _STATE}
+    act = _u8(b["active"])
+    rad = _f(b["radius"]) if b.get("radius") is not None else None
+    r = ref().ref_engine_steps(len(act), *(_p(a[k]) for k in _STATE), _p(rad), _p(act),
+                               int(compute_mode), int(integrator), theta, dt, eps, int(steps))
+    if r != 0:
+        raise RuntimeError("reference Engine threw")
+    return a
+
+
+def ref_engine_update(b: dict, eps, dt, frame_time, frames, compute_mode=0, integrator=0,
+                      theta=0.5, adaptive=False, eta=0.01, dt_min=1e-8, dt_max=0.01,
+                      initial_dt=0.001):
+    """`frames` calls of the reference Engine::update(frame_time); returns
+    (final state, steps per frame, adaptive dt after the last frame)."""
+    a = {k: _f(b[k]).copy() for k in _STATE}
+    act = _u8(b["active"])
+    steps = np.zeros(frames, np.int32)
+    dt_out = np.zeros(1)
+    r = ref().ref_engine_update(len(act), *(_p(a[k]) for k in _STATE), _p(act),
+                                int(compute_mode), int(integrator), theta, dt, eps,
+                                int(adaptive), eta, dt_min, dt_max, initial_dt, frame_time,
+                                int(frames), _p(steps), _p(dt_out))
+    if r != 0:
+        raise RuntimeError("reference Engine threw")
+    return a, steps, float(dt_out[0])
+
+
+_ENERGY_KEYS = ("ke", "pe", "e", "px", "py", "pz", "lx", "ly", "lz", "comx", "comy", "comz", "m")
+
+
+def _energy_args(b):
+    # hold the converted arrays: ctypes gets raw pointers
+    arrs = [_f(b[k]) for k in ("px", "py", "pz", "vx", "vy", "vz", "mass")]
+    return arrs, _u8(b["active"])
+
+
+def energy_tracker(b: dict, eps):
+    """The native engine's EnergyTracker::compute restated (or_energy_tracker)."""
+    out = np.empty(13)
+    arrs, act = _energy_args(b)
+    lib().or_energy_tracker(len(act), *(_p(x) for x in arrs), _p(act), eps, _p(out))
+    return dict(zip(_ENERGY_KEYS, out.tolist()))
+
+
+def ref_energy_tracker(b: dict, eps):
+    """EnergyTracker::compute of the reference itself."""
+    out = np.empty(13)
+    arrs, act = _energy_args(b)
+    ref().ref_energy_tracker(len(act), *(_p(x) for x in arrs), _p(act), eps, _p(out))
+    return dict(zip(_ENERGY_KEYS, out.tolist()))
 
 
 def adaptive_dt(b: dict, eps, eta, dt_min, dt_max):
@@ -289,11 +387,10 @@ def adaptive_dt(b: dict, eps, eta, dt_min, dt_max):
 
 def energy(b: dict, eps, nthreads=None):
     out = np.empty(13)
-    lib().or_energy(len(b["px"]), *(_p(_f(b[k])) for k in ("px", "py", "pz", "vx", "vy", "vz",
-                                                            "mass")), _p(_u8(b["active"])), eps,
-                    _p(out), nthreads or threads())
-    keys = ("ke", "pe", "e", "px", "py", "pz", "lx", "ly", "lz", "comx", "comy", "comz", "m")
-    return dict(zip(keys, out.tolist()))
+    arrs, act = _energy_args(b)
+    lib().or_energy(len(act), *(_p(x) for x in arrs), _p(act), eps, _p(out),
+                    nthreads or threads())
+    return dict(zip(_ENERGY_KEYS, out.tolist()))
 
 
 def force_error(a, ref_a, active=None):
