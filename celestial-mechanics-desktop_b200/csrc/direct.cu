@@ -256,11 +256,25 @@ __global__ void k_direct_reduce(int n, int chunks, const double* __restrict__ pa
 // subtract them in source order, one (target, component) chain per thread.
 // The sequence of roundings of every target's sum is unchanged, so the
 // result is bit-identical to CpuParallelBackend's.
+//
+// ORDER selects the rounding and summation order of another CPU backend of
+// the desktop app (without the shell theorem; with it every backend runs
+// CpuParallelBackend's arithmetic):
+//   kOrderParallel  CpuParallelBackend: c = ((m*inv)*inv)*inv, one running sum;
+//   kOrderSimd      SimdSingleThreadBackend (SimdSingleThreadBackend.cs:43-165)
+//                   and the native engine's CPU brute force (engine/src/sim/
+//                   engine.cpp:649-674): c = m*((inv*inv)*inv), sources in
+//                   row order (the vector lanes are summed in lane order);
+//   kOrderPairwise  CpuSingleThreadBackend's Newton's-third-law loop
+//                   (CpuSingleThreadBackend.cs:50-159): the same c, and a
+//                   body's sum is (its running sum over lower rows, which the
+//                   loop adds into ax[j] as +c*(x_lower - x_j), i.e. minus
+//                   the term) + (its running sum over higher rows).
 constexpr int kPTi = 8;     // targets per block
 constexpr int kPTj = 128;   // sources per tile
 constexpr int kPThreads = 256;
 
-template <bool SHELL>
+template <bool SHELL, int ORDER>
 __global__ void __launch_bounds__(kPThreads)
 k_direct_fp64_pairs(int n, const double* __restrict__ px, const double* __restrict__ py,
                     const double* __restrict__ pz, const double* __restrict__ m,
@@ -284,7 +298,9 @@ k_direct_fp64_pairs(int n, const double* __restrict__ px, const double* __restri
     // accumulator thread: (target, component)
     const int acc_t = threadIdx.x / 3, acc_c = threadIdx.x % 3;
     const bool accum = threadIdx.x < 3 * kPTi;
+    constexpr bool kSplit = !SHELL && ORDER == kOrderPairwise;
     double sum = 0.0;
+    double hi = 0.0;  // kSplit: the sum over higher rows (sum holds the lower rows')
     for (int base = 0; base < n; base += kPTj) {
         for (int p = threadIdx.x; p < kPTi * kPTj; p += kPThreads) {
             const int ti = p / kPTj, tj = p % kPTj;
@@ -300,7 +316,10 @@ k_direct_fp64_pairs(int n, const double* __restrict__ px, const double* __restri
                 const double mj = m[j];
                 double c;
                 const double R = SHELL ? rad[j] : 0.0;
-                if (!SHELL || R <= 0.0) {
+                if (!SHELL && ORDER != kOrderParallel) {
+                    const double inv = 1.0 / sqrt(__dadd_rn(raw, eps2));
+                    c = __dmul_rn(mj, __dmul_rn(__dmul_rn(inv, inv), inv));
+                } else if (!SHELL || R <= 0.0) {
                     const double inv = 1.0 / sqrt(__dadd_rn(raw, eps2));
                     c = __dmul_rn(__dmul_rn(__dmul_rn(mj, inv), inv), inv);
                 } else if (sqrt(raw) < R) {
@@ -323,25 +342,45 @@ k_direct_fp64_pairs(int n, const double* __restrict__ px, const double* __restri
         __syncthreads();
         if (accum) {
             const int cnt = min(kPTj, n - base);
-            for (int tj = 0; tj < cnt; tj++)
-                if (s_ok[acc_t][tj]) sum = __dsub_rn(sum, s_t[acc_c][acc_t][tj]);
+            if (kSplit) {
+                const int split = i0 + acc_t - base;  // first tj with j > i
+                for (int tj = 0; tj < cnt; tj++) {
+                    if (!s_ok[acc_t][tj]) continue;
+                    if (tj < split) sum = __dsub_rn(sum, s_t[acc_c][acc_t][tj]);
+                    else hi = __dsub_rn(hi, s_t[acc_c][acc_t][tj]);
+                }
+            } else {
+                for (int tj = 0; tj < cnt; tj++)
+                    if (s_ok[acc_t][tj]) sum = __dsub_rn(sum, s_t[acc_c][acc_t][tj]);
+            }
         }
         __syncthreads();
     }
     if (accum) {
         const int i = i0 + acc_t;
+        if (kSplit) sum = __dadd_rn(sum, hi);
         if (i < n) (acc_c == 0 ? ax : acc_c == 1 ? ay : az)[i] = sum;
     }
 }
 
 void direct_fp64(cudaStream_t st, int n, const double* px, const double* py, const double* pz,
                  const double* m, const double* rad, const uint8_t* act, double eps, bool shell,
-                 double* ax, double* ay, double* az) {
+                 int order, double* ax, double* ay, double* az) {
     if (n <= 0) return;
     const double eps2 = eps * eps;
     const int g = ceil_div(n, kPTi);
-    if (shell) k_direct_fp64_pairs<true><<<g, kPThreads, 0, st>>>(n, px, py, pz, m, rad, act, eps2, ax, ay, az);
-    else k_direct_fp64_pairs<false><<<g, kPThreads, 0, st>>>(n, px, py, pz, m, rad, act, eps2, ax, ay, az);
+    if (shell)
+        k_direct_fp64_pairs<true, kOrderParallel><<<g, kPThreads, 0, st>>>(
+            n, px, py, pz, m, rad, act, eps2, ax, ay, az);
+    else if (order == kOrderSimd)
+        k_direct_fp64_pairs<false, kOrderSimd><<<g, kPThreads, 0, st>>>(
+            n, px, py, pz, m, rad, act, eps2, ax, ay, az);
+    else if (order == kOrderPairwise)
+        k_direct_fp64_pairs<false, kOrderPairwise><<<g, kPThreads, 0, st>>>(
+            n, px, py, pz, m, rad, act, eps2, ax, ay, az);
+    else
+        k_direct_fp64_pairs<false, kOrderParallel><<<g, kPThreads, 0, st>>>(
+            n, px, py, pz, m, rad, act, eps2, ax, ay, az);
 }
 
 void direct_fp32(cudaStream_t st, int n, const double4* sbody, const float* srad,

@@ -47,6 +47,46 @@ def test_direct_fp64_bit_exact_inactive_and_shell(engine, oracle):
     assert np.all(got[0][d.active == 0] == 0.0)
 
 
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("n,inactive", [(1000, 0), (1531, 13)])
+def test_direct_fp64_backend_orders_bit_exact(engine, oracle, order, n, inactive):
+    """NB_FLAG_ORDER_SIMD / NB_FLAG_ORDER_PAIRWISE give the bits of the SIMD
+    backend (and the native engine's CPU brute force) and of the
+    single-thread Newton's-third-law backend."""
+    b = scenarios.plummer(n, seed=40 + order)
+    if inactive:
+        b.active[::inactive] = 0
+    flag = N.FLAG_ORDER_SIMD if order == 1 else N.FLAG_ORDER_PAIRWISE
+    got = _forces(engine, b, 1e-4, MODE_DIRECT_FP64 | flag)
+    want = oracle.direct_forces_order(b.px, b.py, b.pz, b.mass, b.active, 1e-4, order)
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
+
+
+def test_direct_fp64_engine_order_equals_reference_engine(engine, ref_lib):
+    """The SIMD-order flag against the reference's own Engine CPU brute force
+    (oracle/_ref) on the same input: identical accelerations."""
+    b = scenarios.plummer(900, seed=44)
+    b.active[2::31] = 0
+    got = _forces(engine, b, 1e-4, MODE_DIRECT_FP64 | N.FLAG_ORDER_SIMD)
+    d = {k: getattr(b, k) for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az",
+                                     "mass", "active")}
+    d["radius"] = None
+    want = ref_lib.ref_engine_steps(d, 1e-4, 0.0, 1)
+    for g, k in zip(got, ("ax", "ay", "az")):
+        np.testing.assert_array_equal(g, want[k])
+
+
+def test_direct_fp64_orders_with_shell_theorem_are_cpuparallel(engine, oracle):
+    d = scenarios.collisional_disk(600, seed=45, radius_scale=3000.0)
+    want = oracle.direct_forces(d.px, d.py, d.pz, d.mass, d.active, 1e-4, radius=d.radius,
+                                shell=True)
+    for flag in (N.FLAG_ORDER_SIMD, N.FLAG_ORDER_PAIRWISE):
+        got = _forces(engine, d, 1e-4, MODE_DIRECT_FP64 | FLAG_SHELL_THEOREM | flag)
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g, w)
+
+
 def test_known_answers(engine):
     """|a| = 1 for unit masses at distance 1 (test_gravity.cpp:16-45);
     inactive bodies get 0 (test_gravity.cpp:108-130); a lone body gets 0."""
