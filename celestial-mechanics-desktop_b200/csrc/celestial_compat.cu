@@ -75,7 +75,9 @@ int32_t to_error_code(int32_t r) {
 int mode_flags(const Config& c) {
     int f = 0;
     switch (c.compute_mode) {
-        case 0: case 2: f = NB_MODE_DIRECT_FP64; break;
+        // the reference's CPU brute-force arithmetic and order
+        // (Engine::compute_cpu_brute_forces, engine.cpp:649-674)
+        case 0: case 2: f = NB_MODE_DIRECT_FP64 | NB_FLAG_ORDER_SIMD; break;
         case 1: f = NB_MODE_BARNES_HUT_REF; break;
         default: f = NB_MODE_BARNES_HUT; break;
     }
@@ -109,36 +111,39 @@ void step_once(double dt, double softening) {
     set_error(nullptr);
 }
 
-// nb_get_state into host scratch of the handle's capacity.
-struct HostState {
-    std::vector<double> f[11];
-    std::vector<uint8_t> act;
-    std::vector<int32_t> ids;
-    int n = 0;
-};
-
-bool read_state(HostState& s) {
-    for (auto& v : s.f) v.resize((size_t)g_capacity);
-    s.act.resize((size_t)g_capacity);
-    s.ids.resize((size_t)g_capacity);
-    int32_t n = 0;
-    const int32_t r = nb_get_state(g_h, &n, s.f[0].data(), s.f[1].data(), s.f[2].data(),
-                                   s.f[3].data(), s.f[4].data(), s.f[5].data(), s.f[6].data(),
-                                   s.f[7].data(), s.f[8].data(), s.f[9].data(), s.f[10].data(),
-                                   s.act.data(), s.ids.data());
-    if (failed(r, "nb_get_state")) return false;
-    s.n = n;
-    return true;
-}
-
-void copy_out(int first_field, double* a, double* b, double* c, int32_t count) {
+// One field triple of the device state (positions, velocities or
+// accelerations) straight into the caller's arrays: nb_get_state skips the
+// NULL outputs, so only these three arrays of n rows cross PCIe.
+void copy_out(int which, double* a, double* b, double* c, int32_t count) {
     if (!g_h || !a || !b || !c || count <= 0) return;
-    HostState s;
-    if (!read_state(s)) return;
-    const size_t m = (size_t)std::min<int32_t>(count, s.n);
-    std::memcpy(a, s.f[first_field].data(), m * sizeof(double));
-    std::memcpy(b, s.f[first_field + 1].data(), m * sizeof(double));
-    std::memcpy(c, s.f[first_field + 2].data(), m * sizeof(double));
+    int32_t n = 0, na = 0;
+    if (failed(nb_get_body_count(g_h, &n, &na), "nb_get_body_count")) return;
+    if (count < n) {
+        // the caller's arrays hold fewer rows than the state: stage through
+        // host scratch of n rows and copy the first `count`
+        std::vector<double> t[3];
+        for (auto& v : t) v.resize((size_t)n);
+        double* o[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                        nullptr, nullptr, nullptr};
+        for (int k = 0; k < 3; k++) o[3 * which + k] = t[k].data();
+        if (failed(nb_get_state(g_h, nullptr, o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7],
+                                o[8], nullptr, nullptr, nullptr, nullptr),
+                   "nb_get_state"))
+            return;
+        std::memcpy(a, t[0].data(), (size_t)count * sizeof(double));
+        std::memcpy(b, t[1].data(), (size_t)count * sizeof(double));
+        std::memcpy(c, t[2].data(), (size_t)count * sizeof(double));
+    } else {
+        double* o[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                        nullptr, nullptr, nullptr};
+        o[3 * which] = a;
+        o[3 * which + 1] = b;
+        o[3 * which + 2] = c;
+        if (failed(nb_get_state(g_h, nullptr, o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7],
+                                o[8], nullptr, nullptr, nullptr, nullptr),
+                   "nb_get_state"))
+            return;
+    }
     set_error(nullptr);
 }
 
@@ -185,12 +190,20 @@ NB_API void celestial_set_particles(const double* pos_x, const double* pos_y,
     if (!g_h) return;
     const int32_t r = nb_set_state(g_h, count, pos_x, pos_y, pos_z, vel_x, vel_y, vel_z, mass,
                                    radius, nullptr, is_active, nullptr, acc_x, acc_y, acc_z);
-    if (!failed(r, "nb_set_state")) set_error(nullptr);
+    if (failed(r, "nb_set_state")) return;
+    // a new scene restarts the energy tracker (Engine::set_particles calls
+    // energy_tracker_.reset(), engine/src/sim/engine.cpp:195): drifts and the
+    // accumulated error are measured from the next snapshot of this scene
+    g_has_initial = false;
+    g_initial = Snapshot{};
+    g_current = Snapshot{};
+    g_accumulated_error = 0.0;
+    set_error(nullptr);
 }
 
 NB_API void celestial_get_accelerations(double* out_acc_x, double* out_acc_y,
                                         double* out_acc_z, int32_t count) {
-    copy_out(6, out_acc_x, out_acc_y, out_acc_z, count);
+    copy_out(2, out_acc_x, out_acc_y, out_acc_z, count);
 }
 
 NB_API void celestial_get_positions(double* out_pos_x, double* out_pos_y, double* out_pos_z,
@@ -200,7 +213,7 @@ NB_API void celestial_get_positions(double* out_pos_x, double* out_pos_y, double
 
 NB_API void celestial_get_velocities(double* out_vel_x, double* out_vel_y, double* out_vel_z,
                                      int32_t count) {
-    copy_out(3, out_vel_x, out_vel_y, out_vel_z, count);
+    copy_out(1, out_vel_x, out_vel_y, out_vel_z, count);
 }
 
 NB_API void celestial_compute_forces(double softening) {

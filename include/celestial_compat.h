@@ -12,8 +12,12 @@
  *
  * Differences, stated once:
  *   - every compute mode runs on the GPU: the two brute-force modes (0, 2)
- *     use the FP64 direct sum that is bit-identical to the reference's CPU
- *     arithmetic; CPU_BarnesHut (1) uses the reference-semantics walk
+ *     use the FP64 direct sum in the order and rounding of the reference's
+ *     CPU brute force (Engine::compute_cpu_brute_forces, coefficient
+ *     m * inv^3), so CPU_BruteForce trajectories are bit-identical to the
+ *     reference's (the reference's GPU brute-force kernel uses CUDA's rsqrt
+ *     and FMA contraction and has no reproducible bits to match);
+ *     CPU_BarnesHut (1) uses the reference-semantics walk
  *     (monopole, the reference's MAC); GPU_BarnesHut (3) the B200 group walk
  *     (monopole + quadrupole, FP32 pair forces);
  *   - collision modes: Ignore (0) and Merge (3); Elastic (1) and Inelastic (2)

@@ -1,8 +1,9 @@
-"""The `celestial_*` compatibility layer on the GPU, against the oracle: the
-same trajectories bit for bit as the reference's CPU arithmetic (Verlet and
-Yoshida4 steps with the FP64 direct sum, the frame accumulator with the
-adaptive time step), energy and momentum drift as EnergyTracker defines
-them, counts, refused collision modes and the lifecycle rules."""
+"""The `celestial_*` compatibility layer on the GPU, against the oracle and
+the reference's own Engine (oracle/_ref): the same trajectories bit for bit
+as the reference's CPU brute force (Verlet and Yoshida4 steps, the frame
+accumulator with the adaptive time step), energy and momentum drift as
+EnergyTracker defines them, counts, refused collision modes and the
+lifecycle rules."""
 from __future__ import annotations
 
 import numpy as np
@@ -55,9 +56,12 @@ def _download(lib, n):
 
 
 def _chain(oracle, b, dts):
+    """Verlet steps of the given dts with the reference engine's CPU
+    brute-force arithmetic (the SIMD-backend order)."""
     s = bodies_dict(b)
     for dt in dts:
-        s = dict(oracle.verlet_direct(s | {"active": b.active}, EPS, dt, 1), active=b.active)
+        s = dict(oracle.verlet_direct(s | {"active": b.active}, EPS, dt, 1,
+                                      order=oracle.ORDER_SIMD), active=b.active)
     return s
 
 
@@ -101,7 +105,8 @@ def test_compat_update_with_adaptive_dt(lib, oracle):
     s, dt, dts = bodies_dict(b), dt0, []
     for _ in range(3):
         dts.append(dt)
-        s = dict(oracle.verlet_direct(s | {"active": b.active}, EPS, dt, 1), active=b.active)
+        s = dict(oracle.verlet_direct(s | {"active": b.active}, EPS, dt, 1,
+                                      order=oracle.ORDER_SIMD), active=b.active)
         a2 = s["ax"] * s["ax"] + s["ay"] * s["ay"] + s["az"] * s["az"]
         amax = float(np.sqrt(a2[b.active.astype(bool) & (a2 > 0)].max()))
         dt = min(max(eta * float(np.sqrt(EPS / amax)), lo), hi)
@@ -110,6 +115,86 @@ def test_compat_update_with_adaptive_dt(lib, oracle):
     assert len(set(dts)) > 1
     # the accumulator keeps the remainder: 0.0005 + 0.0006 makes one more step
     assert lib.celestial_update(0.0006) == 1
+
+
+@pytest.mark.parametrize("integrator", [0, 1])
+def test_compat_bit_exact_with_the_reference_engine(lib, ref_lib, integrator):
+    """CPU_BruteForce through the compatibility layer against the reference's
+    own Engine (engine.cpp compiled into oracle/_ref) on the same input:
+    identical trajectories, Leapfrog_KDK and Yoshida4."""
+    b = scenarios.plummer(400, seed=31)
+    b.active[7::29] = 0
+    d = bodies_dict(b)
+    d["ax"], d["ay"], d["az"] = ref_lib.direct_forces_order(
+        b.px, b.py, b.pz, b.mass, b.active, EPS, ref_lib.ORDER_SIMD)
+    lib.celestial_set_compute_mode(0)
+    lib.celestial_set_integrator(integrator)
+    arrs = [np.ascontiguousarray(d[k], np.float64)
+            for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az", "mass", "radius")]
+    act = np.ascontiguousarray(b.active, np.uint8)
+    lib.celestial_set_particles(*(a.ctypes.data for a in arrs), act.ctypes.data, b.n)
+    for _ in range(12):
+        lib.celestial_step(1e-3, EPS)
+    want = ref_lib.ref_engine_steps(d, EPS, 1e-3, 12, compute_mode=0, integrator=integrator)
+    _assert_same(_download(lib, 400), want, f"reference engine, integrator {integrator}")
+
+
+def test_compat_adaptive_update_bit_exact_with_the_reference_engine(lib, ref_lib):
+    """celestial_update with the adaptive time step against the reference's
+    Engine::update on the same input: the same step counts, final dt and
+    trajectory."""
+    b = scenarios.plummer(300, seed=32)
+    d = bodies_dict(b)
+    d["ax"], d["ay"], d["az"] = ref_lib.direct_forces_order(
+        b.px, b.py, b.pz, b.mass, b.active, EPS, ref_lib.ORDER_SIMD)
+    eta, lo, hi, dt0 = 0.02, 1e-7, 5e-3, 1e-3
+    lib.celestial_set_compute_mode(0)
+    lib.celestial_set_adaptive_timestep(1, eta, lo, hi, dt0)
+    arrs = [np.ascontiguousarray(d[k], np.float64)
+            for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az", "mass", "radius")]
+    act = np.ascontiguousarray(b.active, np.uint8)
+    lib.celestial_set_particles(*(a.ctypes.data for a in arrs), act.ctypes.data, b.n)
+    got_steps = [lib.celestial_update(3.5e-3) for _ in range(4)]
+    want, steps, dt_last = ref_lib.ref_engine_update(d, EPS, 1e-3, 3.5e-3, 4, adaptive=True,
+                                                     eta=eta, dt_min=lo, dt_max=hi,
+                                                     initial_dt=dt0)
+    assert got_steps == list(steps)
+    assert lib.celestial_get_adaptive_dt() == dt_last
+    got = _download(lib, 300)
+    for k in ("px", "py", "pz", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+
+
+def test_compat_new_scene_restarts_the_energy_tracker(lib):
+    """celestial_set_particles resets the drift bookkeeping, as the
+    reference's Engine::set_particles does (engine.cpp:195): the first
+    snapshot of a new scene is its own baseline."""
+    a = scenarios.plummer(200, seed=33)
+    _upload(lib, a)
+    lib.celestial_compute_forces(EPS)
+    lib.celestial_compute_energy_snapshot()
+    for _ in range(5):
+        lib.celestial_step(1e-3, EPS)
+    lib.celestial_compute_energy_snapshot()
+    assert lib.celestial_get_accumulated_error() > 0.0
+    b = scenarios.plummer(250, seed=34)
+    _upload(lib, b)
+    lib.celestial_compute_forces(EPS)
+    lib.celestial_compute_energy_snapshot()
+    assert lib.celestial_get_energy_drift() == 0.0
+    assert lib.celestial_get_momentum_drift() == 0.0
+    assert lib.celestial_get_angular_momentum_drift() == 0.0
+    assert lib.celestial_get_accumulated_error() == 0.0
+
+
+def test_compat_getters_copy_count_rows(lib):
+    """The getters fill `count` rows; fewer than the state holds is fine."""
+    b = scenarios.plummer(128, seed=35)
+    _upload(lib, b)
+    full = _download(lib, 128)
+    part = _download(lib, 50)
+    for k in ("px", "vy", "az"):
+        np.testing.assert_array_equal(part[k], full[k][:50])
 
 
 def test_compat_energy_drift_as_energy_tracker(lib, oracle):
