@@ -125,14 +125,16 @@ __global__ void k_iota(int n, uint32_t* v) {
 int broad_phase(cudaStream_t st, CollideBufs& b, CollideArgs& a, bool build_tree, int* np) {
     *np = 0;
     if (a.n <= 0) return NB_OK;
-    if (build_tree) {
-        launch_kick_drift_bbox(st, a.n, a.s, false, 0.0, a.bbox_ord, a.n_active_dev, a.err);
-        launch_cube(st, a.bbox_ord, nullptr, a.cube);
+    if (!a.reuse_tree) {
+        if (build_tree) {
+            launch_kick_drift_bbox(st, a.n, a.s, false, 0.0, a.bbox_ord, a.n_active_dev, a.err);
+            launch_cube(st, a.bbox_ord, nullptr, a.cube);
+        }
+        launch_keys_cube(st, a.n, a.s, a.cube, a.keys0, a.vals0, (uint32_t*)a.sort_ws);
+        sort_pairs(st, a.n, a.keys0, a.vals0, a.keys1, a.vals1, a.sort_ws, true, a.err, a.sms);
+        launch_gather(st, a.n_active, a.s, a.vals0, a.sbody, a.srad);
+        tree_build(st, a.tree, a.n_active, a.keys0, a.sbody, a.srad, a.cube, a.leaf_cap, a.err);
     }
-    launch_keys_cube(st, a.n, a.s, a.cube, a.keys0, a.vals0, (uint32_t*)a.sort_ws);
-    sort_pairs(st, a.n, a.keys0, a.vals0, a.keys1, a.vals1, a.sort_ws, true, a.err, a.sms);
-    launch_gather(st, a.n_active, a.s, a.vals0, a.sbody, a.srad);
-    tree_build(st, a.tree, a.n_active, a.keys0, a.sbody, a.srad, a.cube, a.leaf_cap, a.err);
     cudaMemsetAsync(a.n_pairs, 0, sizeof(int), st);
     if (a.n_active > 0)
         k_broad_phase<<<ceil_div(a.n_active, 128), 128, 0, st>>>(

@@ -38,10 +38,16 @@ struct CollideArgs {
     int sms;
     unsigned long long* bbox_ord;
     int* n_active_dev;
+    // the force evaluation of this step left a tree of the current positions
+    // (keys0/vals0 sorted, sbody/srad gathered, multipole pass with radii,
+    // cube): the broad phase queries it instead of building its own
+    bool reuse_tree = false;
 };
 
 int collide_alloc(CollideBufs& b, int capacity, const std::function<int(void**, size_t)>& alloc);
 // All overlapping pairs of active, collidable rows, sorted; *np on the host.
+// build_tree: the bounding cube is recomputed first (otherwise a.cube is
+// current); with a.reuse_tree no key, sort or tree stage runs at all.
 int broad_phase(cudaStream_t st, CollideBufs& b, CollideArgs& a, bool build_tree, int* np);
 // Broad phase + merges + compaction of c.s into c.s_alt.
 int collide_step(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* npairs, int* nmerge,

@@ -68,6 +68,7 @@ struct nb_engine {
     double mac_budget = -3.0;
     int group_bodies = 32;
     double group_pack = 2.25;
+    int group_span = 0;  // >= 32: walk groups cut from cells of <= group_span bodies
     // adaptive time step (AdaptiveTimestepConfig defaults)
     double adapt_eta = 0.01, adapt_dt_min = 1e-8, adapt_dt_max = 0.01;
     double adapt_dt = 0.0;  // the next adaptive step's dt; 0 = take nb_step's dt
@@ -131,18 +132,21 @@ struct nb_engine {
     // captured single step (CUDA graph) and the parameters it was captured with
     cudaGraphExec_t graph_exec = nullptr;
     struct GraphKey {
-        int flags, n, n_active, leaf_cap;
+        int flags, n, n_active, leaf_cap, span;
         double dt, eps, theta, pack, mac_lo, mac_hi, mac_budget;
         const double* state;  // the state arrays swap after a compaction
         bool operator==(const GraphKey& o) const {
             return flags == o.flags && n == o.n && n_active == o.n_active &&
-                   leaf_cap == o.leaf_cap && dt == o.dt && eps == o.eps && theta == o.theta &&
+                   leaf_cap == o.leaf_cap && span == o.span && dt == o.dt && eps == o.eps && theta == o.theta &&
                    pack == o.pack && mac_lo == o.mac_lo && mac_hi == o.mac_hi &&
                    mac_budget == o.mac_budget && state == o.state;
         }
     } graph_key{};
     bool ev_valid = false;
     bool ev_tree = false;
+    bool ev_collide = false;   // ev[4], ev[5] bracket the last collision stage
+    bool tree_current = false; // the last force evaluation left a tree (with radii) of the
+                               // current positions: keys0/vals0, sbody/srad, tree, cube
     double timings[NB_T_COUNT] = {0};
     int64_t counters[NB_C_COUNT] = {0};
 };
@@ -235,8 +239,12 @@ void record(nb_engine* h, int k) {
 int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     const int mode = flags & NB_MODE_MASK;
     const bool shell = (flags & NB_FLAG_SHELL_THEOREM) != 0;
+    // the collision broad phase reuses this evaluation's tree, which then
+    // needs the radii (sorted, and each node's largest radius)
+    const bool radii = shell || (flags & NB_FLAG_COLLISIONS) != 0;
     const int n = h->n;
     Scal* sc = h->scal;
+    h->tree_current = false;
     record(h, 0);
     nb::launch_kick_drift_bbox(h->st, n, h->s, kick, dt, sc->bbox_ord, &sc->n_active, sc->err);
     cudaMemsetAsync(sc->counters, 0, sizeof(sc->counters), h->st);
@@ -244,8 +252,11 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     if (mode == NB_MODE_DIRECT_FP64) {
         record(h, 1);
         record(h, 2);
+        const int order = (flags & NB_FLAG_ORDER_PAIRWISE) ? nb::kOrderPairwise
+                          : (flags & NB_FLAG_ORDER_SIMD)   ? nb::kOrderSimd
+                                                           : nb::kOrderParallel;
         nb::direct_fp64(h->st, n, h->s.px, h->s.py, h->s.pz, h->s.mass, h->s.radius,
-                        h->s.active, eps, shell, h->s.ax, h->s.ay, h->s.az);
+                        h->s.active, eps, shell, order, h->s.ax, h->s.ay, h->s.az);
         record(h, 3);
         h->counters[NB_C_BODY_INTERACTIONS] = (int64_t)h->n_active * (h->n_active - 1);
         h->counters[NB_C_CELL_INTERACTIONS] = 0;
@@ -266,7 +277,7 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err,
                    h->sms);
     // the gather reads the previous step's |a| before the buffer is zeroed
-    nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, shell ? h->srad : nullptr,
+    nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, radii ? h->srad : nullptr,
                       learned ? h->samag : nullptr);
     nb::launch_zero_acc(h->st, n, h->s);
     record(h, 1);
@@ -278,9 +289,10 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
                         &sc->group_ctr, h->sms);
     } else if (mode == NB_MODE_BARNES_HUT || mode == NB_MODE_BARNES_HUT_REF) {
         const bool ref = mode == NB_MODE_BARNES_HUT_REF;
-        nb::tree_build(h->st, h->tree, na, h->keys0, h->sbody, shell ? h->srad : nullptr, sc->cube,
+        nb::tree_build(h->st, h->tree, na, h->keys0, h->sbody, radii ? h->srad : nullptr, sc->cube,
                        ref ? 1 : h->leaf_cap, sc->err);
         h->ev_tree = true;
+        h->tree_current = radii;
         record(h, 2);
         nb::WalkArgs a{};
         a.n = na;
@@ -299,6 +311,8 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
         a.groups = h->groups;
         a.n_groups = &sc->n_groups;
         a.pack = h->group_pack;
+    a.group_span = h->group_span;
+        a.group_span = h->group_span;
         a.counters = sc->counters;
         a.err = sc->err;
         if (ref) {
@@ -328,9 +342,6 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     return NB_OK;
 }
 
-// Capture one device step (forces + second half kick) as a CUDA graph, or
-// reuse the captured one when nothing it depends on changed.  Per-stage
-// timing events are not recorded inside the graph.
 // Yoshida 4th-order sub-step multipliers, computed as the reference computes
 // them (YoshidaCoefficients, engine/include/celestial/sim/yoshida.hpp:19-24)
 constexpr double kCbrt2 = 1.2599210498948732;
@@ -348,9 +359,12 @@ int sub_steps(int flags, double dt, double* sub) {
     return 3;
 }
 
+// Capture one device step (forces + second half kick) as a CUDA graph, or
+// reuse the captured one when nothing it depends on changed.  Per-stage
+// timing events are not recorded inside the graph.
 int step_graph(nb_engine* h, int flags, double dt, double eps) {
     const nb_engine::GraphKey key{flags,           h->n,           h->n_active,
-                                  h->leaf_cap,     dt,             eps,
+                                  h->leaf_cap,     h->group_span,  dt,             eps,
                                   h->theta,        h->group_pack,  h->mac_theta_lo,
                                   h->mac_theta_hi, h->mac_budget,  h->s.px};
     if (h->graph_exec && key == h->graph_key) return NB_OK;
@@ -595,6 +609,11 @@ NB_API int32_t nb_set_param_i32(nb_engine* h, int32_t p, int32_t v) {
             if (v < 1) return fail(h, NB_ERR_INVALID_ARG, "audit samples must be >= 1");
             h->mac_audit_samples = v;
             return NB_OK;
+        case NB_PARAM_GROUP_SPAN:
+            if (v != 0 && (v < 32 || v > 1024))
+                return fail(h, NB_ERR_INVALID_ARG, "group span must be 0 or 32..1024");
+            h->group_span = v;
+            return NB_OK;
         case NB_PARAM_GROUP_BODIES:
             if (v != 32) return fail(h, NB_ERR_INVALID_ARG, "group size must be 32");
             h->group_bodies = v;
@@ -618,6 +637,13 @@ NB_API int32_t nb_get_timings(const nb_engine* hc, double* out, int32_t n) {
         h->timings[NB_T_TRAVERSAL] = t[2];
         h->timings[NB_T_TOTAL] = t[0] + t[1] + t[2];
         h->ev_valid = false;
+    }
+    if (h->ev_collide) {
+        float tc = 0.f;
+        cudaEventSynchronize(h->ev[5]);
+        cudaEventElapsedTime(&tc, h->ev[4], h->ev[5]);
+        h->timings[NB_T_COLLIDE] = tc;
+        h->ev_collide = false;
     }
     for (int i = 0; i < n && i < NB_T_COUNT; i++) out[i] = h->timings[i];
     return NB_OK;
@@ -756,7 +782,12 @@ int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags)
         const double sdt = sub[k % ns];
         if ((r = force_pipeline(h, flags, softening, true, sdt))) return r;
         nb::launch_kick(h->st, h->n, h->s, sdt);
-        if (collide) {
+        // collisions are detected and resolved once per step, on the state at
+        // the end of the step (after the last Yoshida sub-step): the C# solver
+        // runs CollisionDetector after the whole integrator step
+        // (NBodySolver.cs:408-430) and the reference engine's GPU paths after
+        // the last sub-step (engine.cpp:1160-1190)
+        if (collide && k % ns == ns - 1) {
             nb::CollideArgs c{};
             c.n = h->n;
             c.n_active = h->n_active;
@@ -780,9 +811,16 @@ int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags)
             c.sms = h->sms;
             c.bbox_ord = h->scal->bbox_ord;
             c.n_active_dev = &h->scal->n_active;
+            // the second half kick moved no body: the force evaluation's tree
+            // (Barnes-Hut modes) still describes the positions
+            c.reuse_tree = h->tree_current;
             int npairs = 0, nmerge = 0, nkept = 0;
+            record(h, 4);
             if ((r = nb::collide_step(h->st, h->col, c, &npairs, &nmerge, &nkept)))
                 return fail(h, r, "collision step failed");
+            record(h, 5);
+            h->ev_collide = h->timing != 0;
+            h->tree_current = false;  // the state rows are compacted below
             std::swap(h->s, h->s_alt);
             h->n = nkept;
             h->n_active = nkept;
@@ -907,6 +945,8 @@ NB_API int32_t nb_diagnostics(nb_engine* h, double softening, int32_t pe_mode, d
         a.groups = h->groups;
         a.n_groups = &sc->n_groups;
         a.pack = h->group_pack;
+    a.group_span = h->group_span;
+        a.group_span = h->group_span;
         a.counters = nullptr;
         a.err = sc->err;
         nb::walk_group(h->st, h->wcfg, a, true, false, true);
@@ -1297,6 +1337,7 @@ NB_API int32_t nb_mac_harvest(nb_engine* h, int32_t max_records, double sample_f
     a.groups = h->groups;
     a.n_groups = &sc->n_groups;
     a.pack = h->group_pack;
+    a.group_span = h->group_span;
     a.counters = sc->counters;
     a.err = sc->err;
     a.theta2 = h->mac_theta_lo * h->mac_theta_lo;

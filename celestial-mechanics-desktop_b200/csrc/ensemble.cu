@@ -574,6 +574,7 @@ void enqueue_forces(nb_ensemble* h, double eps) {
         a.groups = h->groups;
         a.n_groups = &sc->n_groups;
         a.pack = 2.25;
+        a.group_span = 0;
         a.counters = sc->counters;
         a.err = sc->err;
         a.sys_root = h->d_root;

@@ -806,10 +806,36 @@ __global__ void k_find_groups(TreeBufs t, int2* __restrict__ groups, int* __rest
     if (run_cnt) groups[atomicAdd(n_groups, 1)] = make_int2(run_first, run_cnt);
 }
 
+// Span grouping: the walk-tree nodes holding at most `span` bodies whose
+// parent holds more ("span cells"; the root when it holds at most span, and
+// leaf buckets of coincident keys that hold more) are cut into runs of 32
+// consecutive sorted bodies, the last run taking the rest.  Every warp lane
+// then holds a body (a full group, or a short tail group that the walk
+// replicates over the warp), while a group's box stays inside its span
+// cell, which holds at most `span` bodies: a group can never enclose a dense
+// region it does not belong to.
+__global__ void k_find_groups_span(TreeBufs t, int2* __restrict__ groups,
+                                   int* __restrict__ n_groups, int span) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= *t.n_nodes) return;
+    const int4 lk = t.link[w];
+    if (lk.w > span && lk.y != 0) return;  // an internal node above the span cells
+    const int pb = t.parent_bin[w];
+    if (pb >= 0) {
+        const int pw = t.walk_index[pb];
+        if (t.link[pw].w <= span) return;  // inside a span cell: its ancestor cuts it
+    }
+    for (int off = 0; off < lk.w; off += 32)
+        groups[atomicAdd(n_groups, 1)] = make_int2(lk.z + off, min(32, lk.w - off));
+}
+
 void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n, int2* groups,
-                 int* n_groups, double pack) {
+                 int* n_groups, double pack, int span) {
     cudaMemsetAsync(n_groups, 0, sizeof(int), st);
-    if (n > 0)
+    if (n <= 0) return;
+    if (span >= 32)
+        k_find_groups_span<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, groups, n_groups, span);
+    else
         k_find_groups<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, groups, n_groups, pack);
 }
 
@@ -869,7 +895,7 @@ void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, b
                 bool pot, int mac) {
     if (a.n <= 0) return;
     a.front_cap = cfg.front_cap;
-    find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack);
+    find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack, a.group_span);
     cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
     if (mac == kMacHarvest) {
         k_walk_group<true, false, false, false, kMacHarvest>

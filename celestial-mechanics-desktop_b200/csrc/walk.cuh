@@ -23,6 +23,8 @@ struct WalkArgs {
     int2* groups;               // walk groups: body_first, body_count (<= 32)
     int* n_groups;
     double pack;                // sibling packing box-growth limit (0: no packing)
+    int group_span;             // >= 32: runs of 32 bodies inside cells of <= group_span
+                                // bodies (find_groups); otherwise sibling packing
     // learned MAC / harvest
     const float* samag;         // |a| of each sorted body from the previous step
     const MacDev* mac;          // network image (learned mode)
@@ -48,11 +50,15 @@ struct WalkConfig {
 };
 
 void walk_init(int sms, WalkConfig& cfg);
-// Walk groups: the octree nodes holding <= 32 bodies whose parent holds
-// more (spatially compact sets of consecutive sorted bodies), plus 32-body
-// slices of level-21 buckets that hold more than 32.  groups: >= n entries.
+// Walk groups (sets of at most 32 consecutive sorted bodies), groups: >= n
+// entries.  span >= 32: every walk-tree node holding at most `span` bodies
+// whose parent holds more is cut into runs of 32 consecutive bodies.
+// Otherwise: the octree nodes holding <= 32 bodies whose parent holds more,
+// runs of such siblings packed while the packed box stays within `pack`
+// times the larger part's (0: no packing), plus 32-body slices of level-21
+// buckets that hold more than 32.
 void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n, int2* groups,
-                 int* n_groups, double pack);
+                 int* n_groups, double pack, int span);
 size_t walk_front_bytes(const WalkConfig& cfg);
 // Group walk, FP32 monopole(+quadrupole) on FP64-differenced coordinates.
 // mac: 0 geometric, 1 harvest, 2 learned (1 and 2 need quad, no shell, no

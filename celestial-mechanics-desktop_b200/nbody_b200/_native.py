@@ -37,6 +37,8 @@ FLAG_COLLISIONS = 0x40
 FLAG_LEARNED_MAC = 0x80
 FLAG_YOSHIDA4 = 0x100
 FLAG_ADAPTIVE_DT = 0x200
+FLAG_ORDER_SIMD = 0x400
+FLAG_ORDER_PAIRWISE = 0x800
 # parameters
 PARAM_THETA = 1
 PARAM_LEAF_CAPACITY = 2
@@ -58,9 +60,10 @@ PARAM_MAC_AUDIT_RMS = 17
 PARAM_ADAPTIVE_ETA = 18
 PARAM_ADAPTIVE_DT_MIN = 19
 PARAM_ADAPTIVE_DT_MAX = 20
+PARAM_GROUP_SPAN = 21
 ENS_SHAPES = [(64, 1), (64, 2), (64, 4), (128, 1), (128, 2), (128, 4), (256, 1), (256, 2), (256, 4)]
 # timings / counters
-T_BUILD, T_TRAVERSAL, T_TOTAL, T_SORT, T_TREE, T_COUNT = range(6)
+T_BUILD, T_TRAVERSAL, T_TOTAL, T_SORT, T_TREE, T_COLLIDE, T_COUNT = range(7)
 (C_CELL_INTERACTIONS, C_BODY_INTERACTIONS, C_NODES, C_ACTIVE, C_PAIRS, C_MERGES, C_OVERFLOWS, C_GROUPS,
  C_MAX_GROUP_WORK, C_MAC_EVALS, C_MAC_AUDITS, C_MAC_FALLBACK, C_COUNT) = range(13)
 

@@ -79,6 +79,21 @@ enum nb_mode {
  * current dt is read with nb_get_adaptive_dt.  Steps run one by one (no
  * captured graph: dt changes every step). */
 #define NB_FLAG_ADAPTIVE_DT 0x200
+/* NB_MODE_DIRECT_FP64 only: the rounding and summation order of another of
+ * the desktop app's CPU backends instead of CpuParallelBackend's, so that a
+ * user of that backend gets its bits.
+ *   NB_FLAG_ORDER_SIMD: SimdSingleThreadBackend (SimdSingleThreadBackend.cs:
+ *     43-165), which is also the native engine's CPU brute force
+ *     (Engine::compute_cpu_brute_forces, engine/src/sim/engine.cpp:649-674):
+ *     coefficient m * ((inv * inv) * inv), sources summed in row order.
+ *   NB_FLAG_ORDER_PAIRWISE: CpuSingleThreadBackend's Newton's-third-law loop
+ *     (CpuSingleThreadBackend.cs:50-159): the same coefficient; a body's
+ *     acceleration is its running sum over lower rows plus its running sum
+ *     over higher rows.
+ * With NB_FLAG_SHELL_THEOREM those backends run CpuParallelBackend's
+ * arithmetic, and so do these flags. */
+#define NB_FLAG_ORDER_SIMD 0x400
+#define NB_FLAG_ORDER_PAIRWISE 0x800
 
 /* Parameter ids for nb_set_param_f64 / nb_set_param_i32. */
 enum nb_param {
@@ -118,7 +133,13 @@ enum nb_param {
      * simulation_config.hpp:73-79); setting one restarts from nb_step's dt */
     NB_PARAM_ADAPTIVE_ETA = 18,    /* f64, safety factor eta (default 0.01)                  */
     NB_PARAM_ADAPTIVE_DT_MIN = 19, /* f64, floor (default 1e-8)                               */
-    NB_PARAM_ADAPTIVE_DT_MAX = 20  /* f64, ceiling (default 0.01)                             */
+    NB_PARAM_ADAPTIVE_DT_MAX = 20, /* f64, ceiling (default 0.01)                             */
+    NB_PARAM_GROUP_SPAN = 21       /* i32, 0 or 32..1024: walk groups are runs of 32
+                                      consecutive sorted bodies cut from the walk-tree cells
+                                      holding at most this many bodies whose parent holds
+                                      more (full warps; a group's box stays inside a cell of
+                                      at most this many bodies); 0: octree cells of <= 32
+                                      bodies with NB_PARAM_GROUP_PACK sibling packing       */
 };
 
 /* Indices into nb_get_timings() output (milliseconds, CUDA events).
@@ -130,7 +151,9 @@ enum nb_timing {
     NB_T_TOTAL = 2,     /* whole last force evaluation            */
     NB_T_SORT = 3,      /* keys + radix sort                      */
     NB_T_TREE = 4,      /* radix tree + octree + multipoles       */
-    NB_T_COUNT = 5
+    NB_T_COLLIDE = 5,   /* last collision stage: broad phase, merges,
+                           compaction (NB_FLAG_COLLISIONS)        */
+    NB_T_COUNT = 6
 };
 
 /* Indices into nb_get_counters() output. */

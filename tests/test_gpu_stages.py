@@ -95,6 +95,28 @@ def test_octree_topology_reference_code(engine, ref_lib):
     assert gpu_canonical(t) == ref_canonical(ref_lib.ref_octree(b.px, b.py, b.pz, b.mass, b.active))
 
 
+@pytest.mark.parametrize("n,seed,inactive", [(5000, 21, 7), (1_048_576, 1, 0)])
+def test_octree_topology_reference_code_at_scale(engine, ref_lib, n, seed, inactive):
+    """The walk tree (leaf capacity 1) against the reference's own
+    OctreeBuilder (oracle/_ref) up to the Barnes-Hut workload's size: the
+    Plummer sphere of 1,048,576 bodies, seed 1.  Compared at depths <= 21
+    (keys of 21 bits per axis): every (depth, cell, body count) node and
+    every body's leaf cell.  Mismatch classes: bodies a few ulp from a cell
+    plane, and everything else; both must be empty."""
+    from helpers import topology_mismatches
+
+    b = scenarios.plummer(n, 1.0, 1.0, seed=seed)
+    if inactive:
+        b.active[3::inactive] = 0
+    cube = ref_lib.cube_from_bbox(ref_lib.bbox(b.px, b.py, b.pz, b.active))
+    t = engine.build_octree(b.px, b.py, b.pz, b.mass, b.active, leaf_capacity=1, cube=cube)
+    ref = ref_lib.ref_octree(b.px, b.py, b.pz, b.mass, b.active)
+    mm = topology_mismatches(ref, t, b.px, b.py, b.pz)
+    assert mm["cells"] == 0 and mm["bodies"] == 0, mm
+    if n <= 5000:  # the vectorised form agrees with the set-of-bodies form
+        assert gpu_canonical(t) == ref_canonical(ref)
+
+
 def test_octree_single_body_and_duplicates(engine, oracle):
     t = engine.build_octree(np.array([1.0]), np.array([2.0]), np.array([3.0]), np.array([10.0]),
                             np.ones(1, np.uint8), leaf_capacity=8)

@@ -237,6 +237,64 @@ def test_merge_and_compaction_step_bit_exact(engine, oracle):
     np.testing.assert_allclose(got.radius, out["radius"][keep], rtol=5e-16)
 
 
+def test_merge_and_compaction_at_disk_size(engine, oracle):
+    """The collisional-disk workload's size, 262,144 bodies + the central
+    mass, radii scaled 100x (2,093 overlapping pairs at the start, so the
+    64-per-frame and 2-per-body caps both bind): a dt = 0 step with
+    collisions gives the oracle's pair count, merges (sequential
+    CollisionResolver semantics) and compacted state, bit for bit (merged
+    radii to cbrt's 1 ulp).  The oracle's broad phase is the all-pairs test,
+    split over the host's threads."""
+    d = scenarios.collisional_disk(262_144, seed=2, radius_scale=100.0)
+    engine.set_state(d, old_acc=False)
+    engine.step(1, 0.0, 1e-4, MODE_BARNES_HUT | FLAG_SHELL_THEOREM | FLAG_COLLISIONS)
+    c = engine.counters()
+    got, ids = engine.get_state()
+    lo, hi = oracle.broad_phase(d.px, d.py, d.pz, d.radius, d.active, d.collidable,
+                                nthreads=oracle.threads())
+    out, nm = oracle.resolve_merges(bodies_dict(d), lo, hi)
+    assert len(lo) > 1000 and nm == 64
+    assert c[N.C_PAIRS] == len(lo) and c[N.C_MERGES] == nm
+    dest, kept = oracle.compact_indices(out["active"], out["mass"])
+    assert len(ids) == kept == d.n - nm
+    keep = np.nonzero(dest >= 0)[0]
+    np.testing.assert_array_equal(ids, keep)
+    for k in ("px", "py", "pz", "vx", "vy", "vz", "mass"):
+        np.testing.assert_array_equal(getattr(got, k), out[k][keep], err_msg=k)
+    np.testing.assert_allclose(got.radius, out["radius"][keep], rtol=5e-16)
+
+
+def test_yoshida4_with_merges_once_per_step(engine, oracle):
+    """Yoshida4 with collisions: the three sub-steps run without collisions,
+    then one broad phase, merge and compaction on the state at the end of the
+    step (as the C# solver detects after its whole integrator step and the
+    reference engine's GPU paths after the last sub-step).  Equal to the
+    oracle's Yoshida4 step followed by its broad phase, merges and
+    compaction; the merge count is that step's."""
+    d = scenarios.collisional_disk(3000, seed=14, radius_scale=2500.0)
+    d.ax, d.ay, d.az = oracle.direct_forces(d.px, d.py, d.pz, d.mass, d.active, 1e-4)
+    b = bodies_dict(d)
+    engine.set_param(N.PARAM_MAX_MERGES_FRAME, 64)
+    engine.set_state(d, old_acc=True)
+    dt = 2e-3
+    engine.step(1, dt, 1e-4, MODE_DIRECT_FP64 | FLAG_YOSHIDA4 | FLAG_COLLISIONS)
+    c = engine.counters()
+    got, ids = engine.get_state()
+    y = oracle.yoshida_direct(b, 1e-4, dt, 1)
+    y["active"] = d.active.copy()
+    y["radius"] = d.radius.copy()
+    y["density"] = b["density"].copy()
+    lo, hi = oracle.broad_phase(y["px"], y["py"], y["pz"], y["radius"], y["active"],
+                                d.collidable)
+    out, nm = oracle.resolve_merges(y, lo, hi)
+    assert nm > 0 and c[N.C_MERGES] == nm and c[N.C_PAIRS] == len(lo)
+    dest, kept = oracle.compact_indices(out["active"], out["mass"])
+    keep = np.nonzero(dest >= 0)[0]
+    np.testing.assert_array_equal(ids, keep)
+    for k in ("px", "py", "pz", "vx", "vy", "vz", "mass"):
+        np.testing.assert_array_equal(getattr(got, k), out[k][keep], err_msg=k)
+
+
 def test_collisional_steps_conserve_mass_and_momentum(engine):
     d = scenarios.collisional_disk(20_000, seed=2, radius_scale=1500.0)
     engine.set_state(d, old_acc=False)
