@@ -77,16 +77,20 @@ extern "C" NB_API int32_t nb_sort_pairs_noalloc(uint64_t* keys, int32_t* values,
     if (r != NB_OK) return r;
     cudaStream_t st = (cudaStream_t)stream;
     int* err = (int*)(d.base + kErrOff);
-    // the error word must start clear; sort_pairs clears its own histogram,
-    // tile-counter and look-back words before use
+    // The array keeps the previous call's contents: the error word must start
+    // clear; sort_pairs clears its own histogram, tile-counter and look-back
+    // words before use.  Only this call's own memsets, launches and copies are
+    // checked: an error that earlier, unrelated work left pending in the CUDA
+    // runtime is neither reported as this call's nor cleared.
     if (cudaMemsetAsync(err, 0, sizeof(int) * nb::kErrCount, st) != cudaSuccess) return NB_ERR_CUDA;
-    nb::sort_pairs(st, n, keys, (uint32_t*)values, (uint64_t*)(d.base + kAltKeysOff),
-                   (uint32_t*)(d.base + kAltValsOff), d.base + kWsOff, false, err, d.sms);
+    if (nb::sort_pairs(st, n, keys, (uint32_t*)values, (uint64_t*)(d.base + kAltKeysOff),
+                       (uint32_t*)(d.base + kAltValsOff), d.base + kWsOff, false, err,
+                       d.sms) != cudaSuccess)
+        return NB_ERR_CUDA;
     int host_err[nb::kErrCount] = {0, 0, 0, 0};
     if (cudaMemcpyAsync(host_err, err, sizeof(host_err), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return NB_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return NB_ERR_CUDA;
-    if (cudaGetLastError() != cudaSuccess) return NB_ERR_CUDA;
     if (host_err[nb::kErrTimeout]) return NB_ERR_TIMEOUT;
     return NB_OK;
 }

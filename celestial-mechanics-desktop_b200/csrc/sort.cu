@@ -197,30 +197,49 @@ const void* k_sort_pass_ptr() { return (const void*)k_sort_pass; }
 // Sort n pairs.  Data starts in (k0, v0); the result ends in (k0, v0) (8
 // passes, even count).  ws: sort_workspace_bytes(capacity) bytes.  When
 // `hist_ready` the 8x256 histograms at the head of ws are already filled (by
-// the fused Morton kernel); otherwise they are computed here.
-void sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1,
-                void* ws, bool hist_ready, int* err, int sms) {
-    if (n <= 1) return;
+// the fused Morton kernel); otherwise they are computed here.  Returns the
+// first failing status among this call's own memsets and launches (the
+// launches go through cudaLaunchKernelEx, whose return value belongs to that
+// launch alone, so an error left pending by earlier unrelated work is
+// neither reported nor cleared here).
+cudaError_t sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint64_t* k1,
+                       uint32_t* v1, void* ws, bool hist_ready, int* err, int sms) {
+    if (n <= 1) return cudaSuccess;
     uint32_t* hist = (uint32_t*)ws;
     uint32_t* ctr = hist + 8 * 256;
     uint32_t* look = ctr + 8;
     const int tiles = ceil_div(n, kSortTile);
+    cudaError_t e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.stream = st;
     if (!hist_ready) {
-        cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, st);
-        int grid = min(ceil_div(n, 256 * 8), sms * 8);
-        k_sort_histogram<<<grid, 256, 0, st>>>(n, k0, hist);
+        if ((e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, st)) != cudaSuccess) return e;
+        cfg.gridDim = dim3(min(ceil_div(n, 256 * 8), sms * 8));
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = 0;
+        if ((e = cudaLaunchKernelEx(&cfg, k_sort_histogram, n, (const uint64_t*)k0, hist)) !=
+            cudaSuccess)
+            return e;
     }
-    cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * (8 + (size_t)8 * tiles * 256), st);
+    if ((e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * (8 + (size_t)8 * tiles * 256), st)) !=
+        cudaSuccess)
+        return e;
     uint64_t* ks = k0;
     uint32_t* vs = v0;
     uint64_t* kd = k1;
     uint32_t* vd = v1;
+    cfg.gridDim = dim3(tiles);
+    cfg.blockDim = dim3(kSortThreads);
+    cfg.dynamicSmemBytes = kSortDynSmem;
     for (int p = 0; p < 8; p++) {
-        k_sort_pass<<<tiles, kSortThreads, kSortDynSmem, st>>>(n, 8 * p, ks, vs, kd, vd, hist + 256 * p,
-                                                   look + (size_t)p * tiles * 256, ctr + p, err);
+        if ((e = cudaLaunchKernelEx(&cfg, k_sort_pass, n, 8 * p, (const uint64_t*)ks,
+                                    (const uint32_t*)vs, kd, vd, (const uint32_t*)(hist + 256 * p),
+                                    look + (size_t)p * tiles * 256, ctr + p, err)) != cudaSuccess)
+            return e;
         uint64_t* tk = ks; ks = kd; kd = tk;
         uint32_t* tv = vs; vs = vd; vd = tv;
     }
+    return cudaSuccess;
 }
 
 }  // namespace nb

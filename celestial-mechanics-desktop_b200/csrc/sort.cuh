@@ -6,7 +6,8 @@ namespace nb {
 
 void sort_init();
 size_t sort_workspace_bytes(int capacity);
-void sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint64_t* k1, uint32_t* v1,
-                void* ws, bool hist_ready, int* err, int sms);
+// Returns the first failing status of the call's own memsets and launches.
+cudaError_t sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint64_t* k1,
+                       uint32_t* v1, void* ws, bool hist_ready, int* err, int sms);
 
 }  // namespace nb

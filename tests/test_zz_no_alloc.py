@@ -5,8 +5,9 @@ by their own pool allocator, or they sit on a latency-critical path where a
 device-wide synchronising allocation is not allowed).  They pass device
 buffers they already own.  This test owns those buffers through torch (the
 caller's allocator), calls the entry point through the C ABI twice in a row
-on different inputs, and checks each result bit for bit against the
-existing nb_sort_pairs entry point (integer work: exact).
+on different inputs, and checks each result bit for bit (integer work:
+exact) against the existing nb_sort_pairs entry point and against the
+oracle's stable sort, which shares no code with the CUDA kernels.
 
 The file is named so that pytest collects it last.
 """
@@ -34,7 +35,7 @@ def _sort_on_device(keys: np.ndarray, vals: np.ndarray):
     return dk.cpu().numpy().view(np.uint64), dv.cpu().numpy()
 
 
-def test_noalloc_sort_matches_existing_entry_point_twice():
+def test_noalloc_sort_matches_existing_entry_point_twice(oracle):
     from nbody_b200 import Engine
 
     rng = np.random.Generator(np.random.PCG64(77))
@@ -50,6 +51,9 @@ def test_noalloc_sort_matches_existing_entry_point_twice():
             want_k, want_v = e.sort_pairs(keys, vals)
             np.testing.assert_array_equal(got_k, want_k)
             np.testing.assert_array_equal(got_v, want_v)
+            ork, orv = oracle.stable_sort(keys, vals)
+            np.testing.assert_array_equal(got_k, ork)
+            np.testing.assert_array_equal(got_v, orv)
 
 
 def test_noalloc_sort_rejects_sizes_beyond_the_maximum():
