@@ -204,14 +204,21 @@ def reference_bh_seconds(b, threads: int) -> tuple[float, str]:
 
 
 def run_reference(args, ws, rank):
+    """The reference's own CPU Barnes-Hut (oracle/_ref: BarnesHutSolver with
+    its job system on all host threads, theta 0.5, monopole, FP64) on the
+    headline input: W untimed and K timed full force evaluations, and its
+    force error on the same 4096 sampled bodies the engine's arms are judged
+    on.  Only the scenario generator of the package is imported, so the
+    engine library is never loaded in this process."""
     if rank != 0:
         return
+    import oracle
     from nbody_b200 import scenarios
 
     b = scenarios.plummer(args.n, 1.0, 1.0, seed=SEED)
     threads = os.cpu_count() or 1
-    warm = min(args.warmup, 1)
-    steps = max(1, min(args.steps, 3))
+    warm, steps = max(args.warmup, 0), max(1, args.steps)
+    acc = None
     for _ in range(warm):
         reference_bh_seconds(b, threads)
     total = 0.0
@@ -220,8 +227,19 @@ def run_reference(args, ws, rank):
         s, kind = reference_bh_seconds(b, threads)
         total += s
     value = steps / total
-    sample = (f"N=1,048,576 Plummer seed 1: {steps} full force evaluations (serial tree build + "
-              f"parallel walk, theta 0.5, monopole), {warm} warm-up")
+    # force error of the reference's evaluation against the FP64 direct sum
+    # on the engine's audit sample (nb_force_error's draw, restated)
+    if oracle.ref() is not None:
+        acc, _, _ = oracle.ref_bh_forces(b.px, b.py, b.pz, b.mass, b.active, EPS, THETA, True,
+                                         threads)
+    else:
+        acc = oracle.bh_forces(b.px, b.py, b.pz, b.mass, b.active, EPS, THETA, nthreads=threads)
+    t = scenarios.sample_rows(b.active, ERR_SAMPLES, ERR_SEED).astype(np.int32)
+    want = oracle.direct_forces_targets(b.px, b.py, b.pz, b.mass, b.active, EPS, t,
+                                        nthreads=threads)
+    err = oracle.force_error((acc[0][t], acc[1][t], acc[2][t]), want)
+    sample = (f"N={args.n:,} Plummer seed 1: {steps} full force evaluations (serial tree build "
+              f"+ parallel walk, theta 0.5, monopole), {warm} warm-up")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * total / steps,
@@ -229,6 +247,9 @@ def run_reference(args, ws, rank):
         "data": "synthetic (seeded Plummer sphere)",
         "config": {"workload": workload_name(args.n), "n": args.n, "theta": THETA, "eps": EPS,
                    "multipole": "monopole (reference)", "mac": "geometric"},
+        "force_error": {"mean": err[0], "max": err[1], "rms": err[2],
+                        "vs": f"FP64 direct sum, the same {ERR_SAMPLES} sampled bodies as the "
+                              "engine's arms"},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
@@ -333,7 +354,7 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
     deterministic, so both passes evaluate identical steps)."""
     import torch
 
-    acc = dict(walk=0.0, build=0.0, sort=0.0, tree=0.0, inter=0, flops=0.0, evals=0)
+    acc = dict(walk=0.0, build=0.0, sort=0.0, tree=0.0, inter=0, flops=0.0, evals=0, groups=0)
     eng.set_state(b, old_acc=False)
     eng.step(1, 0.0, EPS, mode_geo)
     eng.step(max(args.warmup, 3), DT, EPS, flags)
@@ -348,6 +369,7 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
         acc["inter"] += int(c[N.C_CELL_INTERACTIONS] + c[N.C_BODY_INTERACTIONS])
         acc["flops"] += FLOPS_CELL_QUAD * c[N.C_CELL_INTERACTIONS] + FLOPS_BODY * c[N.C_BODY_INTERACTIONS]
         acc["evals"] += int(c[N.C_MAC_EVALS])
+        acc["groups"] += int(c[N.C_GROUPS])
 
     clocks = Clocks(dev)
     clocks.start()
@@ -392,16 +414,21 @@ def timed_arm(eng, b, stream, args, ws, dev, flags, N, mode_geo, label):
            "force_error": {"mean": err[0], "max": err[1], "rms": err[2]},
            "stage_ms": {s: acc[s] / k for s in ("build", "walk", "sort", "tree")},
            "walk_flops_per_step": acc["flops"] / k, "network_rows_per_step": acc["evals"] / k,
+           "walk_groups_per_step": acc["groups"] / k,
+           "group_fill": (int(c[N.C_ACTIVE]) / (acc["groups"] / k) / 32.0
+                          if acc["groups"] else None),
            "clocks": clk, "audit": audit_state}
     return out
 
 
-def run_b200(args, ws, rank, local):
+def run_b200(args, ws, rank, local, trained=None):
     """Learned vs geometric MAC at a fixed force error on one system: the
-    network is trained on the GPU, the geometric theta and the learned budget
-    are each set to the loosest value whose rms relative force error against
-    the FP64 direct sum stays <= 1e-3, and both are timed; theta = 0.5 (the
-    plain Barnes-Hut configuration) is timed beside them."""
+    network is trained on the GPU (or, given `trained` = (parameters,
+    screen) from an earlier run, loaded), the geometric theta and the learned
+    budget are each set to the loosest value whose rms relative force error
+    against the FP64 direct sum stays <= 1e-3, and both are timed; theta = 0.5
+    (the plain Barnes-Hut configuration) is timed beside them.  Returns the
+    line (rank 0) and the trained (parameters, screen)."""
     import torch
 
     from nbody_b200 import FLAG_LEARNED_MAC, MODE_BARNES_HUT, Engine, scenarios
@@ -415,10 +442,18 @@ def run_b200(args, ws, rank, local):
     b = (scenarios.hernquist(n, 1.0, 1.0, seed=4) if big else
          scenarios.plummer(n, 1.0, 1.0, seed=SEED))
     eng = Engine(max(n, N_BODIES), device=dev)
+    if args.group_span is not None:
+        eng.set_param(N.PARAM_GROUP_SPAN, int(args.group_span))
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     geo, learned = MODE_BARNES_HUT, MODE_BARNES_HUT | FLAG_LEARNED_MAC
 
-    train = train_learned_mac(eng, N, scenarios, log)
+    if trained is None:
+        train = train_learned_mac(eng, N, scenarios, log)
+    else:
+        eng.mac_set_params(trained[0])
+        eng.mac_set_screen(trained[1])
+        train = {"loaded": "the network trained in this run's headline line"}
+    trained_out = (eng.mac_get_params(), eng.mac_get_screen())
     theta_g, rms_g, scan_g = calibrate(eng, b, N, N.PARAM_THETA, THETA_GRID, geo, geo, log)
     budget, rms_l, scan_l = calibrate(eng, b, N, N.PARAM_MAC_BUDGET, BUDGET_GRID, learned, geo, log)
 
@@ -524,6 +559,8 @@ def run_b200(args, ws, rank, local):
                                                         "uniformly sampled bodies, last step"),
             "learned": {"budget_log10": budget, "calibration_rms": rms_l,
                         "network_rows_per_step": arm_l["network_rows_per_step"],
+                        "walk_groups_per_step": arm_l["walk_groups_per_step"],
+                        "group_fill": arm_l["group_fill"],
                         "audit_in_timed_region": arm_l["audit"],
                         "stage_ms": arm_l["stage_ms"], "training": train, "scan": scan_l},
             "geometric_same_error": {k: arm_g[k] for k in ("steps_per_s", "ms_per_step",
@@ -563,7 +600,7 @@ def run_b200(args, ws, rank, local):
             "clocks": clk,
         }
     eng.close()
-    return line
+    return line, trained_out
 
 
 def run_theta05(args, ws, rank, local):
@@ -584,6 +621,8 @@ def run_theta05(args, ws, rank, local):
     n = args.n
     b = scenarios.plummer(n, 1.0, 1.0, seed=SEED)
     eng = Engine(n, device=dev)
+    if args.group_span is not None:
+        eng.set_param(N.PARAM_GROUP_SPAN, int(args.group_span))
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     eng.set_param(N.PARAM_THETA, THETA)
     arm = timed_arm(eng, b, stream, args, ws, dev, mode, N, mode,
@@ -901,6 +940,7 @@ def run_ds1000(args, ws, rank, local):
     ms, clk = _timed_steps(eng, stream, steps, dt, eps, MODE_DIRECT_FP64, dev, ws)
     e1 = eng.diagnostics(eps)["e"]
     drift = (e1 - e0) / abs(e0)
+    final, _ = eng.get_state()
     line = None
     if rank == 0:
         d = {k: getattr(b, k) for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az",
@@ -911,9 +951,12 @@ def run_ds1000(args, ws, rank, local):
         w = oracle.verlet_direct(d, eps, dt, cpu_steps, nthreads=threads) if cpu_steps else None
         cpu_s = time.perf_counter() - t
         cpu_drift = None
+        same = None
         if w is not None:
             w["active"] = b.active
             cpu_drift = (oracle.energy(w, eps)["e"] - oracle.energy(d, eps)["e"]) / abs(e0)
+            same = all(np.array_equal(getattr(final, k), w[k])
+                       for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az"))
         line = {"metric": METRIC, "value": steps / (ms / 1e3), "unit": "steps/s", "n_gpus": ws,
                 "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -921,6 +964,7 @@ def run_ds1000(args, ws, rank, local):
                 "config": {"workload": "ds_plummer_1000", "n": n, "eps": eps, "dt": dt,
                            "seed": 0, "force": "direct sum FP64, CpuParallelBackend rounding"},
                 "energy_drift": drift, "cpu_energy_drift": cpu_drift,
+                "trajectory_bit_identical_to_cpu": same,
                 "pairs_per_s": n * (n - 1) * steps / (ms / 1e3),
                 "cpu_baseline": None if w is None else {
                     "value": steps / cpu_s, "unit": "steps/s", "cores": threads, "kind": "port",
@@ -957,8 +1001,15 @@ def run_disk(args, ws, rank, local):
     eng.set_state(d, old_acc=False)
     p0 = eng.diagnostics(eps, pe_mode=1)
     ms, clk = _timed_steps(eng, stream, steps, dt, eps, flags, dev, ws)
+    # stage times of one more instrumented step (CUDA events): force
+    # evaluation stages and the collision stage (broad phase on the force
+    # evaluation's tree, merges, compaction)
     p1 = eng.diagnostics(eps, pe_mode=1)
     st, ids = eng.get_state()
+    eng.step(1, dt, eps, flags)
+    tm = eng.timings()
+    stage_ms = {"sort": tm[N.T_SORT], "tree": tm[N.T_TREE], "walk": tm[N.T_TRAVERSAL],
+                "collide": tm[N.T_COLLIDE]}
     line = None
     if rank == 0:
         dp = np.sqrt(sum((p1[k] - p0[k]) ** 2 for k in ("px", "py", "pz")))
@@ -974,7 +1025,8 @@ def run_disk(args, ws, rank, local):
                 "merges_per_1000_steps_frac": (n + 1 - len(ids)) / (n + 1) * 1000.0 / steps,
                 "energy_drift": (p1["e"] - p0["e"]) / abs(p0["e"]),
                 "momentum_drift_abs": dp, "momentum_scale": pn,
-                "mass_drift": (p1["m"] - p0["m"]) / p0["m"], "clocks": clk}
+                "mass_drift": (p1["m"] - p0["m"]) / p0["m"], "stage_ms": stage_ms,
+                "clocks": clk}
         if ws == 1 and not args.no_cpu_baseline:
             # the reference's own Barnes-Hut force evaluation of the initial
             # disk on all host threads (theta 0.5, monopole); the collision
@@ -1000,6 +1052,95 @@ def run_disk(args, ws, rank, local):
     return line
 
 
+def _sub_args(args, workload, steps, **kw):
+    a = argparse.Namespace(**vars(args))
+    a.workload, a.steps, a.n = workload, steps, N_BODIES
+    a.warmup = 3
+    a.long_steps = 0
+    for k, v in kw.items():
+        setattr(a, k, v)
+    return a
+
+
+def _med_clock(line):
+    c = (line or {}).get("clocks") or {}
+    return {"sm_mhz": c.get("sm_mhz"), "reasons": c.get("reasons")}
+
+
+def config_summaries(args, ws, rank, local, trained, log):
+    """Every other configuration of the benchmark suite, each at its own
+    step count, summarised beside the headline line: the FP64 direct sum
+    N=1000 (10,000 steps), the FP32 direct sum at N=2^20, the collisional
+    disk (1000 steps), the 512-system ensemble (1000 steps) and the learned
+    vs geometric MAC on the N=4,194,304 Hernquist sphere (50 steps)."""
+    out = {}
+    t0 = time.perf_counter()
+    ln = run_ds1000(_sub_args(args, "ds1000", 10_000), ws, rank, local)
+    if ln:
+        out["ds1000"] = {
+            "steps_per_s": ln["value"], "ms_per_step": ln["ms_per_step"], "steps": ln["steps"],
+            "n": 1000, "dtype": "f64", "pairs_per_s": ln["pairs_per_s"],
+            "energy_drift": ln["energy_drift"], "cpu_energy_drift": ln["cpu_energy_drift"],
+            "trajectory_bit_identical_to_cpu": ln["trajectory_bit_identical_to_cpu"],
+            "cpu_baseline": ln["cpu_baseline"], "clocks": _med_clock(ln)}
+    log(f"configs: ds1000 done ({time.perf_counter() - t0:.1f} s)")
+    ln = run_theta05(_sub_args(args, "direct32", 3), ws, rank, local)
+    if ln:
+        r = ln["roofline"]
+        clk = ln["clocks"].get("sm_mhz")
+        out["direct32"] = {
+            "n": ln["config"]["n"], "ms_per_evaluation": ln["ms_per_step"],
+            "tflops": r["achieved"], "frac": r["frac"],
+            "frac_peak": "SMs x 128 FMA lanes x 2 flop x max SM clock (20 flop per pair)",
+            "frac_at_median_clock": (r["frac"] * (peaks()[0].get("sm_max_mhz", 1965.0) / clk)
+                                     if clk else None),
+            "force_error": ln["force_error"], "cpu_baseline": ln.get("cpu_baseline"),
+            "clocks": _med_clock(ln)}
+    log(f"configs: direct32 done ({time.perf_counter() - t0:.1f} s)")
+    ln = run_disk(_sub_args(args, "disk", 1000), ws, rank, local)
+    if ln:
+        out["disk"] = {k: ln[k] for k in ("value", "ms_per_step", "steps", "bodies_left",
+                                          "merged", "merges_per_1000_steps_frac",
+                                          "energy_drift", "momentum_drift_abs", "momentum_scale",
+                                          "mass_drift")}
+        out["disk"]["steps_per_s"] = out["disk"].pop("value")
+        out["disk"]["n"] = ln["config"]["n"]
+        out["disk"]["stage_ms"] = ln.get("stage_ms")
+        out["disk"]["cpu_baseline"] = ln.get("cpu_baseline")
+        out["disk"]["clocks"] = _med_clock(ln)
+    log(f"configs: disk done ({time.perf_counter() - t0:.1f} s)")
+    ln = run_ensemble(_sub_args(args, "ensemble", 1000), ws, rank, local)
+    if ln:
+        out["ensemble"] = {
+            "steps_per_s": ln["value"], "ms_per_step": ln["ms_per_step"], "steps": ln["steps"],
+            "systems": ln["config"]["systems"], "bodies": ln["config"]["bodies"],
+            "interactions_per_s": ln["interactions_per_s"], "force_error": ln["force_error"],
+            "energy_drift": ln["energy_drift"], "autotune": ln["autotune"],
+            "cpu_baseline": ln["cpu_baseline"], "e2e": ln["e2e"], "clocks": _med_clock(ln)}
+    log(f"configs: ensemble done ({time.perf_counter() - t0:.1f} s)")
+    ln, _ = run_b200(_sub_args(args, "mac4m", 50, no_cpu_baseline=True), ws, rank, local,
+                     trained=trained)
+    if ln:
+        out["mac4m"] = {
+            "n": ln["config"]["n"], "steps": ln["steps"],
+            "learned_steps_per_s": ln["value"],
+            "learned_rms": ln["force_error"]["rms"],
+            "learned_budget_log10": ln["learned"]["budget_log10"],
+            "geometric_steps_per_s": ln["geometric_same_error"]["steps_per_s"],
+            "geometric_rms": ln["geometric_same_error"]["force_error"]["rms"],
+            "geometric_theta": ln["geometric_same_error"]["theta"],
+            "learned_over_geometric_steps": ln["learned_over_geometric_steps"],
+            "theta_0_5_steps_per_s": ln["geometric_theta_0_5"]["steps_per_s"],
+            "walk_frac_fp32": ln["roofline"]["frac"],
+            "interactions_per_step": {"learned": ln["interactions_per_step"],
+                                      "geometric": ln["geometric_same_error"]
+                                      ["interactions_per_step"]},
+            "clocks": _med_clock(ln)}
+    log(f"configs: mac4m done ({time.perf_counter() - t0:.1f} s)")
+    out["wall_s"] = time.perf_counter() - t0
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1008,6 +1149,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--group-span", type=int, default=None,
+                    help="walk groups: runs of 32 bodies cut from cells of at most this many "
+                         "bodies (NB_PARAM_GROUP_SPAN; 0 = sibling packing)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="bh1m: skip the other configurations' summaries")
     ap.add_argument("--long-steps", type=int, default=1000,
                     help="bh1m: steps of the audited long run after the timed arms (0 = skip)")
     ap.add_argument("--n", type=int, default=N_BODIES,
@@ -1016,7 +1162,8 @@ def main():
                     choices=["bh1m", "mac4m", "theta05", "direct32", "ensemble", "ds1000",
                              "disk", "compact4m"],
                     help="bh1m: the headline line, learned vs geometric MAC at rms <= 1e-3 on "
-                         "the N=1,048,576 Plummer sphere; mac4m: the same on the N=4,194,304 "
+                         "the N=1,048,576 Plummer sphere, with every other configuration "
+                         "summarised under `configs`; mac4m: the same on the N=4,194,304 "
                          "Hernquist sphere; theta05: plain geometric theta 0.5 only; direct32: "
                          "FP32 direct sum on the same sphere; ensemble: "
                          "512 Plummer systems, 1000 steps; ds1000: FP64 direct sum N=1000, 10k "
@@ -1027,6 +1174,7 @@ def main():
         args.steps = {"bh1m": 100, "mac4m": 50, "theta05": 100, "direct32": 3, "ensemble": 1000,
                       "ds1000": 10_000, "disk": 1000, "compact4m": 10}[args.workload]
     ws, rank, local = dist_setup()
+    log = (lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank)
@@ -1048,11 +1196,19 @@ def main():
             if line is not None:
                 print(json.dumps(line))
         else:
-            line = run_b200(args, ws, rank, local)
+            line, trained = run_b200(args, ws, rank, local)
             if line is not None:
                 # the learned arm adds one kernel per step (per-node screen terms)
                 # and its audit three (FP64 targets, chunk reduction, gather)
                 line["gpu_launches"] = (launches_per_step() + 1) * args.steps + 3
+            if args.workload == "bh1m" and not args.no_configs:
+                if ws == 1:
+                    cfg = config_summaries(args, ws, rank, local, trained, log)
+                else:
+                    cfg = {"skipped": "the other configurations are summarised at n_gpus = 1"}
+                if line is not None:
+                    line["configs"] = cfg
+            if line is not None:
                 print(json.dumps(line))
     finally:
         if ws > 1:

@@ -185,3 +185,30 @@ def ensemble(systems: int = 512, seed: int = 3) -> list[Bodies]:
     """Independent Plummer systems (scale 1 AU, 1 Msun each) of log-uniform size."""
     sizes = ensemble_sizes(systems, seed=seed)
     return [plummer(int(k), 1.0, 1.0, seed=seed * 100003 + s) for s, k in enumerate(sizes)]
+
+
+def sample_rows(active: np.ndarray, ns: int, seed: int) -> np.ndarray:
+    """The bodies nb_force_error samples: the first `ns` entries of a
+    SplitMix64-driven partial Fisher-Yates shuffle of the active rows in
+    index order (all active rows when ns <= 0 or ns >= their count).  The
+    shuffle is kept sparse (only displaced positions are stored), so a few
+    thousand draws from millions of rows cost milliseconds."""
+    cand = np.flatnonzero(np.asarray(active) != 0)
+    na = len(cand)
+    if ns <= 0 or ns >= na:
+        return cand.copy()
+    mask = (1 << 64) - 1
+    x = int(seed) & mask
+    moved: dict[int, int] = {}
+    out = np.empty(ns, np.int64)
+    for k in range(ns):
+        x = (x + 0x9E3779B97F4A7C15) & mask
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        z ^= z >> 31
+        j = k + z % (na - k)
+        vk, vj = moved.get(k, k), moved.get(j, j)
+        moved[k], moved[j] = vj, vk
+        out[k] = cand[vj]
+    return out
