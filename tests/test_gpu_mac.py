@@ -3,8 +3,11 @@ walk's inference routine against the CPU oracle, and the harvest -> train ->
 learned-walk pipeline.
 
 Tolerances: gradients agree with the oracle (same BF16 rounding points,
-float64 sums) to 2e-2 relative in norm per parameter block; predictions to
-2e-2 in normalised units (FP32 accumulation order only)."""
+float64 sums) to 2e-3 relative in norm per parameter block: what is left is
+FP32 against float64 accumulation and the rare element whose FP32 value sits
+on a BF16 rounding boundary and rounds the other way (one BF16 ulp, 2^-8,
+of that element); predictions to 2e-2 in normalised units (FP32
+accumulation order only)."""
 from __future__ import annotations
 
 import numpy as np
@@ -32,11 +35,12 @@ def test_training_gradient_matches_oracle(engine):
     engine.mac_set_params(np.concatenate([p, norm]))
     g, loss = engine.mac_gradient(X, Y)
     wl, wg, _ = M.forward_backward(p, norm, X, Y, bf=True)
-    assert loss == pytest.approx(wl, rel=2e-3)
+    assert loss == pytest.approx(wl, rel=1e-4)
+    errs = []
     for lo, hi in ((M.W1, M.B1), (M.B1, M.W2), (M.W2, M.B2), (M.B2, M.W3), (M.W3, M.B3),
                    (M.B3, M.NPARAM)):
-        e = np.linalg.norm(g[lo:hi] - wg[lo:hi]) / max(np.linalg.norm(wg[lo:hi]), 1e-30)
-        assert e < 2e-2, (lo, hi, e)
+        errs.append(np.linalg.norm(g[lo:hi] - wg[lo:hi]) / max(np.linalg.norm(wg[lo:hi]), 1e-30))
+    assert max(errs) < 2e-3, errs
 
 
 def test_training_is_bitwise_reproducible():
