@@ -726,6 +726,7 @@ def run_ensemble(args, ws, rank, local):
     ens = Ensemble(sizes, ds_max_n=ENS_DS_MAX, device=dev)
     ens.set_state(systems)
     shape, shape_ms = ens.autotune(EPS)
+    tree_choice, tree_ms = ens.autotune_tree(EPS)
     e0, _, _ = ens.energy(EPS)
     ens.step(max(args.warmup, 3), ENS_DT, EPS)
     ens.set_state(systems)
@@ -812,7 +813,12 @@ def run_ensemble(args, ws, rank, local):
             "interactions_per_step": {"direct_pairs": c["direct_pairs"],
                                       "tree_cell": c["tree_cell"], "tree_body": c["tree_body"]},
             "autotune": {"shape": list(__import__("nbody_b200")._native.ENS_SHAPES[shape]),
-                         "ms_per_shape": [round(float(x), 4) for x in shape_ms]},
+                         "ms_per_shape": [round(float(x), 4) for x in shape_ms],
+                         "tree": {"choice": list(__import__("nbody_b200")._native
+                                                 .ENS_TREE_CHOICES[tree_choice]),
+                                  "choices": "(walk block shape 0: 8 warps x 3, 1: 4 warps x 6; "
+                                             "walk-group span)",
+                                  "ms_per_choice": [round(float(x), 4) for x in tree_ms]}},
             "force_error": {"direct_rms_max": float(rms[small].max()),
                             "direct_rms_median": float(np.median(rms[small])),
                             "tree_rms_max": float(rms[~small].max()) if (~small).any() else None,

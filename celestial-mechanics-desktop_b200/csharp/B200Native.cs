@@ -35,7 +35,7 @@ internal static unsafe class B200Native
         ParamMacThetaHi = 12, ParamMacScreenQuantile = 13, ParamEnsDirectShape = 14,
         ParamMacAuditInterval = 15, ParamMacAuditSamples = 16, ParamMacAuditRms = 17,
         ParamAdaptiveEta = 18, ParamAdaptiveDtMin = 19, ParamAdaptiveDtMax = 20,
-        ParamGroupSpan = 21;
+        ParamGroupSpan = 21, ParamEnsWalkShape = 22;
 
     // enum nb_timing, enum nb_counter
     public const int TBuild = 0, TTraversal = 1, TTotal = 2, TSort = 3, TTree = 4, TCollide = 5,
@@ -44,7 +44,7 @@ internal static unsafe class B200Native
         CPairs = 4, CMerges = 5, COverflows = 6, CGroups = 7, CMaxGroupWork = 8, CMacEvals = 9,
         CMacAudits = 10, CMacFallback = 11, CCount = 12;
 
-    public const int MacParams = 4801, MacNorm = 18, MacScreen = 10;
+    public const int MacParams = 4801, MacNorm = 18, MacScreen = 10, EnsTreeChoices = 8;
     public const int NoAllocSortMax = 1048576;
 
     // ---- lifetime ---------------------------------------------------------
@@ -135,6 +135,8 @@ internal static unsafe class B200Native
         double softening);
     [DllImport(Lib)] public static extern int nb_ens_autotune(IntPtr h, double softening,
         int* shape, double* msPerShape);
+    [DllImport(Lib)] public static extern int nb_ens_autotune_tree(IntPtr h, double softening,
+        int* choice, double* msPerChoice);
     [DllImport(Lib)] public static extern int nb_ens_force_error(IntPtr h, int samples, ulong seed,
         double softening, double* rms, double* maxErr);
     [DllImport(Lib)] public static extern int nb_ens_energy(IntPtr h, double softening,

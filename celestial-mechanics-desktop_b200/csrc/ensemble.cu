@@ -391,6 +391,8 @@ struct nb_ensemble {
     int ds_max_n = 2048;
     double theta = 0.5;
     int leaf_cap = 8;
+    int walk_shape = 0;                   // tree branch: walk block shape (0: 8 warps, 1: 4)
+    int group_span = 0;                   // tree branch: walk-group span (0: sibling packing)
     int shape = 4;                        // direct tile shape (128 x 2 until tuned)
     int shape_blocks[nb::kNumShapes] = {0};  // resident blocks per SM of each shape
     // device
@@ -420,7 +422,7 @@ struct nb_ensemble {
     // graph of one step
     cudaGraphExec_t graph = nullptr;
     double g_dt = 0, g_eps = -1, g_theta = -1;
-    int g_shape = -1;
+    int g_shape = -1, g_walk = -1, g_span = -1;
     // counters of the last evaluation
     long long ds_pairs = 0;
     long long bh_cell = 0, bh_body = 0;
@@ -528,18 +530,10 @@ void launch_cubes(nb_ensemble* h) {
                                                 h->d_com);
 }
 
-// Forces at the current positions: the direct branch on the second stream,
-// the tree branch on the first; the first stream waits for both.
-void enqueue_forces(nb_ensemble* h, double eps) {
+// The tree branch: keys, sort, tree and walk of all tree systems on `st`.
+void launch_tree(nb_ensemble* h, cudaStream_t st, double eps) {
     EnsScal* sc = h->scal;
-    launch_cubes(h);
-    cudaEventRecord(h->ev_fork, h->st);
-    cudaStreamWaitEvent(h->st2, h->ev_fork, 0);
-    launch_direct(h, h->st2, eps);
-    cudaEventRecord(h->ev_join, h->st2);
-    cudaMemsetAsync(sc->counters, 0, sizeof(sc->counters), h->st);
     if (h->n_bh > 0) {
-        cudaStream_t st = h->st;
         const int n = h->n_bh;
         const double4* cubes = h->d_cubes + h->nds;  // tree systems follow the direct ones
         const double* half16 = h->d_half16 + h->nds;
@@ -574,14 +568,41 @@ void enqueue_forces(nb_ensemble* h, double eps) {
         a.groups = h->groups;
         a.n_groups = &sc->n_groups;
         a.pack = 2.25;
-        a.group_span = 0;
+        a.group_span = h->group_span;
         a.counters = sc->counters;
         a.err = sc->err;
         a.sys_root = h->d_root;
-        nb::walk_group(st, h->wcfg, a, true, false, false, 0);
+        nb::walk_group(st, h->wcfg, a, true, false, false, 0, h->walk_shape);
     }
+}
+
+// Forces at the current positions: the direct branch on the second stream,
+// the tree branch on the first; the first stream waits for both.
+void enqueue_forces(nb_ensemble* h, double eps) {
+    EnsScal* sc = h->scal;
+    launch_cubes(h);
+    cudaEventRecord(h->ev_fork, h->st);
+    cudaStreamWaitEvent(h->st2, h->ev_fork, 0);
+    launch_direct(h, h->st2, eps);
+    cudaEventRecord(h->ev_join, h->st2);
+    cudaMemsetAsync(sc->counters, 0, sizeof(sc->counters), h->st);
+    launch_tree(h, h->st, eps);
     cudaStreamWaitEvent(h->st, h->ev_join, 0);
 }
+
+// Walk-group spans the tree autotuner tries (0: sibling packing); choice k
+// is walk shape k / 4 with span kEnsSpans[k % 4].
+constexpr int kEnsSpans[4] = {0, 64, 128, 256};
+
+// A span cell must lie inside one system: with span below the smallest tree
+// system's body count, a walk-tree node holding at most `span` bodies can
+// contain neither a whole system nor parts of two.
+int smallest_tree_system(const nb_ensemble* h) {
+    int m = 1 << 30;
+    for (int k = h->nds; k < h->nsys; k++) m = std::min(m, h->off[k + 1] - h->off[k]);
+    return m;
+}
+static_assert(NB_ENS_TREE_CHOICES == 8, "two walk shapes x four spans");
 
 void collect(nb_ensemble* h) {
     unsigned long long c[4] = {0, 0, 0, 0};
@@ -593,7 +614,7 @@ void collect(nb_ensemble* h) {
 
 int ens_graph(nb_ensemble* h, double dt, double eps) {
     if (h->graph && h->g_dt == dt && h->g_eps == eps && h->g_theta == h->theta &&
-        h->g_shape == h->shape)
+        h->g_shape == h->shape && h->g_walk == h->walk_shape && h->g_span == h->group_span)
         return NB_OK;
     if (h->graph) {
         cudaGraphExecDestroy(h->graph);
@@ -620,6 +641,8 @@ int ens_graph(nb_ensemble* h, double dt, double eps) {
     h->g_eps = eps;
     h->g_theta = h->theta;
     h->g_shape = h->shape;
+    h->g_walk = h->walk_shape;
+    h->g_span = h->group_span;
     return NB_OK;
 }
 
@@ -812,6 +835,20 @@ NB_API int32_t nb_ens_set_param_i32(nb_ensemble* h, int32_t p, int32_t v) {
         }
         return NB_OK;
     }
+    if (p == NB_PARAM_GROUP_SPAN) {
+        if (v != 0 && (v < 32 || v > 1024))
+            return efail(h, NB_ERR_INVALID_ARG, "group span must be 0 or 32..1024");
+        if (v != 0 && v >= smallest_tree_system(h))
+            return efail(h, NB_ERR_INVALID_ARG,
+                         "group span must be below the smallest tree system's body count");
+        h->group_span = v;
+        return NB_OK;
+    }
+    if (p == NB_PARAM_ENS_WALK_SHAPE) {
+        if (v < 0 || v > 1) return efail(h, NB_ERR_INVALID_ARG, "walk shape must be 0 or 1");
+        h->walk_shape = v;
+        return NB_OK;
+    }
     if (p == NB_PARAM_ENS_DIRECT_SHAPE) {
         if (v < 0 || v >= nb::kNumShapes)
             return efail(h, NB_ERR_INVALID_ARG, "shape must be 0..%d", nb::kNumShapes - 1);
@@ -935,6 +972,53 @@ NB_API int32_t nb_ens_autotune(nb_ensemble* h, double softening, int32_t* shape,
     return build_items(h, best);
 }
 
+NB_API int32_t nb_ens_autotune_tree(nb_ensemble* h, double softening, int32_t* choice,
+                                    double* ms_per_choice) {
+    if (!h || !(softening >= 0.0)) return NB_ERR_INVALID_ARG;
+    if (!h->has_state) return efail(h, NB_ERR_STATE, "no state set");
+    cudaSetDevice(h->device);
+    int best = 0;
+    float best_ms = 1e30f;
+    if (h->n_bh > 0) {
+        launch_cubes(h);  // the tree systems' cubes of the current positions
+        const int smallest = smallest_tree_system(h);
+        for (int k = 0; k < NB_ENS_TREE_CHOICES; k++) {
+            if (ms_per_choice) ms_per_choice[k] = -1.0;
+            if (kEnsSpans[k % 4] >= smallest) continue;  // could cross systems
+            h->walk_shape = k / 4;
+            h->group_span = kEnsSpans[k % 4];
+            launch_tree(h, h->st, softening);  // warm-up
+            float t = 1e30f;
+            for (int rep = 0; rep < 3; rep++) {
+                cudaEventRecord(h->ev_t0, h->st);
+                launch_tree(h, h->st, softening);
+                cudaEventRecord(h->ev_t1, h->st);
+                const int r = ens_check(h);
+                if (r) return r;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, h->ev_t0, h->ev_t1);
+                t = std::min(t, ms);
+            }
+            if (ms_per_choice) ms_per_choice[k] = t;
+            if (t < best_ms) {
+                best_ms = t;
+                best = k;
+            }
+        }
+    } else if (ms_per_choice) {
+        for (int k = 0; k < NB_ENS_TREE_CHOICES; k++) ms_per_choice[k] = -1.0;
+    }
+    h->walk_shape = best / 4;
+    h->group_span = kEnsSpans[best % 4];
+    if (choice) *choice = best;
+    // the accelerations of the tree systems come from the chosen configuration
+    if (h->n_bh > 0) {
+        launch_tree(h, h->st, softening);
+        return ens_check(h);
+    }
+    return NB_OK;
+}
+
 NB_API int32_t nb_ens_force_error(nb_ensemble* h, int32_t samples, uint64_t seed,
                                   double softening, double* rms, double* max_err) {
     if (!h || samples <= 0 || !rms || !(softening >= 0.0)) return NB_ERR_INVALID_ARG;
@@ -1018,7 +1102,7 @@ NB_API int32_t nb_ens_energy(nb_ensemble* h, double softening, double* energy, d
 NB_API int32_t nb_ens_get_counters(const nb_ensemble* h, int64_t* out, int32_t n) {
     if (!h || !out) return NB_ERR_INVALID_ARG;
     const int64_t v[] = {h->ds_pairs, h->bh_cell, h->bh_body, h->graph_launches, h->n_items,
-                         h->shape};
+                         h->shape, h->walk_shape, h->group_span};
     for (int i = 0; i < n && i < (int)(sizeof(v) / sizeof(v[0])); i++) out[i] = v[i];
     return NB_OK;
 }

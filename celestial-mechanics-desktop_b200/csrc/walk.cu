@@ -75,11 +75,23 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
 // with theta <= 2h/d < theta_hi is recorded for training); kMacLearned
 // (geometric below theta, open at or above theta_hi, the network decides in
 // between).
-template <bool QUAD, bool SHELL, bool POT, bool GUARD, int MAC>
-__global__ void __launch_bounds__((MAC == kMacLearned ? kMacWarps : kWalkWarps) * 32,
-                                  MAC == kMacLearned ? NB_WALK_MAC_BLOCKS : 3)
+// SHAPE (geometric walk only) selects the block shape: 0 = 8 warps x 3
+// blocks per SM, 1 = 4 warps x 6 blocks per SM (the same warps per SM in
+// smaller blocks; the ensembles' autotuner picks one).
+constexpr int kWalkWarpsSmall = 4;
+template <int MAC, int SHAPE>
+struct WalkShape {
+    static constexpr int warps =
+        MAC == kMacLearned ? kMacWarps : (SHAPE == 1 ? kWalkWarpsSmall : kWalkWarps);
+    static constexpr int min_blocks =
+        MAC == kMacLearned ? NB_WALK_MAC_BLOCKS : (SHAPE == 1 ? 6 : 3);
+};
+
+template <bool QUAD, bool SHELL, bool POT, bool GUARD, int MAC, int SHAPE = 0>
+__global__ void __launch_bounds__(WalkShape<MAC, SHAPE>::warps * 32,
+                                  WalkShape<MAC, SHAPE>::min_blocks)
 k_walk_group(WalkArgs a) {
-    constexpr int WARPS = MAC == kMacLearned ? kMacWarps : kWalkWarps;
+    constexpr int WARPS = WalkShape<MAC, SHAPE>::warps;
     extern __shared__ __align__(16) float s_walk[];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -874,6 +886,17 @@ void walk_init(int sms, WalkConfig& cfg) {
         &per_sm, k_walk_group<true, false, false, false, kMacGeometric>, kWalkThreads, kWalkSmem);
     if (per_sm < 1) per_sm = 1;
     cfg.blocks = sms * per_sm;
+    // the small-block shape of the quadrupole walk (ensembles)
+    for (int g = 0; g < 2; g++)
+        cudaFuncSetAttribute(g ? (const void*)k_walk_group<true, false, false, true, kMacGeometric, 1>
+                               : (const void*)k_walk_group<true, false, false, false, kMacGeometric, 1>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kWalkWarpsSmall * kWarpFloats * 4);
+    int per_sm_small = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm_small, k_walk_group<true, false, false, false, kMacGeometric, 1>,
+        kWalkWarpsSmall * 32, kWalkWarpsSmall * kWarpFloats * 4);
+    if (per_sm_small < 1) per_sm_small = 1;
     int per_sm_mac = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &per_sm_mac, k_walk_group<true, false, false, false, kMacLearned>, kMacWarps * 32,
@@ -884,6 +907,9 @@ void walk_init(int sms, WalkConfig& cfg) {
     cfg.blocks_mac = sms * per_sm_mac;
     if (cfg.blocks_mac * kMacWarps > cfg.blocks * kWalkWarps)
         cfg.blocks_mac = cfg.blocks * kWalkWarps / kMacWarps;
+    cfg.blocks_small = sms * per_sm_small;
+    if (cfg.blocks_small * kWalkWarpsSmall > cfg.blocks * kWalkWarps)
+        cfg.blocks_small = cfg.blocks * kWalkWarps / kWalkWarpsSmall;
     cfg.front_cap = 16384;
 }
 
@@ -892,7 +918,7 @@ size_t walk_front_bytes(const WalkConfig& cfg) {
 }
 
 void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,
-                bool pot, int mac) {
+                bool pot, int mac, int shape) {
     if (a.n <= 0) return;
     a.front_cap = cfg.front_cap;
     find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack, a.group_span);
@@ -905,6 +931,13 @@ void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, b
     if (mac == kMacLearned) {
         k_walk_group<true, false, false, false, kMacLearned>
             <<<cfg.blocks_mac, kMacWarps * 32, kWalkSmemMac, st>>>(a);
+        return;
+    }
+    if (shape == 1 && quad && !shell && !pot) {
+        const WalkKernel k = a.eps2 > 0.0
+                                 ? k_walk_group<true, false, false, false, kMacGeometric, 1>
+                                 : k_walk_group<true, false, false, true, kMacGeometric, 1>;
+        k<<<cfg.blocks_small, kWalkWarpsSmall * 32, kWalkWarpsSmall * kWarpFloats * 4, st>>>(a);
         return;
     }
     const WalkKernel k = pick_walk(quad, shell, pot, !(a.eps2 > 0.0));

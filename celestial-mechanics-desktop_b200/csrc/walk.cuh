@@ -46,6 +46,7 @@ struct WalkArgs {
 struct WalkConfig {
     int blocks;        // persistent grid size
     int blocks_mac;    // persistent grid size of the learned-MAC walk
+    int blocks_small;  // persistent grid size of the small-block geometric walk (shape 1)
     int front_cap;
 };
 
@@ -62,9 +63,11 @@ void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n
 size_t walk_front_bytes(const WalkConfig& cfg);
 // Group walk, FP32 monopole(+quadrupole) on FP64-differenced coordinates.
 // mac: 0 geometric, 1 harvest, 2 learned (1 and 2 need quad, no shell, no
-// potential, softening > 0).
+// potential, softening > 0).  shape (geometric quadrupole walk without shell
+// theorem or potential): 0 = blocks of 8 warps, 1 = blocks of 4 warps (the
+// same warps per SM).
 void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,
-                bool pot, int mac = 0);
+                bool pot, int mac = 0, int shape = 0);
 // Per-body FP64 walk with the reference's MAC, monopole, child order.
 void walk_reference(cudaStream_t st, WalkArgs a, bool shell);
 

@@ -90,6 +90,16 @@ class Ensemble:
         self._check(N.lib.nb_ens_autotune(self._h, float(softening), N.ptr(shape), N.ptr(ms)))
         return int(shape[0]), ms
 
+    def autotune_tree(self, softening: float):
+        """Fastest (walk block shape, walk-group span) of the tree branch on
+        the current state; returns (choice index into N.ENS_TREE_CHOICES,
+        ms per choice, -1 for choices not tried)."""
+        choice = np.zeros(1, np.int32)
+        ms = np.zeros(len(N.ENS_TREE_CHOICES))
+        self._check(N.lib.nb_ens_autotune_tree(self._h, float(softening), N.ptr(choice),
+                                               N.ptr(ms)))
+        return int(choice[0]), ms
+
     def force_error(self, samples: int, seed: int, softening: float):
         rms = np.zeros(len(self.sizes))
         mx = np.zeros(len(self.sizes))

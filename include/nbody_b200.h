@@ -134,6 +134,9 @@ enum nb_param {
     NB_PARAM_ADAPTIVE_ETA = 18,    /* f64, safety factor eta (default 0.01)                  */
     NB_PARAM_ADAPTIVE_DT_MIN = 19, /* f64, floor (default 1e-8)                               */
     NB_PARAM_ADAPTIVE_DT_MAX = 20, /* f64, ceiling (default 0.01)                             */
+    NB_PARAM_ENS_WALK_SHAPE = 22,  /* i32, ensembles: tree-branch walk block shape, 0 = 8 warps
+                                      x 3 blocks per SM, 1 = 4 warps x 6 (default 0), normally
+                                      set by nb_ens_autotune_tree                            */
     NB_PARAM_GROUP_SPAN = 21       /* i32, 0 or 32..1024: walk groups are runs of 32
                                       consecutive sorted bodies cut from the walk-tree cells
                                       holding at most this many bodies whose parent holds
@@ -415,6 +418,15 @@ NB_API int32_t nb_ens_step(nb_ensemble* h, int32_t n_steps, double dt, double so
  * the times, -1 for a shape that cannot run. */
 NB_API int32_t nb_ens_autotune(nb_ensemble* h, double softening, int32_t* shape,
                                double* ms_per_shape);
+/* Times the tree branch (keys, sort, tree, walk of every tree system) on the
+ * current state for each walk block shape (NB_PARAM_ENS_WALK_SHAPE 0, 1) and
+ * walk-group span (NB_PARAM_GROUP_SPAN 0, 64, 128, 256), 3 runs each with
+ * CUDA events, and keeps the fastest: choice k is shape k / 4 with the k % 4-th
+ * span.  ms_per_choice (NB_ENS_TREE_CHOICES entries, may be NULL) gets the
+ * times.  The tree systems' accelerations are then those of the choice. */
+#define NB_ENS_TREE_CHOICES 8
+NB_API int32_t nb_ens_autotune_tree(nb_ensemble* h, double softening, int32_t* choice,
+                                    double* ms_per_choice);
 /* Per system (in `sizes` order): rms and max relative error of the current
  * accelerations against an FP64 direct sum on up to `samples` bodies. */
 NB_API int32_t nb_ens_force_error(nb_ensemble* h, int32_t samples, uint64_t seed,
@@ -423,7 +435,8 @@ NB_API int32_t nb_ens_force_error(nb_ensemble* h, int32_t samples, uint64_t seed
 NB_API int32_t nb_ens_energy(nb_ensemble* h, double softening, double* energy, double* kinetic,
                              double* potential);
 /* direct pairs per evaluation, tree body-cell and body-body interactions of
- * the last evaluation, graph launches so far, direct work items, direct shape */
+ * the last evaluation, graph launches so far, direct work items, direct shape,
+ * tree walk shape, walk-group span */
 NB_API int32_t nb_ens_get_counters(const nb_ensemble* h, int64_t* out, int32_t n);
 /* Device time per step of the last nb_ens_step (or of the last evaluation). */
 NB_API int32_t nb_ens_get_timings(const nb_ensemble* h, double* ms_per_step);

@@ -167,3 +167,36 @@ def test_rejects_bad_input():
         b[1].px[3] = np.nan
         with pytest.raises(NBodyError):
             ens.set_state(b)
+
+
+def test_tree_autotune_choices_keep_systems_apart_and_accurate():
+    """nb_ens_autotune_tree times every (walk block shape, walk-group span)
+    it may use on the current state and keeps the fastest.  A span at or
+    above the smallest tree system's size is never tried (its groups could
+    take bodies of two systems) and is refused as a parameter; every tried
+    configuration gives each tree system its theta = 0.5 accuracy."""
+    sizes = [100, 2049, 3000, 5000, 8192]
+    systems = _systems(sizes, seed=6, spread=0.5)
+    with Ensemble(sizes, ds_max_n=2048) as ens:
+        ens.set_state(systems)
+        choice, ms = ens.autotune_tree(EPS)
+        assert 0 <= choice < len(N.ENS_TREE_CHOICES)
+        assert ms[choice] > 0 and ms[choice] == min(m for m in ms if m > 0)
+        # every span below 2049 is tried for both block shapes
+        assert np.all(ms > 0)
+        for k, (shape, span) in enumerate(N.ENS_TREE_CHOICES):
+            ens.set_param(N.PARAM_ENS_WALK_SHAPE, shape)
+            ens.set_param(N.PARAM_GROUP_SPAN, span)
+            ens.compute_forces(EPS)
+            errs = _per_system_errors(ens, systems)
+            for s, (rms, mx) in enumerate(errs):
+                bound = 1e-5 if sizes[s] <= 2048 else 1e-3
+                assert rms < bound, (k, s, rms)
+    with Ensemble([100, 300], ds_max_n=64) as small:
+        # tree systems of 100 and 300 bodies: spans of 128 and up are refused
+        with pytest.raises(Exception):
+            small.set_param(N.PARAM_GROUP_SPAN, 128)
+        small.set_param(N.PARAM_GROUP_SPAN, 64)
+        small.set_state(_systems([100, 300], seed=7))
+        choice, ms = small.autotune_tree(EPS)
+        assert ms[2] == -1 and ms[3] == -1 and ms[6] == -1 and ms[7] == -1
