@@ -11,17 +11,19 @@
 // (engine/src/physics/collision_resolver.cpp:8-18).
 //
 // Merge: the reference GPU kernel (resolve_merges_kernel.cu:43-194) resolves
-// pairs under try-locks, so which pairs merge depends on thread timing.
-// Pairs per step are few (the per-frame cap is 64), so the merge here runs
-// the CPU resolver's sequential semantics (collision_resolver.cpp:20-100,
-// 190-250) in pair order in one device thread: deterministic and identical
-// to the CPU reference.
+// pairs under try-locks, so which pairs merge depends on thread timing.  Here
+// the pairs are decided in parallel in conflict-free rounds (k_merge_rounds)
+// that reproduce the CPU resolver's sequential semantics
+// (collision_resolver.cpp:20-100, 190-250) bit for bit: deterministic and
+// identical to the CPU reference.
 //
 // Compaction: replaces the ~35-launch scan/scatter of compact_kernel.cu:
 // 191-407 (with a host scan above 262,144 bodies) by one kernel: warp ballot
 // / popc ranks, decoupled look-back across 4096-row tiles, and a scatter of
 // every state field.  Mask is_active && mass > 0 (compact_kernel.cu:39);
 // row order is preserved.
+#include <climits>
+
 #include "collide.cuh"
 #include "sort.cuh"
 
@@ -48,6 +50,7 @@ int collide_alloc(CollideBufs& b, int capacity, const std::function<int(void**, 
     if ((r = alloc((void**)&b.pair_vals_alt, sizeof(uint32_t) * b.pair_cap))) return r;
     if ((r = alloc((void**)&b.pair_sort_ws, sort_workspace_bytes(b.pair_cap)))) return r;
     if ((r = alloc((void**)&b.merge_count, sizeof(int) * (size_t)capacity))) return r;
+    if ((r = alloc((void**)&b.owner, sizeof(int) * (size_t)capacity))) return r;
     const size_t tiles = (size_t)ceil_div(capacity, kCompTile) + 1;
     if ((r = alloc((void**)&b.look, sizeof(uint32_t) * tiles))) return r;
     return alloc((void**)&b.tile_ctr, sizeof(uint32_t) * 4);
@@ -174,50 +177,137 @@ __device__ __forceinline__ double wavg(double ma, double a, double mb, double b,
 }
 
 // CollisionResolver::resolve in Merge mode (collision_resolver.cpp:20-100)
-// with resolve_merge (:190-250) and DensityModel (density_model.cpp:10-22).
-__global__ void k_merge_sequential(State s, const uint64_t* __restrict__ pairs, int np,
-                                   int max_frame, int max_body, int density_merge,
-                                   double min_radius, int* __restrict__ counts,
-                                   int* __restrict__ n_merges) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int total = 0;
-    for (int k = 0; k < np; k++) {
-        const int a = (int)(pairs[k] >> 32), b = (int)(pairs[k] & 0xFFFFFFFFu);
-        if (!s.active[a] || !s.active[b]) continue;
-        if (total >= max_frame) continue;
-        if (counts[a] >= max_body || counts[b] >= max_body) continue;
-        const double ma = s.mass[a], mb = s.mass[b];
-        const double M = __dadd_rn(ma, mb);
-        if (!(M < 1e-30)) {
-            const double vx = wavg(ma, s.vx[a], mb, s.vx[b], M);
-            const double vy = wavg(ma, s.vy[a], mb, s.vy[b], M);
-            const double vz = wavg(ma, s.vz[a], mb, s.vz[b], M);
-            const double x = wavg(ma, s.px[a], mb, s.px[b], M);
-            const double y = wavg(ma, s.py[a], mb, s.py[b], M);
-            const double z = wavg(ma, s.pz[a], mb, s.pz[b], M);
-            const int sv = (ma >= mb) ? a : b;
-            const int vc = (ma >= mb) ? b : a;
-            double rm;
-            if (density_merge) {
-                double sd = s.density[sv];
-                if (sd < 1e-30) sd = dm_density(s.mass[sv], s.radius[sv], min_radius);
-                rm = dm_radius(M, sd, min_radius);
-            } else {
-                const double ra = s.radius[a], rb = s.radius[b];
-                rm = cbrt(__dadd_rn(__dmul_rn(__dmul_rn(ra, ra), ra), __dmul_rn(__dmul_rn(rb, rb), rb)));
-            }
-            s.px[sv] = x; s.py[sv] = y; s.pz[sv] = z;
-            s.vx[sv] = vx; s.vy[sv] = vy; s.vz[sv] = vz;
-            s.mass[sv] = M;
-            s.radius[sv] = rm;
-            s.density[sv] = dm_density(M, rm, min_radius);
-            s.active[vc] = 0;
+// with resolve_merge (:190-250) and DensityModel (density_model.cpp:10-22):
+// pairs in sorted order; a pair is skipped when either body is inactive,
+// when max_frame merges happened before it, or when either body already took
+// part in max_body merges; otherwise the heavier body (the first on a tie)
+// takes the pair's mass, momentum-weighted velocity, mass-weighted position
+// and density-preserving radius, and the other becomes inactive.
+// The same resolver semantics with the pairs decided in parallel, bit for
+// bit the sequential loop's result.  One block takes the sorted pairs in
+// windows of kMergeThreads (one pair per thread) and resolves each window in
+// rounds.  In a round a pending pair is ready when it is the lowest pending
+// pair touching each of its two bodies (the `owner` words, reset for the
+// pending pairs' bodies and lowered by atomicMin): no earlier pending pair
+// can change its bodies' flags, counts, masses or positions any more, and the
+// ready pairs of a round touch disjoint bodies.  The per-frame cap depends on
+// the merges of all earlier pairs: with E merges among the resolved earlier
+// pairs and U earlier pairs still pending, the merge count at this pair lies
+// in [E, E + U]; the pair waits while that range straddles the cap.  The
+// lowest pending pair is always ready with U = 0, so every round resolves at
+// least one pair; after max_frame merges every later pair is a skip.
+constexpr int kMergeThreads = 1024;
+
+__device__ __forceinline__ void merge_pair(State& s, int a, int b, int density_merge,
+                                           double min_radius, int* counts) {
+    const double ma = s.mass[a], mb = s.mass[b];
+    const double M = __dadd_rn(ma, mb);
+    if (!(M < 1e-30)) {
+        const double vx = wavg(ma, s.vx[a], mb, s.vx[b], M);
+        const double vy = wavg(ma, s.vy[a], mb, s.vy[b], M);
+        const double vz = wavg(ma, s.vz[a], mb, s.vz[b], M);
+        const double x = wavg(ma, s.px[a], mb, s.px[b], M);
+        const double y = wavg(ma, s.py[a], mb, s.py[b], M);
+        const double z = wavg(ma, s.pz[a], mb, s.pz[b], M);
+        const int sv = (ma >= mb) ? a : b;
+        const int vc = (ma >= mb) ? b : a;
+        double rm;
+        if (density_merge) {
+            double sd = s.density[sv];
+            if (sd < 1e-30) sd = dm_density(s.mass[sv], s.radius[sv], min_radius);
+            rm = dm_radius(M, sd, min_radius);
+        } else {
+            const double ra = s.radius[a], rb = s.radius[b];
+            rm = cbrt(__dadd_rn(__dmul_rn(__dmul_rn(ra, ra), ra), __dmul_rn(__dmul_rn(rb, rb), rb)));
         }
-        const int surv = (s.mass[a] > 0 && s.active[a]) ? a : b;
-        counts[surv]++;
-        total++;
+        s.px[sv] = x; s.py[sv] = y; s.pz[sv] = z;
+        s.vx[sv] = vx; s.vy[sv] = vy; s.vz[sv] = vz;
+        s.mass[sv] = M;
+        s.radius[sv] = rm;
+        s.density[sv] = dm_density(M, rm, min_radius);
+        s.active[vc] = 0;
     }
-    *n_merges = total;
+    const int surv = (s.mass[a] > 0 && s.active[a]) ? a : b;
+    counts[surv]++;
+}
+
+// Exclusive count of `flag` over the threads before this one in the block,
+// and the block's total.  All threads call it.
+__device__ __forceinline__ int block_excl_count(bool flag, int* s_warp, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, flag);
+    __syncthreads();  // s_warp may still be read by the previous call
+    if (lane == 0) s_warp[warp] = __popc(m);
+    __syncthreads();
+    int off = 0, tot = 0;
+    for (int w = 0; w < kMergeThreads / 32; w++) {
+        const int c = s_warp[w];
+        if (w < warp) off += c;
+        tot += c;
+    }
+    *total = tot;
+    return off + __popc(m & lanemask_lt());
+}
+
+__global__ void __launch_bounds__(kMergeThreads)
+k_merge_rounds(State s, const uint64_t* __restrict__ pairs, int np, int max_frame, int max_body,
+               int density_merge, double min_radius, int* __restrict__ counts,
+               int* __restrict__ owner, int* __restrict__ n_merges, int* err) {
+    __shared__ int s_warp[kMergeThreads / 32];
+    const int t = threadIdx.x;
+    int merged = 0;  // merges of the finished windows (the same in every thread)
+    for (int base = 0; base < np && merged < max_frame; base += kMergeThreads) {
+        const int k = base + t;
+        bool pending = k < np;
+        bool event = false;  // this pair merged (or counted as a merge)
+        int a = 0, b = 0;
+        if (pending) {
+            const uint64_t pk = pairs[k];
+            a = (int)(pk >> 32);
+            b = (int)(pk & 0xFFFFFFFFu);
+        }
+        int left = 0;
+        block_excl_count(pending, s_warp, &left);
+        for (int round = 0; left > 0; round++) {
+            if (round > kMergeThreads) {  // cannot happen: a round resolves >= 1 pair
+                if (t == 0) dev_flag(err, kErrTimeout);
+                break;
+            }
+            if (pending) {
+                owner[a] = INT_MAX;
+                owner[b] = INT_MAX;
+            }
+            __syncthreads();
+            if (pending) {
+                atomicMin(&owner[a], k);
+                atomicMin(&owner[b], k);
+            }
+            __syncthreads();
+            const bool ready = pending && owner[a] == k && owner[b] == k;
+            int tot_unused = 0;
+            const int pend_before = block_excl_count(pending, s_warp, &tot_unused);
+            const int ev_before = block_excl_count(event, s_warp, &tot_unused);
+            if (ready) {
+                const int E = merged + ev_before;
+                if (!s.active[a] || !s.active[b] || E >= max_frame) {
+                    pending = false;  // a skip, whatever the cap
+                } else if (E + pend_before < max_frame) {
+                    pending = false;
+                    if (counts[a] < max_body && counts[b] < max_body) {
+                        merge_pair(s, a, b, density_merge, min_radius, counts);
+                        event = true;
+                    }
+                }
+                // otherwise the cap is undecided: wait for the earlier pairs
+            }
+            __syncthreads();  // this round's merges are visible to the next
+            block_excl_count(pending, s_warp, &left);
+        }
+        int ev_total = 0;
+        block_excl_count(event, s_warp, &ev_total);
+        merged += ev_total;
+    }
+    if (t == 0) *n_merges = merged < max_frame ? merged : max_frame;
 }
 
 // ---- compaction ---------------------------------------------------------
@@ -328,9 +418,9 @@ int collide_step(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* npairs, i
     cudaMemsetAsync(a.n_merges, 0, sizeof(int), st);
     if (w > 0) {
         cudaMemsetAsync(b.merge_count, 0, sizeof(int) * (size_t)a.n, st);
-        k_merge_sequential<<<1, 32, 0, st>>>(a.s, b.pair_keys, w, a.max_frame, a.max_body,
-                                             a.density_merge, a.min_radius, b.merge_count,
-                                             a.n_merges);
+        k_merge_rounds<<<1, kMergeThreads, 0, st>>>(a.s, b.pair_keys, w, a.max_frame,
+                                                    a.max_body, a.density_merge, a.min_radius,
+                                                    b.merge_count, b.owner, a.n_merges, a.err);
     }
     launch_compact(st, b, a.n, a.s, a.s_alt, nullptr, true, a.n_kept, a.err);
     int host[2] = {0, 0};

@@ -15,6 +15,7 @@ struct CollideBufs {
     uint32_t* pair_vals_alt;
     void* pair_sort_ws;
     int* merge_count;      // per row, merges this step
+    int* owner;            // per row, the lowest pending pair touching it (merge rounds)
     uint32_t* look;        // compaction look-back words
     uint32_t* tile_ctr;
     int capacity;
