@@ -15,7 +15,8 @@ CSRC = HERE / "csrc"
 LIB = HERE / "libnbody_b200.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = ["engine.cu", "bodies.cu", "sort.cu", "tree.cu", "walk.cu", "direct.cu", "diag.cu",
-           "collide.cu", "noalloc.cu", "mac.cu", "ensemble.cu", "celestial_compat.cu"]
+           "collide.cu", "noalloc.cu", "mac.cu", "mac_tc.cu", "ensemble.cu",
+           "celestial_compat.cu"]
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "--extended-lambda", "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared",
          "-cudart", "shared"]

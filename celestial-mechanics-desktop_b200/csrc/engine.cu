@@ -1593,8 +1593,8 @@ NB_API int32_t nb_mac_train(nb_engine* h, int32_t epochs, int32_t batch, double 
         cudaMemsetAsync(h->mac_loss, 0, sizeof(float), h->st);
         for (int row0 = 0; row0 < n; row0 += batch) {
             const int rows = std::min(batch, n - row0);
-            nb::mac_grad(h->st, h->mac_X, h->mac_Y, order, row0, rows, h->mac_dev, h->mac_ti,
-                         h->mac_G, h->mac_loss, h->sms, h->mac_part);
+            nb::mac_grad(h->st, h->mac_X, h->mac_Y, order, row0, rows, h->mac_P, h->mac_dev,
+                         h->mac_ti, h->mac_G, h->mac_loss, h->sms, h->mac_part, h->scal->err);
             nb::mac_adam(h->st, h->mac_P, h->mac_G, h->mac_m, h->mac_v, ++h->mac_adam_step, (float)lr);
             nb::mac_image(h->st, h->mac_P, h->mac_norm, h->mac_dev, h->mac_ti);
         }
@@ -1653,8 +1653,8 @@ NB_API int32_t nb_mac_gradient(nb_engine* h, const float* X, const float* Y, int
         !(r = upload(h, dY, Y, sizeof(float) * (size_t)n)) &&
         !(r = upload(h, dO, ord.data(), sizeof(int) * (size_t)n))) {
         cudaMemsetAsync(h->mac_loss, 0, sizeof(float), h->st);
-        nb::mac_grad(h->st, dX, dY, dO, 0, n, h->mac_dev, h->mac_ti, h->mac_G, h->mac_loss, h->sms,
-                     h->mac_part);
+        nb::mac_grad(h->st, dX, dY, dO, 0, n, h->mac_P, h->mac_dev, h->mac_ti, h->mac_G,
+                     h->mac_loss, h->sms, h->mac_part, h->scal->err);
         float l = 0.f;
         if (!(r = download(h, grad, h->mac_G, sizeof(float) * nb::kMacParams)) &&
             !(r = download(h, &l, h->mac_loss, sizeof(float))) && !(r = check_device(h)) && loss)

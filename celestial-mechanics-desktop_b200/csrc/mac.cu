@@ -402,12 +402,13 @@ __global__ void k_mac_adam(float* __restrict__ P, const float* __restrict__ G, f
 size_t mac_grad_partial_bytes(int sms) { return sizeof(float) * (size_t)kAccFloats * sms * 4; }
 
 void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order, int row0,
-              int nrows, const MacDev* w, const MacTrainImage* ti, float* grad, float* loss,
-              int sms, float* part) {
+              int nrows, const float* P, const MacDev* w, const MacTrainImage* ti, float* grad,
+              float* loss, int sms, float* part, int* err) {
     if (nrows <= 0) {
         cudaMemsetAsync(grad, 0, sizeof(float) * kMacParams, st);
         return;
     }
+#ifdef NB_MAC_TRAIN_WARP_MMA
     // per call: the attribute belongs to the current device, and handles on
     // several devices share this function (a host-side call of a microsecond)
     cudaFuncSetAttribute((const void*)k_mac_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -416,6 +417,18 @@ void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order,
     const int blocks = min(ceil_div(tiles, kTrainWarps), sms * 4);
     k_mac_train<<<blocks, kTrainWarps * 32, kTrainSmem, st>>>(X, Y, order, row0, nrows, w, ti,
                                                                1.f / (float)nrows, part);
+    (void)P;
+    (void)err;
+#else
+    (void)ti;
+    // tcgen05: one CTA per SM (its shared memory admits one), tiles of 128 rows
+    cudaFuncSetAttribute((const void*)k_mac_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)mac_train_tc_smem());
+    const int tiles = (nrows + 127) / 128;
+    const int blocks = min(tiles, sms);
+    k_mac_train_tc<<<blocks, 128, mac_train_tc_smem(), st>>>(
+        X, Y, order, row0, nrows, P, w, 1.f / (float)nrows, part, kAccFloats, kAccLoss, err);
+#endif
     k_mac_grad_reduce<<<ceil_div(kMacParams + 1, 256), 256, 0, st>>>(blocks, part, grad, loss);
 }
 

@@ -30,9 +30,18 @@ void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w, Ma
 // to *loss.  part: mac_grad_partial_bytes(sms) of scratch.  The result is
 // bitwise reproducible (no floating-point atomics).
 size_t mac_grad_partial_bytes(int sms);
+// P: the FP32 master parameters (the tensor-core kernel stages W1, W2 from
+// them as BF16); err: the device error word (a bounded wait that expired).
 void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order, int row0,
-              int nrows, const MacDev* w, const MacTrainImage* ti, float* grad, float* loss,
-              int sms, float* part);
+              int nrows, const float* P, const MacDev* w, const MacTrainImage* ti, float* grad,
+              float* loss, int sms, float* part, int* err);
+// The tcgen05 training kernel (mac_tc.cu): one CTA of 128 threads per SM.
+__global__ void k_mac_train_tc(const float* __restrict__ X, const float* __restrict__ Y,
+                               const int* __restrict__ order, int row0, int nrows,
+                               const float* __restrict__ P, const MacDev* __restrict__ w,
+                               float inv_batch, float* __restrict__ part, int acc_floats,
+                               int loss_index, int* err);
+size_t mac_train_tc_smem();
 void mac_adam(cudaStream_t st, float* P, const float* G, float* m, float* v, int step, float lr);
 void mac_predict(cudaStream_t st, const float* X, int n, const MacDev* w, float* out);
 // Per walk-tree node (2n slots, *t.n_nodes used): screen term and log2 mass.

@@ -60,6 +60,11 @@ constexpr int kWalkSmemMac = kMacWarps * (kWarpFloats + kMacWarpWords) * 4;
 static_assert(NB_WALK_MAC_BLOCKS * (kWalkSmemMac + 1024) <= 228 * 1024, "learned walk blocks per SM");
 static_assert(kMacWarps <= kWalkWarps, "the stacks are sized for the geometric block shape");
 
+// Non-binding prefetch of the line holding *p into L1 (no register).
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     float y = x - c;
     float t = s + y;
@@ -500,6 +505,17 @@ k_walk_group(WalkArgs a) {
                     // cell list need, loaded together (one memory latency per
                     // round); the learned variant, short of registers, loads
                     // the quadrupole only for accepted cells
+#ifndef NB_WALK_NO_PREFETCH
+                    if (MAC == kMacLearned) {
+                        // the words this round may read after the test (the
+                        // per-node screen term, the quadrupole of an accepted
+                        // or undecided cell) start their trip to L1 now, beside
+                        // the node words, instead of one memory latency later
+                        prefetch_l1(&a.t.q0[node]);
+                        prefetch_l1(&a.t.q1[node]);
+                        prefetch_l1(&a.mac_node[node]);
+                    }
+#endif
                     lk = a.t.link[node];
                     const double4 cm = a.t.com[node];
                     float4 nq1 = make_float4(0.f, 0.f, 0.f, 0.f);
