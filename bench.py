@@ -240,6 +240,7 @@ def run_reference(args, ws, rank):
     err = oracle.force_error((acc[0][t], acc[1][t], acc[2][t]), want)
     sample = (f"N={args.n:,} Plummer seed 1: {steps} full force evaluations (serial tree build "
               f"+ parallel walk, theta 0.5, monopole), {warm} warm-up")
+    ref_gpu = reference_gpu_context(b)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * total / steps,
@@ -254,7 +255,46 @@ def run_reference(args, ws, rank):
                          "sample": sample},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference_gpu": ref_gpu,
     }))
+
+
+def reference_gpu_context(b):
+    """Two of the reference's own CUDA kernels built for this GPU
+    (oracle/_ref/libcelestial_ref_gpu.so), for context beside the CPU
+    timing: the FP64 tiled gravity kernel on the FP64 direct-sum workload
+    (N = 1000) and on the headline sphere (one launch at N = 2^20), and the
+    radix sort on that sphere's 1,048,576 keys (its time, and whether its
+    output is sorted and stable).  None when the library or a GPU is absent."""
+    import oracle
+    from nbody_b200 import scenarios
+
+    try:
+        import torch
+
+        if oracle.ref_gpu() is None or not torch.cuda.is_available():
+            return None
+    except Exception:  # noqa: BLE001
+        return None
+    out = {}
+    c1 = scenarios.plummer(1000, 1.0, 1.0, seed=0)
+    _, ms = oracle.ref_gpu_gravity(c1.px, c1.py, c1.pz, c1.mass, c1.active, 1e-4, reps=100)
+    out["gravity_fp64_n1000"] = {"ms_per_launch": ms, "pairs_per_s": 1000 * 999 / (ms / 1e3),
+                                 "note": "forces only (the reference's GPU brute-force step also "
+                                         "kicks and drifts on the device)"}
+    _, ms = oracle.ref_gpu_gravity(b.px, b.py, b.pz, b.mass, b.active, EPS, reps=1)
+    n = len(b.px)
+    out["gravity_fp64_n1048576"] = {"ms_per_launch": ms,
+                                    "pairs_per_s": float(n) * (n - 1) / (ms / 1e3)}
+    keys, _, _ = oracle.morton_cube(b.px, b.py, b.pz, b.active)
+    vals = np.arange(n, dtype=np.int32)
+    k, v, ms = oracle.ref_gpu_radix_sort(keys, vals)
+    ok_sorted = bool(np.all(k[1:] >= k[:-1]))
+    want_k, want_v = oracle.stable_sort(keys, vals)
+    out["radix_sort_n1048576"] = {"ms": ms, "sorted": ok_sorted,
+                                  "stable": bool(np.array_equal(v, want_v)),
+                                  "keys_out_of_order": int(np.count_nonzero(k[1:] < k[:-1]))}
+    return out
 
 
 TRAIN_SYSTEMS = [  # (generator, N, seed): the learned MAC's training runs

@@ -18,6 +18,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libcelestial_ref.so"
+REF_GPU_LIB = HERE / "_ref" / "libcelestial_ref_gpu.so"
 # root of the reference repository (only needed to build _ref)
 REF_ENV = "CELESTIAL_REF"
 
@@ -86,8 +87,14 @@ _REF_SIGS = {
     "ref_energy_tracker": (None, [i32, P, P, P, P, P, P, P, P, f64, P]),
 }
 
+_REF_GPU_SIGS = {
+    "ref_gpu_gravity": (i32, [i32, P, P, P, P, P, f64, i32, P, P, P, P]),
+    "ref_gpu_radix_sort": (i32, [i32, P, P, P]),
+}
+
 _lib = None
 _ref = None
+_ref_gpu = None
 
 
 def lib():
@@ -105,6 +112,42 @@ def ref():
     if _ref is None and REF_LIB.exists():
         _ref = _load(REF_LIB, _REF_SIGS)
     return _ref
+
+
+def ref_gpu():
+    """Two of the reference's own CUDA kernels (FP64 gravity, radix sort)
+    built for sm_100a, or None when they were not built.  Loading it needs a
+    CUDA runtime; calling it needs a GPU."""
+    global _ref_gpu
+    if _ref_gpu is None and REF_GPU_LIB.exists():
+        _ref_gpu = _load(REF_GPU_LIB, _REF_GPU_SIGS)
+    return _ref_gpu
+
+
+def ref_gpu_gravity(px, py, pz, m, active, eps, reps=3):
+    """The reference's tiled FP64 gravity kernel on the current GPU: the
+    accelerations and the mean time per launch (ms)."""
+    n = len(px)
+    px, py, pz, m = map(_f, (px, py, pz, m))
+    act = _u8(active)
+    ax, ay, az = np.empty(n), np.empty(n), np.empty(n)
+    ms = np.zeros(1)
+    r = ref_gpu().ref_gpu_gravity(n, _p(px), _p(py), _p(pz), _p(m), _p(act), eps, int(reps),
+                                  _p(ax), _p(ay), _p(az), _p(ms))
+    if r != 0:
+        raise RuntimeError("reference gravity kernel failed")
+    return (ax, ay, az), float(ms[0])
+
+
+def ref_gpu_radix_sort(keys, values):
+    """The reference's launch_radix_sort on the current GPU: its output
+    (keys, values) and the time (ms)."""
+    k = np.ascontiguousarray(keys, np.uint64).copy()
+    v = np.ascontiguousarray(values, np.int32).copy()
+    ms = np.zeros(1)
+    if ref_gpu().ref_gpu_radix_sort(len(k), _p(k), _p(v), _p(ms)) != 0:
+        raise RuntimeError("reference radix sort failed")
+    return k, v, float(ms[0])
 
 
 def _f(a, n=None):
