@@ -2,10 +2,11 @@
 //
 // Broad phase: replaces broad_phase_collision_kernel (engine/src/cuda/
 // collision_kernel.cu:16-64), which only compares each body with the next 31
-// in Morton order and so misses pairs, with a query of the octree: a body
-// descends into every cell whose box, grown by the largest radius inside it,
-// lies within its own radius; at leaves it applies the reference's exact
-// FP64 test |xi - xj|^2 < (ri + rj)^2 (collision_kernel.cu:40-52).  Each pair
+// in Morton order and so misses pairs, with a query of the octree: a warp
+// descends, for a group of up to 32 consecutive sorted bodies, into every
+// cell whose box, grown by the largest radius inside it, meets the group's
+// spheres; at the leaves each body gets the reference's exact FP64 test
+// |xi - xj|^2 < (ri + rj)^2 (collision_kernel.cu:40-52).  Each pair
 // is emitted once (by its lower row) as the key lo << 32 | hi and the keys
 // are radix-sorted, which is CollisionResolver::sort_pairs' order
 // (engine/src/physics/collision_resolver.cpp:8-18).
@@ -26,6 +27,7 @@
 
 #include "collide.cuh"
 #include "sort.cuh"
+#include "walk.cuh"
 
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
@@ -58,65 +60,133 @@ int collide_alloc(CollideBufs& b, int capacity, const std::function<int(void**, 
 
 // ---- broad phase ----------------------------------------------------------
 
-__global__ void k_broad_phase(int n, State s, const double4* __restrict__ sbody,
-                              const float* __restrict__ srad, const uint64_t* __restrict__ skeys,
-                              const uint32_t* __restrict__ sidx, TreeBufs t,
-                              const double* __restrict__ cube, uint64_t* __restrict__ pairs,
-                              int cap, int* __restrict__ count, int* err) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const uint32_t row = sidx[k];
-    if (!s.collidable[row]) return;
-    const double xi = s.px[row], yi = s.py[row], zi = s.pz[row], ri = s.radius[row];
+// Warp-cooperative broad phase: one warp per walk group of up to 32
+// consecutive sorted bodies.  The warp walks the tree once for the group's
+// box, the union of its collidable bodies' spheres (x +- r) widened by the
+// same pad as the cell boxes: a node is accepted when the gap between the
+// group box and its padded cell box is within the node's largest radius
+// (1 + 1e-9).  The ball of every body lies inside the group box, so every
+// node a body's own query accepts is accepted here; accepted leaves are
+// collected, and each lane runs the exact FP64 test of its body against their
+// bodies (higher rows only), so the pair set is the per-body query's.
+constexpr int kBpWarps = 8;
+constexpr int kBpStack = 1024;   // nodes pending per warp
+constexpr int kBpLeaves = 64;    // candidate leaves per evaluation
+
+__global__ void __launch_bounds__(kBpWarps * 32)
+k_broad_phase_groups(State s, const uint64_t* __restrict__ skeys,
+                     const uint32_t* __restrict__ sidx, TreeBufs t,
+                     const double* __restrict__ cube, const int2* __restrict__ groups,
+                     const int* __restrict__ n_groups, unsigned* group_ctr,
+                     uint64_t* __restrict__ pairs, int cap, int* __restrict__ count, int* err) {
+    __shared__ int s_stack[kBpWarps][kBpStack];
+    __shared__ int2 s_leaf[kBpWarps][kBpLeaves];
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int* stk = s_stack[warp];
+    int2* lv = s_leaf[warp];
     const double h = cube[3];
     const double lo[3] = {cube[0] - h, cube[1] - h, cube[2] - h};
     const double pad = 1e-9 * h;
-    int stack[176];
-    int sp = 0;
-    stack[sp++] = 0;
-    int visits = 0;  // every node is visited at most once per body
-    while (sp > 0) {
-        if (++visits > 2 * n + 64) {
-            dev_flag(err, kErrOverflow);
-            break;
-        }
-        const int node = stack[--sp];
-        const int4 lk = t.link[node];
-        const float4 q1 = t.q1[node];
-        // the node's cell box from its level and the key of its first body
-        const int L = t.level[node];
-        const uint64_t key = skeys[lk.z];
-        const double w = ldexp(2.0 * h, -L);
-        const uint32_t c[3] = {compact21(key >> 2) >> (21 - L), compact21(key >> 1) >> (21 - L),
-                               compact21(key) >> (21 - L)};
-        const double p[3] = {xi, yi, zi};
-        double d2 = 0.0;
-        for (int a = 0; a < 3; a++) {
-            const double b0 = lo[a] + c[a] * w - pad, b1 = lo[a] + (c[a] + 1) * w + pad;
-            const double e = p[a] < b0 ? b0 - p[a] : (p[a] > b1 ? p[a] - b1 : 0.0);
-            d2 += e * e;
-        }
-        const double reach = ri + (double)q1.z;
-        if (d2 > reach * reach * (1.0 + 1e-9)) continue;
-        if (lk.y == 0) {
-            for (int j = lk.z; j < lk.z + lk.w; j++) {
-                const uint32_t rj = sidx[j];
-                if (rj <= row || !s.collidable[rj]) continue;
-                const double dx = xi - s.px[rj], dy = yi - s.py[rj], dz = zi - s.pz[rj];
-                const double dd = dx * dx + dy * dy + dz * dz;
-                const double sr = ri + s.radius[rj];
-                if (dd < sr * sr) {
-                    const int slot = atomicAdd(count, 1);
-                    if (slot < cap) pairs[slot] = ((uint64_t)row << 32) | rj;
-                    else dev_flag(err, kErrCapacity);
+    const int ng = *n_groups;
+    const int nnodes = *t.n_nodes;
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = (int)atomicAdd(group_ctr, 1u);
+        g = __shfl_sync(FULL, g, 0);
+        if (g >= ng) break;
+        const int2 grp = groups[g];
+        const bool valid = lane < grp.y;
+        const uint32_t row = valid ? sidx[grp.x + lane] : 0u;
+        const bool mine = valid && s.collidable[row];
+        const double x = mine ? s.px[row] : 0.0, y = mine ? s.py[row] : 0.0;
+        const double z = mine ? s.pz[row] : 0.0, r = mine ? s.radius[row] : 0.0;
+        if (!__any_sync(FULL, mine)) continue;
+        const double glo[3] = {warp_min(mine ? x - r : 1e300) - pad,
+                               warp_min(mine ? y - r : 1e300) - pad,
+                               warp_min(mine ? z - r : 1e300) - pad};
+        const double ghi[3] = {warp_max(mine ? x + r : -1e300) + pad,
+                               warp_max(mine ? y + r : -1e300) + pad,
+                               warp_max(mine ? z + r : -1e300) + pad};
+        // the exact test of this lane's body against the collected leaves
+        int nl = 0;
+        auto evaluate = [&]() {
+            __syncwarp();
+            for (int e = 0; e < nl; e++) {
+                const int2 L = lv[e];
+                for (int j = L.x; j < L.x + L.y; j++) {
+                    const uint32_t rj = sidx[j];
+                    if (!mine || rj <= row || !s.collidable[rj]) continue;
+                    const double dx = x - s.px[rj], dy = y - s.py[rj], dz = z - s.pz[rj];
+                    const double dd = dx * dx + dy * dy + dz * dz;
+                    const double sr = r + s.radius[rj];
+                    if (dd < sr * sr) {
+                        const int slot = atomicAdd(count, 1);
+                        if (slot < cap) pairs[slot] = ((uint64_t)row << 32) | rj;
+                        else dev_flag(err, kErrCapacity);
+                    }
                 }
             }
-            continue;
+            nl = 0;
+            __syncwarp();
+        };
+        int sp = 1;
+        if (lane == 0) stk[0] = 0;
+        __syncwarp();
+        int visited = 0;
+        while (sp > 0) {
+            if (visited > nnodes) {  // each node is taken at most once per group
+                if (lane == 0) dev_flag(err, kErrOverflow);
+                break;
+            }
+            const int take = min(32, sp);
+            const int node = lane < take ? stk[sp - take + lane] : -1;
+            sp -= take;
+            visited += take;
+            __syncwarp();
+            bool accept = false;
+            int4 lk = make_int4(0, 0, 0, 0);
+            if (node >= 0) {
+                lk = t.link[node];
+                const float reach = t.q1[node].z;
+                const int Lv = t.level[node];
+                const uint64_t key = skeys[lk.z];
+                const double w = ldexp(2.0 * h, -Lv);
+                const uint32_t c[3] = {compact21(key >> 2) >> (21 - Lv),
+                                       compact21(key >> 1) >> (21 - Lv), compact21(key) >> (21 - Lv)};
+                double d2 = 0.0;
+                for (int a = 0; a < 3; a++) {
+                    const double b0 = lo[a] + c[a] * w - pad, b1 = lo[a] + (c[a] + 1) * w + pad;
+                    const double e = ghi[a] < b0 ? b0 - ghi[a] : (glo[a] > b1 ? glo[a] - b1 : 0.0);
+                    d2 += e * e;
+                }
+                const double rr = (double)reach;
+                accept = d2 <= rr * rr * (1.0 + 1e-9);
+            }
+            // accepted leaves -> candidates
+            const bool is_leaf = accept && lk.y == 0;
+            const unsigned ml = __ballot_sync(FULL, is_leaf);
+            if (ml) {
+                if (nl + __popc(ml) > kBpLeaves) evaluate();
+                if (is_leaf) lv[nl + __popc(ml & lanemask_lt())] = make_int2(lk.z, lk.w);
+                nl += __popc(ml);
+                __syncwarp();
+            }
+            // children of accepted internal nodes -> stack
+            const int nch = (accept && lk.y > 0) ? lk.y : 0;
+            const int inc = warp_incl_scan(nch);
+            const int tot = __shfl_sync(FULL, inc, 31);
+            if (tot > 0) {
+                if (sp + tot > kBpStack) {
+                    if (lane == 0) dev_flag(err, kErrOverflow);
+                } else {
+                    for (int k = 0; k < nch; k++) stk[sp + inc - nch + k] = lk.x + k;
+                    sp += tot;
+                }
+                __syncwarp();
+            }
         }
-        for (int ch = lk.x + lk.y - 1; ch >= lk.x; ch--) {
-            if (sp < 176) stack[sp++] = ch;
-            else dev_flag(err, kErrOverflow);
-        }
+        if (nl) evaluate();
     }
 }
 
@@ -139,10 +209,14 @@ int broad_phase(cudaStream_t st, CollideBufs& b, CollideArgs& a, bool build_tree
         tree_build(st, a.tree, a.n_active, a.keys0, a.sbody, a.srad, a.cube, a.leaf_cap, a.err);
     }
     cudaMemsetAsync(a.n_pairs, 0, sizeof(int), st);
-    if (a.n_active > 0)
-        k_broad_phase<<<ceil_div(a.n_active, 128), 128, 0, st>>>(
-            a.n_active, a.s, a.sbody, a.srad, a.keys0, a.vals0, a.tree, a.cube, b.pair_keys,
-            b.pair_cap, a.n_pairs, a.err);
+    if (a.n_active > 0) {
+        // walk groups of the tree (sibling packing), one warp each
+        find_groups(st, a.tree, a.sbody, a.n_active, a.groups, a.n_groups, 2.25, 0);
+        cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
+        k_broad_phase_groups<<<a.sms * 4, kBpWarps * 32, 0, st>>>(
+            a.s, a.keys0, a.vals0, a.tree, a.cube, a.groups, a.n_groups, a.group_ctr,
+            b.pair_keys, b.pair_cap, a.n_pairs, a.err);
+    }
     int cnt = 0;
     if (cudaMemcpyAsync(&cnt, a.n_pairs, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)

@@ -43,6 +43,11 @@ struct CollideArgs {
     // (keys0/vals0 sorted, sbody/srad gathered, multipole pass with radii,
     // cube): the broad phase queries it instead of building its own
     bool reuse_tree = false;
+    // walk-group buffers the broad phase (re)fills: >= n_active entries, the
+    // device group count and a work counter
+    int2* groups = nullptr;
+    int* n_groups = nullptr;
+    unsigned* group_ctr = nullptr;
 };
 
 int collide_alloc(CollideBufs& b, int capacity, const std::function<int(void**, size_t)>& alloc);

@@ -814,6 +814,9 @@ int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags)
             // the second half kick moved no body: the force evaluation's tree
             // (Barnes-Hut modes) still describes the positions
             c.reuse_tree = h->tree_current;
+            c.groups = h->groups;
+            c.n_groups = &h->scal->n_groups;
+            c.group_ctr = &h->scal->group_ctr;
             int npairs = 0, nmerge = 0, nkept = 0;
             record(h, 4);
             if ((r = nb::collide_step(h->st, h->col, c, &npairs, &nmerge, &nkept)))
@@ -1266,6 +1269,9 @@ NB_API int32_t nb_broad_phase(nb_engine* h, int32_t n, const double* px, const d
     c.sms = h->sms;
     c.bbox_ord = sc->bbox_ord;
     c.n_active_dev = &sc->n_active;
+    c.groups = h->groups;
+    c.n_groups = &sc->n_groups;
+    c.group_ctr = &sc->group_ctr;
     int np = 0;
     if ((r = nb::broad_phase(h->st, h->col, c, true, &np)))
         return fail(h, r, "broad phase failed");
