@@ -592,7 +592,7 @@ void enqueue_forces(nb_ensemble* h, double eps) {
 
 // Walk-group spans the tree autotuner tries (0: sibling packing); choice k
 // is walk shape k / 4 with span kEnsSpans[k % 4].
-constexpr int kEnsSpans[4] = {0, 64, 128, 256};
+constexpr int kEnsSpans[4] = {0, 256, 512, 1024};
 
 // A span cell must lie inside one system: with span below the smallest tree
 // system's body count, a walk-tree node holding at most `span` bodies can

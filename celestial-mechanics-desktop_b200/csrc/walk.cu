@@ -29,18 +29,6 @@ constexpr int kWalkThreads = kWalkWarps * 32;
 // Interaction-list capacities per warp (entries before a flush).  128 / 128
 // measured within 1 % of 96 / 96 and 64 / 64 on both walks: a smaller list
 // gives L1 more of the shared-memory carve-out but flushes more often.
-// NB_WALK_PIPELINE (learned walk): the next batch of 32 nodes is popped
-// before the current batch pushes its children, and its node words are
-// fetched by cp.async into a per-warp shared-memory buffer while the current
-// batch is tested and emitted (shorter lists make room for the buffers).
-#ifdef NB_WALK_PIPELINE
-#ifndef NB_WALK_CELL_CAP
-#define NB_WALK_CELL_CAP 64
-#endif
-#ifndef NB_WALK_PART_CAP
-#define NB_WALK_PART_CAP 96
-#endif
-#endif
 #ifndef NB_WALK_CELL_CAP
 #define NB_WALK_CELL_CAP 128
 #endif
@@ -66,14 +54,8 @@ constexpr int kMacGeometric = 0, kMacHarvest = 1, kMacLearned = 2;
 #endif
 constexpr int kMacWarps = NB_WALK_MAC_WARPS;
 // learned variant: + per warp 32 staged rows (4 words), 32 outputs and 32
-// pending node ids (and, pipelined, two batches of 32 node-word records of
-// 16 words: link, centre of mass, q1)
-#ifdef NB_WALK_PIPELINE
-constexpr int kMacPipeWords = 2 * 32 * 16;
-#else
-constexpr int kMacPipeWords = 0;
-#endif
-constexpr int kMacWarpWords = 32 * 4 + 32 + 32 + kMacPipeWords;
+// pending node ids
+constexpr int kMacWarpWords = 32 * 4 + 32 + 32;
 constexpr int kWalkSmemMac = kMacWarps * (kWarpFloats + kMacWarpWords) * 4;
 static_assert(NB_WALK_MAC_BLOCKS * (kWalkSmemMac + 1024) <= 228 * 1024, "learned walk blocks per SM");
 static_assert(kMacWarps <= kWalkWarps, "the stacks are sized for the geometric block shape");
@@ -81,25 +63,6 @@ static_assert(kMacWarps <= kWalkWarps, "the stacks are sized for the geometric b
 // Non-binding prefetch of the line holding *p into L1 (no register).
 __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-
-// The node words one lane needs for a test, fetched asynchronously.
-struct __align__(16) NodeWords {
-    int4 link;
-    double4 com;
-    float4 q1;
-};
-
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-    asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 __device__ __forceinline__ void kahan(float& s, float& c, float x) {
@@ -158,14 +121,11 @@ k_walk_group(WalkArgs a) {
     uint32_t* xs = nullptr;
     float* ys = nullptr;
     int* pend = nullptr;
-    NodeWords* stage = nullptr;  // pipelined learned walk: two batches of 32 records
     if (MAC == kMacLearned) {
         xs = (uint32_t*)(s_walk + WARPS * kWarpFloats) + warp * kMacWarpWords;
         ys = (float*)(xs + 32 * 4);
         pend = (int*)(ys + 32);
-        stage = (NodeWords*)(pend + 32);
     }
-    (void)stage;
 
     for (;;) {
         int g = 0;
@@ -520,67 +480,20 @@ k_walk_group(WalkArgs a) {
             emit(pn, tc, lf, op, plk, prx, pry, prz, pm, make_float4(0.f, 0.f, 0.f, 0.f), 0.f);
         };
         int rounds = 0;
-#ifdef NB_WALK_PIPELINE
-        constexpr bool kPipe = MAC == kMacLearned;
-#else
-        constexpr bool kPipe = false;
-#endif
-        int fl_node = -1, fl_take = 0, fl_buf = 0;  // the batch whose words are in flight
-        // pop up to 32 nodes for the next batch and start fetching their words
-        auto pop_issue = [&]() {
-            fl_take = min(32, sp);
-            fl_node = (lane < fl_take) ? stk[sp - fl_take + lane] : -1;
-            sp -= fl_take;
-            __syncwarp();
-            fl_buf ^= 1;
-            if (fl_node >= 0) {
-                NodeWords* d = &stage[fl_buf * 32 + lane];
-                cp_async16(&d->link, &a.t.link[fl_node]);
-                cp_async16(&d->com, &a.t.com[fl_node]);
-                cp_async16((char*)&d->com + 16, (const char*)&a.t.com[fl_node] + 16);
-                cp_async16(&d->q1, &a.t.q1[fl_node]);
-                prefetch_l1(&a.t.q0[fl_node]);
-                prefetch_l1(&a.mac_node[fl_node]);
-            }
-            cp_async_commit();
-        };
-        while (sp > 0 || (MAC == kMacLearned && npend > 0) || (kPipe && fl_take > 0)) {
+        while (sp > 0 || (MAC == kMacLearned && npend > 0)) {
             if (++rounds > kMaxWalkRounds) {
                 if (lane == 0) dev_flag(a.err, kErrOverflow);
                 break;
             }
-            if (kPipe && fl_take == 0) {
-                if (sp == 0) {
-                    flush_pending();
-                    continue;
-                }
-                pop_issue();
-            } else if (!kPipe && MAC == kMacLearned && sp == 0) {
+            if (MAC == kMacLearned && sp == 0) {
                 flush_pending();
                 continue;
             }
             {
-                int node, cur_buf = 0;
-                if (kPipe) {
-                    node = fl_node;
-                    cur_buf = fl_buf;
-                    // the next batch leaves the stack before this one pushes
-                    // its children; its words arrive while this one is tested
-                    fl_take = 0;
-                    fl_node = -1;
-                    if (sp > 0) {
-                        pop_issue();
-                        cp_async_wait<1>();
-                    } else {
-                        cp_async_wait<0>();
-                    }
-                    __syncwarp();
-                } else {
-                    const int take = min(32, sp);
-                    node = (lane < take) ? stk[sp - take + lane] : -1;
-                    sp -= take;
-                    __syncwarp();  // every lane holds its node before the pushes below
-                }
+                const int take = min(32, sp);
+                const int node = (lane < take) ? stk[sp - take + lane] : -1;
+                sp -= take;
+                __syncwarp();  // every lane holds its node before the pushes below
                 bool take_cell = false, is_leaf = false, open = false, in_band = false;
                 int4 lk = make_int4(0, 0, 0, 0);
                 float rx = 0.f, ry = 0.f, rz = 0.f, mass = 0.f, half = 0.f, d2 = 0.f;
@@ -593,7 +506,7 @@ k_walk_group(WalkArgs a) {
                     // round); the learned variant, short of registers, loads
                     // the quadrupole only for accepted cells
 #ifndef NB_WALK_NO_PREFETCH
-                    if (MAC == kMacLearned && !kPipe) {
+                    if (MAC == kMacLearned) {
                         // the words this round may read after the test (the
                         // per-node screen term, the quadrupole of an accepted
                         // or undecided cell) start their trip to L1 now, beside
@@ -603,17 +516,9 @@ k_walk_group(WalkArgs a) {
                         prefetch_l1(&a.mac_node[node]);
                     }
 #endif
-                    double4 cm;
+                    lk = a.t.link[node];
+                    const double4 cm = a.t.com[node];
                     float4 nq1 = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (kPipe) {
-                        const NodeWords& wd = stage[cur_buf * 32 + lane];
-                        lk = wd.link;
-                        cm = wd.com;
-                        nq1 = wd.q1;
-                    } else {
-                        lk = a.t.link[node];
-                        cm = a.t.com[node];
-                    }
                     if (MAC == kMacGeometric) {
                         nq1 = a.t.q1[node];
                         if (QUAD) nq0 = a.t.q0[node];
@@ -621,7 +526,7 @@ k_walk_group(WalkArgs a) {
                     }
                     if (cm.w > 0.0) {
                         live = true;
-                        half = (MAC == kMacGeometric || kPipe) ? nq1.y : a.t.q1[node].y;
+                        half = MAC == kMacGeometric ? nq1.y : a.t.q1[node].y;
                         rx = (float)(cm.x - gcx);
                         ry = (float)(cm.y - gcy);
                         rz = (float)(cm.z - gcz);

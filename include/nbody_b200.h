@@ -141,8 +141,9 @@ enum nb_param {
                                       consecutive sorted bodies cut from the walk-tree cells
                                       holding at most this many bodies whose parent holds
                                       more (full warps; a group's box stays inside a cell of
-                                      at most this many bodies); 0: octree cells of <= 32
-                                      bodies with NB_PARAM_GROUP_PACK sibling packing       */
+                                      at most this many bodies; default 1024); 0: octree
+                                      cells of <= 32 bodies with NB_PARAM_GROUP_PACK sibling
+                                      packing                                                */
 };
 
 /* Indices into nb_get_timings() output (milliseconds, CUDA events).
@@ -420,7 +421,7 @@ NB_API int32_t nb_ens_autotune(nb_ensemble* h, double softening, int32_t* shape,
                                double* ms_per_shape);
 /* Times the tree branch (keys, sort, tree, walk of every tree system) on the
  * current state for each walk block shape (NB_PARAM_ENS_WALK_SHAPE 0, 1) and
- * walk-group span (NB_PARAM_GROUP_SPAN 0, 64, 128, 256), 3 runs each with
+ * walk-group span (NB_PARAM_GROUP_SPAN 0, 256, 512, 1024), 3 runs each with
  * CUDA events, and keeps the fastest: choice k is shape k / 4 with the k % 4-th
  * span.  ms_per_choice (NB_ENS_TREE_CHOICES entries, may be NULL) gets the
  * times.  The tree systems' accelerations are then those of the choice. */
