@@ -81,10 +81,17 @@ k_broad_phase_groups(State s, const uint64_t* __restrict__ skeys,
                      uint64_t* __restrict__ pairs, int cap, int* __restrict__ count, int* err) {
     __shared__ int s_stack[kBpWarps][kBpStack];
     __shared__ int2 s_leaf[kBpWarps][kBpLeaves];
+    __shared__ double s_cand[kBpWarps][4][32];  // staged candidates: x, y, z, radius
+    __shared__ uint32_t s_crow[kBpWarps][32];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int* stk = s_stack[warp];
     int2* lv = s_leaf[warp];
+    double* cx = s_cand[warp][0];
+    double* cy = s_cand[warp][1];
+    double* cz = s_cand[warp][2];
+    double* crad = s_cand[warp][3];
+    uint32_t* cr = s_crow[warp];
     const double h = cube[3];
     const double lo[3] = {cube[0] - h, cube[1] - h, cube[2] - h};
     const double pad = 1e-9 * h;
@@ -108,23 +115,57 @@ k_broad_phase_groups(State s, const uint64_t* __restrict__ skeys,
         const double ghi[3] = {warp_max(mine ? x + r : -1e300) + pad,
                                warp_max(mine ? y + r : -1e300) + pad,
                                warp_max(mine ? z + r : -1e300) + pad};
-        // the exact test of this lane's body against the collected leaves
+        // The exact test of this lane's body against the bodies of the
+        // collected leaves: the leaves' bodies are flattened 32 at a time,
+        // each lane loads one candidate into the warp's staging slots (32
+        // independent loads per round trip), then every lane tests its body
+        // against the staged candidates (broadcast shared-memory reads).  The
+        // test rounds as the all-pairs loop does, without FMA contraction.
         int nl = 0;
         auto evaluate = [&]() {
             __syncwarp();
-            for (int e = 0; e < nl; e++) {
-                const int2 L = lv[e];
-                for (int j = L.x; j < L.x + L.y; j++) {
-                    const uint32_t rj = sidx[j];
-                    if (!mine || rj <= row || !s.collidable[rj]) continue;
-                    const double dx = x - s.px[rj], dy = y - s.py[rj], dz = z - s.pz[rj];
-                    const double dd = dx * dx + dy * dy + dz * dz;
-                    const double sr = r + s.radius[rj];
-                    if (dd < sr * sr) {
-                        const int slot = atomicAdd(count, 1);
-                        if (slot < cap) pairs[slot] = ((uint64_t)row << 32) | rj;
-                        else dev_flag(err, kErrCapacity);
+            for (int b0 = 0; b0 < nl; b0 += 32) {
+                const int2 L = (b0 + lane < nl) ? lv[b0 + lane] : make_int2(0, 0);
+                const int incl = warp_incl_scan(L.y);
+                const int T = __shfl_sync(FULL, incl, 31);
+                for (int t0 = 0; t0 < T; t0 += 32) {
+                    const int tt = t0 + lane;
+                    int pos = 0;  // first lane whose inclusive count exceeds tt
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const int v = __shfl_sync(FULL, incl, pos + step - 1);
+                        if (v <= tt) pos += step;
                     }
+                    const int first = __shfl_sync(FULL, L.x, pos);
+                    const int excl = __shfl_sync(FULL, incl - L.y, pos);
+                    const int take = min(32, T - t0);
+                    if (lane < take) {
+                        const uint32_t rj = sidx[first + (tt - excl)];
+                        // a body that is not collidable gets row 0, which no
+                        // lane's row is below: never tested
+                        cr[lane] = s.collidable[rj] ? rj : 0u;
+                        cx[lane] = s.px[rj];
+                        cy[lane] = s.py[rj];
+                        cz[lane] = s.pz[rj];
+                        crad[lane] = s.radius[rj];
+                    }
+                    __syncwarp();
+                    if (mine) {
+                        for (int k = 0; k < take; k++) {
+                            const uint32_t rj = cr[k];
+                            if (rj <= row) continue;
+                            const double dx = x - cx[k], dy = y - cy[k], dz = z - cz[k];
+                            const double dd = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                                        __dmul_rn(dz, dz));
+                            const double sr = r + crad[k];
+                            if (dd < __dmul_rn(sr, sr)) {
+                                const int slot = atomicAdd(count, 1);
+                                if (slot < cap) pairs[slot] = ((uint64_t)row << 32) | rj;
+                                else dev_flag(err, kErrCapacity);
+                            }
+                        }
+                    }
+                    __syncwarp();
                 }
             }
             nl = 0;
@@ -409,34 +450,45 @@ k_compact(int n, State s, State d, int32_t* __restrict__ dest, uint32_t* look,
     }
     if (lane == 0) s_wtot[warp] = wcount;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (warp == 0) {
+        // warp-wide look-back: lane q reads predecessor j - q, so one L2
+        // round trip covers 32 tiles; the words are consumed nearest first up
+        // to the first inclusive prefix or the first unpublished word
         uint32_t tot = 0;
         for (int w = 0; w < kCompThreads / 32; w++) tot += s_wtot[w];
         uint32_t excl = 0;
         if (tile == 0) {
-            atomicExch(&look[0], kCFlagPre | tot);
+            if (lane == 0) atomicExch(&look[0], kCFlagPre | tot);
         } else {
-            atomicExch(&look[tile], kCFlagAgg | tot);
+            if (lane == 0) atomicExch(&look[tile], kCFlagAgg | tot);
             int j = tile - 1;
             uint32_t spins = 0;
-            while (j >= 0) {
-                const uint32_t v = *(volatile uint32_t*)&look[j];
-                if ((v & ~kCValMask) == 0) {
-                    if (++spins > kSpinLimit) {
-                        dev_flag(err, kErrTimeout);
-                        break;
-                    }
-                    continue;
+            for (;;) {
+                const uint32_t v = (j - lane >= 0) ? *(volatile uint32_t*)&look[j - lane] : 0u;
+                const uint32_t f = v & ~kCValMask;
+                // tile 0 always publishes a prefix: j - lane == 0 ends the chain
+                const unsigned stop = __ballot_sync(0xFFFFFFFFu, f == kCFlagPre ||
+                                                                     (f != 0 && j - lane == 0));
+                const unsigned unpub = __ballot_sync(0xFFFFFFFFu, f == 0);
+                const int first_stop = stop ? __ffs(stop) - 1 : 32;
+                const int first_unpub = unpub ? __ffs(unpub) - 1 : 32;
+                const bool done = first_stop < first_unpub;
+                const int used = done ? first_stop + 1 : first_unpub;
+                excl += __reduce_add_sync(0xFFFFFFFFu, lane < used ? (v & kCValMask) : 0u);
+                if (done) break;
+                j -= used;
+                if (used == 0 && ++spins > kSpinLimit) {
+                    if (lane == 0) dev_flag(err, kErrTimeout);
+                    break;
                 }
-                excl += v & kCValMask;
-                if ((v & ~kCValMask) == kCFlagPre) break;
-                j--;
             }
             __threadfence();
-            atomicExch(&look[tile], kCFlagPre | (excl + tot));
+            if (lane == 0) atomicExch(&look[tile], kCFlagPre | (excl + tot));
         }
-        s_base = excl;
-        if (tile == (int)gridDim.x - 1) *n_kept = (int)(excl + tot);
+        if (lane == 0) {
+            s_base = excl;
+            if (tile == (int)gridDim.x - 1) *n_kept = (int)(excl + tot);
+        }
     }
     __syncthreads();
     uint32_t off = s_base;

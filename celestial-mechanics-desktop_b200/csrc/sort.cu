@@ -22,6 +22,7 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPre = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1;
+constexpr int kLookBatch = 8;  // look-back words read per round trip
 
 constexpr int kSortDynSmem = kSortTile * 12;
 const void* k_sort_pass_ptr();
@@ -128,22 +129,40 @@ k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* 
     } else {
         atomicExch(&my[d], kFlagAgg | real_cnt);
     }
+    // The look-back reads kLookBatch predecessors' words at once (independent
+    // loads, one L2 round trip) and consumes them nearest first up to the
+    // first inclusive prefix or the first word not yet published; with every
+    // tile of a pass resident at once the prefixes are still in flight when
+    // a tile looks back, so one word per round trip made the chain the
+    // pass's critical path.
     uint32_t excl = 0;
     if (tile > 0) {
         int j = tile - 1;
         uint32_t spins = 0;
-        while (j >= 0) {
-            uint32_t v = ld_volatile(look + (size_t)j * 256 + d);
-            if ((v & ~kValMask) == 0) {
-                if (++spins > kSpinLimit) {
-                    dev_flag(err, kErrTimeout);
+        for (;;) {
+            uint32_t v[kLookBatch];
+#pragma unroll
+            for (int q = 0; q < kLookBatch; q++)
+                v[q] = (j - q >= 0) ? ld_volatile(look + (size_t)(j - q) * 256 + d) : 0u;
+            int used = 0;
+            bool done = false;
+#pragma unroll
+            for (int q = 0; q < kLookBatch; q++) {
+                const uint32_t f = v[q] & ~kValMask;
+                if (f == 0) break;  // not yet published: read again from here
+                excl += v[q] & kValMask;
+                used = q + 1;
+                if (f == kFlagPre || j - q == 0) {  // tile 0 always publishes a prefix
+                    done = true;
                     break;
                 }
-                continue;
             }
-            excl += v & kValMask;
-            if ((v & ~kValMask) == kFlagPre) break;
-            j--;
+            if (done) break;
+            j -= used;
+            if (used == 0 && ++spins > kSpinLimit) {
+                dev_flag(err, kErrTimeout);
+                break;
+            }
         }
         __threadfence();
         atomicExch(&my[d], kFlagPre | (excl + real_cnt));

@@ -273,117 +273,126 @@ __global__ void k_octree_emit(int n, TreeBufs t, int leaf_cap) {
     });
 }
 
-__device__ __forceinline__ void quad_add(double q[6], double m, double dx, double dy, double dz) {
-    double r2 = dx * dx + dy * dy + dz * dz;
-    q[0] += m * (3.0 * dx * dx - r2);
-    q[1] += m * (3.0 * dy * dy - r2);
-    q[2] += m * (3.0 * dx * dy);
-    q[3] += m * (3.0 * dx * dz);
-    q[4] += m * (3.0 * dy * dz);
-}
+// Moments of a set of point masses or child cells accumulated in one pass
+// about a reference point r0 (the first member): M, S = sum m d, the second
+// moments T = sum m d d^T (d = x - r0) and, for cells, the sum of the
+// children's own traceless quadrupoles.  The centre of mass is r0 + S / M and
+// the traceless quadrupole about it follows from the parallel-axis shift
+// C = T - M D D^T (D = S / M), Q = 3 C - tr(C) I + sum Q_child; with r0 inside
+// the cell the shift cancels nothing larger than the cell's own spread.
+struct Moments {
+    double M = 0, sx = 0, sy = 0, sz = 0;
+    double txx = 0, tyy = 0, tzz = 0, txy = 0, txz = 0, tyz = 0;
+    double qxx = 0, qyy = 0, qxy = 0, qxz = 0, qyz = 0;
+    __device__ __forceinline__ void add(double m, double dx, double dy, double dz) {
+        M += m;
+        const double mx = m * dx, my = m * dy, mz = m * dz;
+        sx += mx; sy += my; sz += mz;
+        txx = fma(mx, dx, txx); tyy = fma(my, dy, tyy); tzz = fma(mz, dz, tzz);
+        txy = fma(mx, dy, txy); txz = fma(mx, dz, txz); tyz = fma(my, dz, tyz);
+    }
+    // centre of mass (r0 when massless) and the quadrupole about it
+    __device__ __forceinline__ void finish(double r0x, double r0y, double r0z, double4& com,
+                                           float4& q0, float& qyz_out) const {
+        double Dx = 0, Dy = 0, Dz = 0;
+        if (M > 0) {
+            Dx = sx / M; Dy = sy / M; Dz = sz / M;
+        }
+        const double cxx = txx - M * Dx * Dx, cyy = tyy - M * Dy * Dy, czz = tzz - M * Dz * Dz;
+        const double cxy = txy - M * Dx * Dy, cxz = txz - M * Dx * Dz, cyz = tyz - M * Dy * Dz;
+        com = make_double4(r0x + Dx, r0y + Dy, r0z + Dz, M);
+        q0 = make_float4((float)(qxx + 2.0 * cxx - cyy - czz), (float)(qyy + 2.0 * cyy - cxx - czz),
+                         (float)(qxy + 3.0 * cxy), (float)(qxz + 3.0 * cxz));
+        qyz_out = (float)(qyz + 3.0 * cyz);
+    }
+};
 
 // sys_half16: batched systems (keys carry the system in their top bits): the
 // half-size of each system's cube times 2^4, the half-size its level-0 cell
 // would have; null for one system in `cube`.
-__global__ void k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody,
-                           const float* __restrict__ srad, const double* __restrict__ cube,
-                           const uint64_t* __restrict__ skeys,
-                           const double* __restrict__ sys_half16) {
+// One thread per walk node: a leaf reduces its bodies in one pass, then the
+// thread climbs; the last child to arrive at a parent reduces it from its
+// children in child order (deterministic).  Per level the climb makes three
+// dependent L2 trips: the parent's walk index; its link / level / parent words
+// together with the arrival atomic; every child word in one loop.
+__global__ void __launch_bounds__(256)
+k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody,
+            const float* __restrict__ srad, const double* __restrict__ cube,
+            const uint64_t* __restrict__ skeys, const double* __restrict__ sys_half16) {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
     int nn = *t.n_nodes;
     if (w >= nn) return;
-    int4 lk = t.link[w];
+    const int4 lk = __ldg(&t.link[w]);
     if (lk.y != 0) return;  // internal nodes are reduced by their last child
     auto root_half_of = [&](int first) {
         return sys_half16 ? sys_half16[skeys[first] >> kEnsSysShift] : cube[3];
     };
-    double root_half = root_half_of(lk.z);
+    int pb = __ldg(&t.parent_bin[w]);
     {
         // leaf: moments straight from its bodies
-        double M = 0, sx = 0, sy = 0, sz = 0;
+        const double half = ldexp(root_half_of(lk.z), -__ldg(&t.level[w]));
+        const double4 p0 = sbody[lk.z];
+        Moments mo;
         float rmax = 0.f;
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        double lo[3] = {p0.x, p0.y, p0.z}, hi[3] = {p0.x, p0.y, p0.z};
+#pragma unroll 4
         for (int b = lk.z; b < lk.z + lk.w; b++) {
-            double4 p = sbody[b];
-            M += p.w;
-            sx += p.w * p.x;
-            sy += p.w * p.y;
-            sz += p.w * p.z;
+            const double4 p = sbody[b];
+            mo.add(p.w, p.x - p0.x, p.y - p0.y, p.z - p0.z);
             if (srad) rmax = fmaxf(rmax, srad[b]);
             lo[0] = fmin(lo[0], p.x); lo[1] = fmin(lo[1], p.y); lo[2] = fmin(lo[2], p.z);
             hi[0] = fmax(hi[0], p.x); hi[1] = fmax(hi[1], p.y); hi[2] = fmax(hi[2], p.z);
         }
+        double4 com;
+        float4 q0;
+        float qyz;
+        mo.finish(p0.x, p0.y, p0.z, com, q0, qyz);
         t.blo[w] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
                                __double2float_rd(lo[2]), 0.f);
         t.bhi[w] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
                                __double2float_ru(hi[2]), 0.f);
-        double cx, cy, cz;
-        if (M > 0) {
-            cx = sx / M; cy = sy / M; cz = sz / M;
-        } else {
-            double4 p = sbody[lk.z];
-            cx = p.x; cy = p.y; cz = p.z;
-        }
-        double q[6] = {0, 0, 0, 0, 0, 0};
-        if (lk.w > 1)
-            for (int b = lk.z; b < lk.z + lk.w; b++) {
-                double4 p = sbody[b];
-                quad_add(q, p.w, p.x - cx, p.y - cy, p.z - cz);
-            }
-        t.com[w] = make_double4(cx, cy, cz, M);
-        t.q0[w] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
-        t.q1[w] = make_float4((float)q[4], (float)ldexp(root_half, -t.level[w]), rmax, 0.f);
+        t.com[w] = com;
+        t.q0[w] = q0;
+        t.q1[w] = make_float4(qyz, (float)half, rmax, 0.f);
     }
     // climb: the last child to arrive reduces the parent
-    int pb = t.parent_bin[w];
     for (int guard = 0; pb >= 0 && guard < 64; guard++) {  // <= 22 levels up
-        int p = __ldcg(&t.walk_index[pb]);
-        __threadfence();
-        int4 pl = __ldcg(&t.link[p]);
+        const int p = __ldg(&t.walk_index[pb]);
+        const int4 pl = __ldg(&t.link[p]);
+        const int plev = __ldg(&t.level[p]);
+        const int ppb = __ldg(&t.parent_bin[p]);
+        __threadfence();  // this thread's node words are visible before its arrival counts
         if (atomicAdd(&t.counter[p], 1) != pl.y - 1) return;
         __threadfence();
-        double M = 0, sx = 0, sy = 0, sz = 0;
+        const double root_half = root_half_of(pl.z);
+        const double2 r0a = __ldcg((const double2*)&t.com[pl.x]);
+        const double r0z = __ldcg((const double*)&t.com[pl.x] + 2);
+        Moments mo;
         float rmax = 0.f;
-        for (int c = pl.x; c < pl.x + pl.y; c++) {
-            double2 a = __ldcg((const double2*)&t.com[c]);
-            double2 b = __ldcg((const double2*)&t.com[c] + 1);
-            M += b.y;
-            sx += b.y * a.x;
-            sy += b.y * a.y;
-            sz += b.y * b.x;
-            rmax = fmaxf(rmax, __ldcg(&t.q1[c]).z);
-        }
-        double cx, cy, cz;
-        if (M > 0) {
-            cx = sx / M; cy = sy / M; cz = sz / M;
-        } else {
-            double2 a = __ldcg((const double2*)&t.com[pl.x]);
-            double2 b = __ldcg((const double2*)&t.com[pl.x] + 1);
-            cx = a.x; cy = a.y; cz = b.x;
-        }
         float4 blo = make_float4(3e38f, 3e38f, 3e38f, 0.f), bhi = make_float4(-3e38f, -3e38f, -3e38f, 0.f);
+#pragma unroll 2
         for (int c = pl.x; c < pl.x + pl.y; c++) {
+            const double2 a = __ldcg((const double2*)&t.com[c]);
+            const double2 b = __ldcg((const double2*)&t.com[c] + 1);
+            const float4 c0 = __ldcg(&t.q0[c]);
+            const float4 c1 = __ldcg(&t.q1[c]);
             const float4 l = __ldcg(&t.blo[c]), h = __ldcg(&t.bhi[c]);
+            mo.add(b.y, a.x - r0a.x, a.y - r0a.y, b.x - r0z);
+            mo.qxx += c0.x; mo.qyy += c0.y; mo.qxy += c0.z; mo.qxz += c0.w; mo.qyz += c1.x;
+            rmax = fmaxf(rmax, c1.z);
             blo.x = fminf(blo.x, l.x); blo.y = fminf(blo.y, l.y); blo.z = fminf(blo.z, l.z);
             bhi.x = fmaxf(bhi.x, h.x); bhi.y = fmaxf(bhi.y, h.y); bhi.z = fmaxf(bhi.z, h.z);
         }
+        double4 com;
+        float4 q0;
+        float qyz;
+        mo.finish(r0a.x, r0a.y, r0z, com, q0, qyz);
         t.blo[p] = blo;
         t.bhi[p] = bhi;
-        double q[6] = {0, 0, 0, 0, 0, 0};
-        for (int c = pl.x; c < pl.x + pl.y; c++) {
-            double2 a = __ldcg((const double2*)&t.com[c]);
-            double2 b = __ldcg((const double2*)&t.com[c] + 1);
-            float4 c0 = __ldcg(&t.q0[c]);
-            float4 c1 = __ldcg(&t.q1[c]);
-            q[0] += c0.x; q[1] += c0.y; q[2] += c0.z; q[3] += c0.w; q[4] += c1.x;
-            quad_add(q, b.y, a.x - cx, a.y - cy, b.x - cz);
-        }
-        t.com[p] = make_double4(cx, cy, cz, M);
-        t.q0[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
-        root_half = root_half_of(pl.z);
-        t.q1[p] = make_float4((float)q[4], (float)ldexp(root_half, -__ldcg(&t.level[p])), rmax,
-                              0.f);
-        pb = __ldcg(&t.parent_bin[p]);
+        t.com[p] = com;
+        t.q0[p] = q0;
+        t.q1[p] = make_float4(qyz, (float)ldexp(root_half, -plev), rmax, 0.f);
+        pb = ppb;
     }
 }
 
