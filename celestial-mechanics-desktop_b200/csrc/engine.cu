@@ -88,7 +88,6 @@ struct nb_engine {
     float mac_norm_host[nb::kMacNorm] = {0};
     nb::MacDev* mac_dev = nullptr;        // BF16 fragment image for the walk
     float2* mac_node = nullptr;           // per-node screen terms (learned walk)
-    nb::MacTrainImage* mac_ti = nullptr;  // transposed fragments for training
     float *mac_P = nullptr, *mac_m = nullptr, *mac_v = nullptr, *mac_G = nullptr;
     float *mac_norm = nullptr, *mac_loss = nullptr;
     float* mac_part = nullptr;            // per-block gradient partials (training)
@@ -501,7 +500,7 @@ NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
         if ((r = dalloc(h, &h->groups, cap))) break;
         if ((r = dalloc(h, &h->samag, cap))) break;
         if ((r = dalloc(h, &h->mac_node, 2 * cap))) break;
-        if ((r = dalloc(h, &h->mac_dev, 1)) || (r = dalloc(h, &h->mac_ti, 1))) break;
+        if ((r = dalloc(h, &h->mac_dev, 1))) break;
         if ((r = dalloc(h, &h->mac_P, nb::kMacParams)) || (r = dalloc(h, &h->mac_m, nb::kMacParams)) ||
             (r = dalloc(h, &h->mac_v, nb::kMacParams)) || (r = dalloc(h, &h->mac_G, nb::kMacParams)))
             break;
@@ -1425,7 +1424,7 @@ int mac_upload_params(nb_engine* h, const float* P, const float* norm) {
     NB_CUDA(h, cudaMemsetAsync(h->mac_v, 0, sizeof(float) * nb::kMacParams, h->st));
     h->mac_adam_step = 0;
     std::copy(norm, norm + nb::kMacNorm, h->mac_norm_host);
-    nb::mac_image(h->st, h->mac_P, h->mac_norm, h->mac_dev, h->mac_ti);
+    nb::mac_image(h->st, h->mac_P, h->mac_norm, h->mac_dev);
     // a new network invalidates the screen: off until the next fit
     std::fill(h->mac_screen, h->mac_screen + nb::kMacScreen, 0.f);
     h->mac_screen[nb::kMacScreen - 1] = INFINITY;
@@ -1603,9 +1602,9 @@ NB_API int32_t nb_mac_train(nb_engine* h, int32_t epochs, int32_t batch, double 
         for (int row0 = 0; row0 < n; row0 += batch) {
             const int rows = std::min(batch, n - row0);
             nb::mac_grad(h->st, h->mac_X, h->mac_Y, order, row0, rows, h->mac_P, h->mac_dev,
-                         h->mac_ti, h->mac_G, h->mac_loss, h->sms, h->mac_part, h->scal->err);
+                         h->mac_G, h->mac_loss, h->sms, h->mac_part, h->scal->err);
             nb::mac_adam(h->st, h->mac_P, h->mac_G, h->mac_m, h->mac_v, ++h->mac_adam_step, (float)lr);
-            nb::mac_image(h->st, h->mac_P, h->mac_norm, h->mac_dev, h->mac_ti);
+            nb::mac_image(h->st, h->mac_P, h->mac_norm, h->mac_dev);
         }
         float loss = 0.f;
         if ((r = download(h, &loss, h->mac_loss, sizeof(float)))) break;
@@ -1662,7 +1661,7 @@ NB_API int32_t nb_mac_gradient(nb_engine* h, const float* X, const float* Y, int
         !(r = upload(h, dY, Y, sizeof(float) * (size_t)n)) &&
         !(r = upload(h, dO, ord.data(), sizeof(int) * (size_t)n))) {
         cudaMemsetAsync(h->mac_loss, 0, sizeof(float), h->st);
-        nb::mac_grad(h->st, dX, dY, dO, 0, n, h->mac_P, h->mac_dev, h->mac_ti, h->mac_G,
+        nb::mac_grad(h->st, dX, dY, dO, 0, n, h->mac_P, h->mac_dev, h->mac_G,
                      h->mac_loss, h->sms, h->mac_part, h->scal->err);
         float l = 0.f;
         if (!(r = download(h, grad, h->mac_G, sizeof(float) * nb::kMacParams)) &&

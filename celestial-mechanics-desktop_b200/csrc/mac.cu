@@ -112,7 +112,7 @@ void mac_targets(cudaStream_t st, int nrec, const MacRecord* rec, const double4*
 // ---- device image ------------------------------------------------------------
 
 __global__ void k_mac_image(const float* __restrict__ P, const float* __restrict__ norm,
-                            MacDev* __restrict__ w, MacTrainImage* __restrict__ ti) {
+                            MacDev* __restrict__ w) {
     const int tid = threadIdx.x;
     // lane-ordered B fragments: lane = 4 * g + t holds (k = 2t, 2t+1 | 2t+8, 2t+9; n = g)
     for (int e = tid; e < 8 * 32; e += blockDim.x) {
@@ -126,10 +126,7 @@ __global__ void k_mac_image(const float* __restrict__ P, const float* __restrict
         const int kt = e / 256, nt = (e / 32) % 8, lane = e % 32, g = lane >> 2, t4 = lane & 3;
         const int n = nt * 8 + g, k0 = kt * 16 + 2 * t4;
         auto W2 = [&](int k) { return P[kMacW2 + k * kMacHid + n]; };    // W2[k][n]
-        auto W2T = [&](int k) { return P[kMacW2 + n * kMacHid + k]; };   // W2^T[k][n] = W2[n][k]
         w->w2f[kt][nt][lane] = make_uint2(pack_bf16(W2(k0), W2(k0 + 1)), pack_bf16(W2(k0 + 8), W2(k0 + 9)));
-        ti->w2tf[kt][nt][lane] =
-            make_uint2(pack_bf16(W2T(k0), W2T(k0 + 1)), pack_bf16(W2T(k0 + 8), W2T(k0 + 9)));
     }
     for (int e = tid; e < kMacHid; e += blockDim.x) {
         w->b1[e] = P[kMacB1 + e];
@@ -147,231 +144,17 @@ __global__ void k_mac_image(const float* __restrict__ P, const float* __restrict
     }
 }
 
-void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w, MacTrainImage* ti) {
-    k_mac_image<<<1, 256, 0, st>>>(P, norm, w, ti);
+void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w) {
+    k_mac_image<<<1, 256, 0, st>>>(P, norm, w);
 }
 
 // ---- training --------------------------------------------------------------
 
-constexpr int kTrainWarps = 4;
-// Per-warp gradient accumulator, laid out like the parameter vector plus the
-// loss: each warp adds only its own tiles' contributions (no two lanes of an
-// mma tile write the same entry), and the warps' and blocks' accumulators
-// are summed in a fixed order, so a gradient is bitwise reproducible.
+// Gradient accumulator of one training block, laid out like the parameter
+// vector plus the loss; the blocks' accumulators are summed in a fixed order
+// (k_mac_grad_reduce), so a gradient is bitwise reproducible.
 constexpr int kAccLoss = kMacParams;
 constexpr int kAccFloats = (kMacParams + 1 + 3) / 4 * 4;
-// per warp staging of one 16-row tile
-struct TrainStage {
-    __nv_bfloat16 xs[16][16];
-    __nv_bfloat16 h1[16][kMacHid];
-    __nv_bfloat16 g2[16][kMacHid];
-    __nv_bfloat16 g1[16][kMacHid];
-};
-constexpr int kTrainSmem = kTrainWarps * (kAccFloats * 4 + (int)sizeof(TrainStage));
-
-__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16* p) {
-    return *reinterpret_cast<const uint32_t*>(p);
-}
-__device__ __forceinline__ uint32_t pair_of(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
-
-// rows [row0, row0 + nrows) of the batch; X raw features, Y raw targets;
-// grad (4801 floats) and loss accumulate over the whole launch.
-__global__ void __launch_bounds__(kTrainWarps * 32)
-k_mac_train(const float* __restrict__ X, const float* __restrict__ Y,
-            const int* __restrict__ order, int row0, int nrows, const MacDev* __restrict__ w,
-            const MacTrainImage* __restrict__ ti, float inv_batch, float* __restrict__ part) {
-    extern __shared__ __align__(16) float s_train[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t4 = lane & 3;
-    for (int e = threadIdx.x; e < kTrainWarps * kAccFloats; e += blockDim.x) s_train[e] = 0.f;
-    float* A = s_train + warp * kAccFloats;  // this warp's accumulator
-    TrainStage& ST = reinterpret_cast<TrainStage*>(s_train + kTrainWarps * kAccFloats)[warp];
-    __syncthreads();
-    const int tiles = (nrows + 15) / 16;
-    for (int tile = blockIdx.x * kTrainWarps + warp; tile < tiles; tile += gridDim.x * kTrainWarps) {
-        // 1. stage 16 normalised rows (rows past the end get zero gradient)
-        const int r_lo = tile * 16;
-        for (int e = lane; e < 16 * 16; e += 32) {
-            const int r = e / 16, k = e % 16;
-            float v = 0.f;
-            if (k < kMacIn && r_lo + r < nrows) {
-                const int row = order[row0 + r_lo + r];
-                v = (X[(size_t)row * kMacIn + k] - w->mean[k]) * w->inv_std[k];
-            }
-            ST.xs[r][k] = __float2bfloat16_rn(v);
-        }
-        __syncwarp();
-        // 2. layer 1 -> h1 (bf16, row-major in smem)
-        const uint32_t a0 = ld_pair(&ST.xs[g][2 * t4]), a1 = ld_pair(&ST.xs[g + 8][2 * t4]);
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            const float bl = w->b1[nt * 8 + 2 * t4], bh = w->b1[nt * 8 + 2 * t4 + 1];
-            float c[4] = {bl, bh, bl, bh};
-            mma_bf16(c, a0, a1, 0u, 0u, w->w1f[nt][lane]);
-            const int col = nt * 8 + 2 * t4;
-            ST.h1[g][col] = __float2bfloat16_rn(fmaxf(c[0], 0.f));
-            ST.h1[g][col + 1] = __float2bfloat16_rn(fmaxf(c[1], 0.f));
-            ST.h1[g + 8][col] = __float2bfloat16_rn(fmaxf(c[2], 0.f));
-            ST.h1[g + 8][col + 1] = __float2bfloat16_rn(fmaxf(c[3], 0.f));
-        }
-        __syncwarp();
-        // 3. layer 2 (pre-activations kept in registers) and output
-        float z2[8][4];
-        float y0 = 0.f, y1 = 0.f;
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            const float bl = w->b2[nt * 8 + 2 * t4], bh = w->b2[nt * 8 + 2 * t4 + 1];
-            z2[nt][0] = bl; z2[nt][1] = bh; z2[nt][2] = bl; z2[nt][3] = bh;
-#pragma unroll
-            for (int kt = 0; kt < 4; kt++) {
-                const int k0 = kt * 16 + 2 * t4;
-                mma_bf16(z2[nt], ld_pair(&ST.h1[g][k0]), ld_pair(&ST.h1[g + 8][k0]),
-                         ld_pair(&ST.h1[g][k0 + 8]), ld_pair(&ST.h1[g + 8][k0 + 8]),
-                         w->w2f[kt][nt][lane]);
-            }
-            const float wl = w->w3[nt * 8 + 2 * t4], wh = w->w3[nt * 8 + 2 * t4 + 1];
-            y0 = fmaf(fmaxf(z2[nt][0], 0.f), wl, fmaf(fmaxf(z2[nt][1], 0.f), wh, y0));
-            y1 = fmaf(fmaxf(z2[nt][2], 0.f), wl, fmaf(fmaxf(z2[nt][3], 0.f), wh, y1));
-        }
-        y0 += __shfl_xor_sync(0xFFFFFFFFu, y0, 1);
-        y0 += __shfl_xor_sync(0xFFFFFFFFu, y0, 2);
-        y1 += __shfl_xor_sync(0xFFFFFFFFu, y1, 1);
-        y1 += __shfl_xor_sync(0xFFFFFFFFu, y1, 2);
-        y0 += w->b3;
-        y1 += w->b3;
-        // 4. loss and dL/dy for rows g and g + 8 (mean squared error)
-        float d0 = 0.f, d1 = 0.f, lsq = 0.f;
-        if (r_lo + g < nrows) {
-            const float tg = (Y[order[row0 + r_lo + g]] - w->y_mean) / w->y_std;
-            d0 = 2.f * (y0 - tg) * inv_batch;
-            if (t4 == 0) lsq += (y0 - tg) * (y0 - tg);
-        }
-        if (r_lo + g + 8 < nrows) {
-            const float tg = (Y[order[row0 + r_lo + g + 8]] - w->y_mean) / w->y_std;
-            d1 = 2.f * (y1 - tg) * inv_batch;
-            if (t4 == 0) lsq += (y1 - tg) * (y1 - tg);
-        }
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) lsq += __shfl_xor_sync(0xFFFFFFFFu, lsq, o);
-        if (lane == 0) A[kAccLoss] += lsq;
-        // 5. g2 = dy w3 [z2 > 0]; dw3, db2 partials; db3
-        float pdb3 = (t4 == 0) ? d0 + d1 : 0.f;
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            const int col = nt * 8 + 2 * t4;
-            const float wl = w->w3[col], wh = w->w3[col + 1];
-            const float g00 = z2[nt][0] > 0.f ? d0 * wl : 0.f, g01 = z2[nt][1] > 0.f ? d0 * wh : 0.f;
-            const float g10 = z2[nt][2] > 0.f ? d1 * wl : 0.f, g11 = z2[nt][3] > 0.f ? d1 * wh : 0.f;
-            ST.g2[g][col] = __float2bfloat16_rn(g00);
-            ST.g2[g][col + 1] = __float2bfloat16_rn(g01);
-            ST.g2[g + 8][col] = __float2bfloat16_rn(g10);
-            ST.g2[g + 8][col + 1] = __float2bfloat16_rn(g11);
-            float w3l = fmaxf(z2[nt][0], 0.f) * d0 + fmaxf(z2[nt][2], 0.f) * d1;
-            float w3h = fmaxf(z2[nt][1], 0.f) * d0 + fmaxf(z2[nt][3], 0.f) * d1;
-            float b2l = g00 + g10, b2h = g01 + g11;
-#pragma unroll
-            for (int o = 4; o < 32; o <<= 1) {  // sum over g (lanes with the same t)
-                w3l += __shfl_xor_sync(0xFFFFFFFFu, w3l, o);
-                w3h += __shfl_xor_sync(0xFFFFFFFFu, w3h, o);
-                b2l += __shfl_xor_sync(0xFFFFFFFFu, b2l, o);
-                b2h += __shfl_xor_sync(0xFFFFFFFFu, b2h, o);
-            }
-            if (g == 0) {
-                A[kMacW3 + col] += w3l;
-                A[kMacW3 + col + 1] += w3h;
-                A[kMacB2 + col] += b2l;
-                A[kMacB2 + col + 1] += b2h;
-            }
-        }
-#pragma unroll
-        for (int o = 4; o < 32; o <<= 1) pdb3 += __shfl_xor_sync(0xFFFFFFFFu, pdb3, o);
-        if (lane == 0) A[kMacB3] += pdb3;
-        __syncwarp();
-        // 6. dW2 += H1^T G2: M = 64 inputs (4 m-tiles), N = 64 outputs, K = 16 rows
-#pragma unroll
-        for (int mt = 0; mt < 4; mt++) {
-            const int i0 = mt * 16 + g;
-            const uint32_t b_a0 = pair_of(ST.h1[2 * t4][i0], ST.h1[2 * t4 + 1][i0]);
-            const uint32_t b_a1 = pair_of(ST.h1[2 * t4][i0 + 8], ST.h1[2 * t4 + 1][i0 + 8]);
-            const uint32_t b_a2 = pair_of(ST.h1[2 * t4 + 8][i0], ST.h1[2 * t4 + 9][i0]);
-            const uint32_t b_a3 = pair_of(ST.h1[2 * t4 + 8][i0 + 8], ST.h1[2 * t4 + 9][i0 + 8]);
-#pragma unroll
-            for (int nt = 0; nt < 8; nt++) {
-                const int j = nt * 8 + g;
-                const uint2 bb = make_uint2(pair_of(ST.g2[2 * t4][j], ST.g2[2 * t4 + 1][j]),
-                                            pair_of(ST.g2[2 * t4 + 8][j], ST.g2[2 * t4 + 9][j]));
-                float c[4] = {0.f, 0.f, 0.f, 0.f};
-                mma_bf16(c, b_a0, b_a1, b_a2, b_a3, bb);
-                const int col = nt * 8 + 2 * t4;
-                A[kMacW2 + i0 * kMacHid + col] += c[0];
-                A[kMacW2 + i0 * kMacHid + col + 1] += c[1];
-                A[kMacW2 + (i0 + 8) * kMacHid + col] += c[2];
-                A[kMacW2 + (i0 + 8) * kMacHid + col + 1] += c[3];
-            }
-        }
-        // 7. dH1 = G2 W2^T, g1 = dH1 [h1 > 0]; db1
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int kt = 0; kt < 4; kt++) {
-                const int k0 = kt * 16 + 2 * t4;
-                mma_bf16(c, ld_pair(&ST.g2[g][k0]), ld_pair(&ST.g2[g + 8][k0]),
-                         ld_pair(&ST.g2[g][k0 + 8]), ld_pair(&ST.g2[g + 8][k0 + 8]),
-                         ti->w2tf[kt][nt][lane]);
-            }
-            const int col = nt * 8 + 2 * t4;
-            const float m00 = __bfloat162float(ST.h1[g][col]) > 0.f ? c[0] : 0.f;
-            const float m01 = __bfloat162float(ST.h1[g][col + 1]) > 0.f ? c[1] : 0.f;
-            const float m10 = __bfloat162float(ST.h1[g + 8][col]) > 0.f ? c[2] : 0.f;
-            const float m11 = __bfloat162float(ST.h1[g + 8][col + 1]) > 0.f ? c[3] : 0.f;
-            ST.g1[g][col] = __float2bfloat16_rn(m00);
-            ST.g1[g][col + 1] = __float2bfloat16_rn(m01);
-            ST.g1[g + 8][col] = __float2bfloat16_rn(m10);
-            ST.g1[g + 8][col + 1] = __float2bfloat16_rn(m11);
-            float bl = m00 + m10, bh = m01 + m11;
-#pragma unroll
-            for (int o = 4; o < 32; o <<= 1) {
-                bl += __shfl_xor_sync(0xFFFFFFFFu, bl, o);
-                bh += __shfl_xor_sync(0xFFFFFFFFu, bh, o);
-            }
-            if (g == 0) {
-                A[kMacB1 + col] += bl;
-                A[kMacB1 + col + 1] += bh;
-            }
-        }
-        __syncwarp();
-        // 8. dW1 += X^T G1: M = 16 features (8 used), N = 64, K = 16 rows
-        {
-            const uint32_t x_a0 = pair_of(ST.xs[2 * t4][g], ST.xs[2 * t4 + 1][g]);
-            const uint32_t x_a1 = pair_of(ST.xs[2 * t4][g + 8], ST.xs[2 * t4 + 1][g + 8]);
-            const uint32_t x_a2 = pair_of(ST.xs[2 * t4 + 8][g], ST.xs[2 * t4 + 9][g]);
-            const uint32_t x_a3 = pair_of(ST.xs[2 * t4 + 8][g + 8], ST.xs[2 * t4 + 9][g + 8]);
-#pragma unroll
-            for (int nt = 0; nt < 8; nt++) {
-                const int j = nt * 8 + g;
-                const uint2 bb = make_uint2(pair_of(ST.g1[2 * t4][j], ST.g1[2 * t4 + 1][j]),
-                                            pair_of(ST.g1[2 * t4 + 8][j], ST.g1[2 * t4 + 9][j]));
-                float c[4] = {0.f, 0.f, 0.f, 0.f};
-                mma_bf16(c, x_a0, x_a1, x_a2, x_a3, bb);
-                const int col = nt * 8 + 2 * t4;
-                if (g < kMacIn) {  // rows g + 8 are padding features
-                    A[kMacW1 + g * kMacHid + col] += c[0];
-                    A[kMacW1 + g * kMacHid + col + 1] += c[1];
-                }
-            }
-        }
-        __syncwarp();
-    }
-    __syncthreads();
-    // this block's partial: its warps' accumulators in warp order
-    for (int e = threadIdx.x; e < kAccFloats; e += blockDim.x) {
-        float sum = 0.f;
-        for (int wi = 0; wi < kTrainWarps; wi++) sum += s_train[wi * kAccFloats + e];
-        part[(size_t)blockIdx.x * kAccFloats + e] = sum;
-    }
-}
 
 // grad = the blocks' partials summed in block order; the loss is added to
 // *loss (it accumulates over the batches of an epoch).
@@ -402,25 +185,12 @@ __global__ void k_mac_adam(float* __restrict__ P, const float* __restrict__ G, f
 size_t mac_grad_partial_bytes(int sms) { return sizeof(float) * (size_t)kAccFloats * sms * 4; }
 
 void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order, int row0,
-              int nrows, const float* P, const MacDev* w, const MacTrainImage* ti, float* grad,
-              float* loss, int sms, float* part, int* err) {
+              int nrows, const float* P, const MacDev* w, float* grad, float* loss, int sms,
+              float* part, int* err) {
     if (nrows <= 0) {
         cudaMemsetAsync(grad, 0, sizeof(float) * kMacParams, st);
         return;
     }
-#ifdef NB_MAC_TRAIN_WARP_MMA
-    // per call: the attribute belongs to the current device, and handles on
-    // several devices share this function (a host-side call of a microsecond)
-    cudaFuncSetAttribute((const void*)k_mac_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kTrainSmem);
-    const int tiles = (nrows + 15) / 16;
-    const int blocks = min(ceil_div(tiles, kTrainWarps), sms * 4);
-    k_mac_train<<<blocks, kTrainWarps * 32, kTrainSmem, st>>>(X, Y, order, row0, nrows, w, ti,
-                                                               1.f / (float)nrows, part);
-    (void)P;
-    (void)err;
-#else
-    (void)ti;
     // tcgen05: one CTA per SM (its shared memory admits one), tiles of 128 rows
     cudaFuncSetAttribute((const void*)k_mac_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)mac_train_tc_smem());
@@ -428,7 +198,6 @@ void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order,
     const int blocks = min(tiles, sms);
     k_mac_train_tc<<<blocks, 128, mac_train_tc_smem(), st>>>(
         X, Y, order, row0, nrows, P, w, 1.f / (float)nrows, part, kAccFloats, kAccLoss, err);
-#endif
     k_mac_grad_reduce<<<ceil_div(kMacParams + 1, 256), 256, 0, st>>>(blocks, part, grad, loss);
 }
 

@@ -5,12 +5,6 @@
 
 namespace nb {
 
-// Transposed layer-2 weights as B fragments, for the activation gradient
-// G2 W2^T of the backward pass.
-struct MacTrainImage {
-    uint2 w2tf[4][8][32];
-};
-
 // Normalisation block: 8 feature means, 8 feature stds, target mean, target std.
 constexpr int kMacNorm = 2 * kMacIn + 2;
 
@@ -24,7 +18,7 @@ void mac_sort_records(cudaStream_t st, int nrec, const MacRecord* rec, MacRecord
 void mac_targets(cudaStream_t st, int nrec, const MacRecord* rec, const double4* sbody,
                  const TreeBufs& t, double eps, float* X, float* Y, int* n_out, int out_off,
                  int out_cap);
-void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w, MacTrainImage* ti);
+void mac_image(cudaStream_t st, const float* P, const float* norm, MacDev* w);
 // Gradient of the mean squared error of rows order[row0 .. row0+nrows) into
 // grad (kMacParams floats, overwritten); the sum of squared errors is added
 // to *loss.  part: mac_grad_partial_bytes(sms) of scratch.  The result is
@@ -33,8 +27,8 @@ size_t mac_grad_partial_bytes(int sms);
 // P: the FP32 master parameters (the tensor-core kernel stages W1, W2 from
 // them as BF16); err: the device error word (a bounded wait that expired).
 void mac_grad(cudaStream_t st, const float* X, const float* Y, const int* order, int row0,
-              int nrows, const float* P, const MacDev* w, const MacTrainImage* ti, float* grad,
-              float* loss, int sms, float* part, int* err);
+              int nrows, const float* P, const MacDev* w, float* grad, float* loss, int sms,
+              float* part, int* err);
 // The tcgen05 training kernel (mac_tc.cu): one CTA of 128 threads per SM.
 __global__ void k_mac_train_tc(const float* __restrict__ X, const float* __restrict__ Y,
                                const int* __restrict__ order, int row0, int nrows,
