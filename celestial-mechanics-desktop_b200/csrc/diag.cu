@@ -233,6 +233,110 @@ void max_acc2(cudaStream_t st, int n, const State& s, unsigned long long* out, i
     if (n > 0) k_max_acc2<<<std::min(ceil_div(n, 256), sms * 4), 256, 0, st>>>(n, s, out);
 }
 
+// ---- the learned MAC's in-run audit ------------------------------------------
+//
+// Direct-sum accelerations of sampled targets from the force evaluation's
+// Morton-sorted FP64 copy of the active bodies (sbody).  Sources come in tiles
+// of 256 consecutive sorted bodies, which sit close together: every tile is
+// differenced in FP64 against its first body, rounded to FP32, and each
+// target's FP64 position is differenced against the same point once per
+// tile, so a pair's FP32 separation carries a relative error of a few FP32
+// ulps of the separation itself (not of the system's extent).  The pair terms
+// are packed FP32 (two targets per instruction, FTZ rsqrt), each tile's FP32
+// partial sum is added to an FP64 accumulator, and the chunk partials are
+// summed in chunk order: deterministic, and within ~1e-6 relative of the FP64
+// direct sum, three orders of magnitude below the audit's error bound.
+constexpr int kAudThreads = 256;
+constexpr int kAudPer = 4;                          // targets per thread, packed in pairs
+constexpr int kAudTargets = kAudThreads * kAudPer;  // targets per block
+constexpr int kAudTile = kAudThreads;               // sources per shared-memory tile
+constexpr int kAudMinChunk = 2048;
+
+__global__ void __launch_bounds__(kAudThreads)
+k_audit_targets(int ns, const double4* __restrict__ sbody, float eps2, const State s,
+                const int32_t* __restrict__ targets, int nt, int chunk,
+                double* __restrict__ part) {
+    __shared__ float4 sj[kAudTile];
+    __shared__ float4 sj2[kAudTile];
+    constexpr int P = kAudPer / 2;
+    const int t0 = blockIdx.x * kAudTargets;
+    double px[kAudPer], py[kAudPer], pz[kAudPer], ax[kAudPer], ay[kAudPer], az[kAudPer];
+#pragma unroll
+    for (int u = 0; u < kAudPer; u++) {
+        const int k = t0 + u * kAudThreads + threadIdx.x;
+        const int i = targets[k < nt ? k : nt - 1];
+        px[u] = s.px[i];
+        py[u] = s.py[i];
+        pz[u] = s.pz[i];
+        ax[u] = ay[u] = az[u] = 0.0;
+    }
+    const f32x2 E2 = pk2(eps2, eps2);
+    const int j0 = blockIdx.y * chunk, j1 = min(ns, j0 + chunk);
+    for (int base = j0; base < j1; base += kAudTile) {
+        const double4 r0 = sbody[base];  // the tile's reference point
+        const int j = base + threadIdx.x;
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);  // past the end: massless
+        if (j < j1) {
+            const double4 b = sbody[j];
+            q = make_float4((float)(b.x - r0.x), (float)(b.y - r0.y), (float)(b.z - r0.z),
+                            (float)b.w);
+        }
+        __syncthreads();  // the previous tile is consumed
+        sj[threadIdx.x] = make_float4(q.x, q.x, q.y, q.y);
+        sj2[threadIdx.x] = make_float4(q.z, q.z, q.w, q.w);
+        __syncthreads();
+        f32x2 BX[P], BY[P], BZ[P], AX[P], AY[P], AZ[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            BX[p] = pk2((float)(px[2 * p] - r0.x), (float)(px[2 * p + 1] - r0.x));
+            BY[p] = pk2((float)(py[2 * p] - r0.y), (float)(py[2 * p + 1] - r0.y));
+            BZ[p] = pk2((float)(pz[2 * p] - r0.z), (float)(pz[2 * p + 1] - r0.z));
+            AX[p] = AY[p] = AZ[p] = 0ull;
+        }
+        const int cnt = min(kAudTile, j1 - base);
+#pragma unroll 8
+        for (int k = 0; k < cnt; k++) {
+            const float4 qa = sj[k], qb = sj2[k];
+            const f32x2 qx = pk2(qa.x, qa.y), qy = pk2(qa.z, qa.w);
+            const f32x2 qz = pk2(qb.x, qb.y), qm = pk2(qb.z, qb.w);
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                const f32x2 dx = sub2(qx, BX[p]), dy = sub2(qy, BY[p]), dz = sub2(qz, BZ[p]);
+                const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+                float ra, rb;
+                upk2(r2, ra, rb);
+                const f32x2 inv = pk2(rsqrt_ftz(ra), rsqrt_ftz(rb));
+                const f32x2 f = mul2(mul2(mul2(inv, inv), inv), qm);
+                AX[p] = fma2(f, dx, AX[p]);
+                AY[p] = fma2(f, dy, AY[p]);
+                AZ[p] = fma2(f, dz, AZ[p]);
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            float lo, hi;
+            upk2(AX[p], lo, hi);
+            ax[2 * p] += lo;
+            ax[2 * p + 1] += hi;
+            upk2(AY[p], lo, hi);
+            ay[2 * p] += lo;
+            ay[2 * p + 1] += hi;
+            upk2(AZ[p], lo, hi);
+            az[2 * p] += lo;
+            az[2 * p + 1] += hi;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < kAudPer; u++) {
+        const int k = t0 + u * kAudThreads + threadIdx.x;
+        if (k >= nt) continue;
+        double* o = part + ((size_t)blockIdx.y * nt + k) * 3;
+        o[0] = ax[u];
+        o[1] = ay[u];
+        o[2] = az[u];
+    }
+}
+
 // out3[v] = sum over chunks c of part[c][v], in chunk order.
 __global__ void k_direct_targets_reduce(int nv, int chunks, const double* __restrict__ part,
                                         double* __restrict__ out3) {
@@ -274,6 +378,28 @@ void direct_targets(cudaStream_t st, int n, const State& s, double eps, int nt,
     }
     k_direct_targets<<<grid, kTgtThreads, 0, st>>>(n, s, eps * eps, targets, nt, chunk, scratch);
     k_direct_targets_reduce<<<ceil_div(3 * nt, 256), 256, 0, st>>>(3 * nt, used, scratch, out3);
+}
+
+size_t audit_targets_scratch_bytes(int sms) {
+    return sizeof(double) * 3 * (size_t)(2 * sms + 1) * kAudTargets;
+}
+
+bool audit_targets(cudaStream_t st, int ns, const double4* sbody, const State& s, double eps,
+                   int nt, const int32_t* targets, double* out3, double* scratch, int sms) {
+    if (nt <= 0 || ns <= 0 || !(eps > 0.0)) return false;
+    const int tiles = ceil_div(nt, kAudTargets);
+    // about two blocks per SM in all, at least kAudMinChunk sources per chunk,
+    // and no more chunk partials than the scratch holds
+    const size_t cap = (size_t)(2 * sms + 1) * kAudTargets;
+    int chunks = std::max(1, std::min(ceil_div(2 * sms, tiles), ceil_div(ns, kAudMinChunk)));
+    if ((size_t)chunks * (size_t)nt > cap) chunks = (int)(cap / (size_t)nt);
+    if (chunks < 1) return false;
+    const int chunk = ceil_div(ceil_div(ns, chunks), kAudTile) * kAudTile;
+    const int used = ceil_div(ns, chunk);
+    k_audit_targets<<<dim3(tiles, used), kAudThreads, 0, st>>>(ns, sbody, (float)(eps * eps), s,
+                                                                targets, nt, chunk, scratch);
+    k_direct_targets_reduce<<<ceil_div(3 * nt, 256), 256, 0, st>>>(3 * nt, used, scratch, out3);
+    return true;
 }
 
 }  // namespace nb

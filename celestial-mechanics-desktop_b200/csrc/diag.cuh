@@ -1,4 +1,5 @@
-// diag.cuh - energy / momentum diagnostics and the sampled FP64 audit.
+// diag.cuh - energy / momentum diagnostics, the sampled FP64 force-error sums
+// and the learned MAC's audit sums.
 #pragma once
 #include "bodies.cuh"
 
@@ -16,5 +17,13 @@ size_t direct_targets_scratch_bytes(int sms);
 void max_acc2(cudaStream_t st, int n, const State& s, unsigned long long* out, int sms);
 void direct_targets(cudaStream_t st, int n, const State& s, double eps, int nt,
                     const int32_t* targets, double* out3, double* scratch, int sms);
+// The learned MAC's audit sums: accelerations of rows targets[0 .. nt) from
+// the ns Morton-sorted active bodies of the last force evaluation (sbody,
+// current positions), FP32 pair terms on tile-differenced FP64 coordinates
+// with FP64 accumulation (within ~1e-6 relative of direct_targets).  eps > 0.
+// Returns false (nothing launched) when the sample does not fit the scratch.
+size_t audit_targets_scratch_bytes(int sms);
+bool audit_targets(cudaStream_t st, int ns, const double4* sbody, const State& s, double eps,
+                   int nt, const int32_t* targets, double* out3, double* scratch, int sms);
 
 }  // namespace nb

@@ -125,7 +125,8 @@ struct nb_engine {
     int32_t* targets = nullptr;
     int2* groups = nullptr;
     double* tgt_out = nullptr;
-    double* tgt_part = nullptr;           // FP64 audit chunk partials
+    double* tgt_part = nullptr;           // FP64 force-error chunk partials
+    double* aud_part = nullptr;           // audit chunk partials
     nb::CollideBufs col{};
     Scal* scal = nullptr;
     std::vector<void*> allocs;
@@ -497,6 +498,7 @@ NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
         if ((r = dalloc(h, (char**)&h->part, nb::diag_partial_bytes(capacity)))) break;
         if ((r = dalloc(h, &h->targets, cap)) || (r = dalloc(h, &h->tgt_out, 3 * cap))) break;
         if ((r = dalloc(h, (char**)&h->tgt_part, nb::direct_targets_scratch_bytes(h->sms)))) break;
+        if ((r = dalloc(h, (char**)&h->aud_part, nb::audit_targets_scratch_bytes(h->sms)))) break;
         if ((r = dalloc(h, &h->groups, cap))) break;
         if ((r = dalloc(h, &h->samag, cap))) break;
         if ((r = dalloc(h, &h->mac_node, 2 * cap))) break;
@@ -762,7 +764,7 @@ NB_API int32_t nb_get_state(nb_engine* h, int32_t* n_out, double* px, double* py
 namespace {
 
 int force_error_stats(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
-                      double* out3);
+                      double* out3, bool sorted = false);
 
 // n_steps Verlet steps with one flag set (no audits).
 int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags) {
@@ -886,9 +888,14 @@ NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softenin
         h->mac_since_audit += k;
         if (h->mac_since_audit >= h->mac_audit_every) {
             h->mac_since_audit = 0;
+            // without collisions the last force evaluation's sorted copy of
+            // the active bodies holds the current positions: the audit sums
+            // run on it
+            const bool sorted = (f & NB_MODE_MASK) != NB_MODE_DIRECT_FP64 &&
+                                (f & NB_FLAG_COLLISIONS) == 0;
             double st[3];
             if ((r = force_error_stats(h, h->mac_audit_samples, 0x5EEDull + (uint64_t)h->mac_audits,
-                                       softening, st)))
+                                       softening, st, sorted)))
                 return r;
             h->mac_audits++;
             h->mac_audit_last_rms = st[2];
@@ -986,8 +993,10 @@ __global__ void k_gather_acc(int ns, const int32_t* __restrict__ targets,
     out[3 * k + 2] = az[i];
 }
 
+// sorted: the last force evaluation's sorted copy of the active bodies holds
+// the current positions, and the sums may run on it (the learned MAC's audit)
 int force_error_stats(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
-                      double* out3) {
+                      double* out3, bool sorted) {
     const int n = h->n;
     int r;
     // SplitMix64-driven partial Fisher-Yates: uniform sample without replacement
@@ -1034,7 +1043,10 @@ int force_error_stats(nb_engine* h, int32_t n_samples, uint64_t seed, double sof
         cand.resize(ns);
     }
     if ((r = upload(h, h->targets, cand.data(), sizeof(int32_t) * (size_t)ns))) return r;
-    nb::direct_targets(h->st, n, h->s, softening, ns, h->targets, h->tgt_out, h->tgt_part, h->sms);
+    if (!sorted || !nb::audit_targets(h->st, h->n_active, h->sbody, h->s, softening, ns,
+                                      h->targets, h->tgt_out, h->aud_part, h->sms))
+        nb::direct_targets(h->st, n, h->s, softening, ns, h->targets, h->tgt_out, h->tgt_part,
+                           h->sms);
     std::vector<double> ref((size_t)ns * 3), ax, ay, az;
     if ((r = download(h, ref.data(), h->tgt_out, sizeof(double) * 3 * (size_t)ns))) return r;
     const bool gathered = 3 * (size_t)ns <= (size_t)h->capacity;  // fits the key scratch

@@ -148,6 +148,34 @@ def test_audit_falls_back_to_geometric():
         assert e.counters()[N.C_MAC_EVALS] > 0
 
 
+@pytest.mark.parametrize("samples", [1, 700, 5000])
+def test_audit_sums_match_fp64_force_error(samples):
+    """The in-run audit sums its sample on the force evaluation's sorted copy
+    (FP32 pair terms on tile-differenced FP64 coordinates, FP64 accumulation);
+    its rms and max relative errors equal nb_force_error's FP64 direct-sum
+    figures for the same sample to 1e-4 relative (the audit reference is within
+    ~1e-6 of the FP64 sum, the errors measured are ~1e-3)."""
+    n = 30_000
+    b = scenarios.hernquist(n, seed=24)
+    p, norm, _, _ = _random_model(11)
+    learned = MODE_BARNES_HUT | FLAG_LEARNED_MAC
+    with Engine(n) as e:
+        e.mac_set_params(np.concatenate([p, norm]))
+        e.set_param(N.PARAM_MAC_BUDGET, -3.0)
+        e.set_state(b, old_acc=False)
+        e.step(1, 0.0, 1e-4, MODE_BARNES_HUT)
+        e.set_param(N.PARAM_MAC_AUDIT_INTERVAL, 3)
+        e.set_param(N.PARAM_MAC_AUDIT_SAMPLES, samples)
+        e.set_param(N.PARAM_MAC_AUDIT_RMS, 1e6)
+        e.step(3, 1e-5, 1e-4, learned)
+        st = e.mac_audit_state()
+        assert st["audits"] == 1
+        mean, mx, rms = e.force_error(samples, 0x5EED, 1e-4)
+        assert rms > 0.0
+        assert st["rms"] == pytest.approx(rms, rel=1e-4)
+        assert st["max"] == pytest.approx(mx, rel=1e-4)
+
+
 def test_harvest_train_and_learned_walk():
     """Harvest -> train -> learned walk on a 60K Plummer sphere; the trained
     criterion reaches the geometric walk's error at theta 0.7 (about the
