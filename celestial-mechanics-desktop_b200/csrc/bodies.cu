@@ -135,23 +135,13 @@ k_keys_cube(int n, State s, const double* __restrict__ cube, uint64_t* __restric
             keys[i] = key;
             vals[i] = (uint32_t)i;
         }
-#ifdef NB_KEYS_HIST_PLAIN
+        // plain shared atomics: measured faster than warp-aggregating the
+        // digits with match_any (whose issue cost exceeds the serialisation
+        // of the few same-bin lanes of a clustered system's high digits)
         if (i < n) {
 #pragma unroll
             for (int p = 0; p < 8; p++) atomicAdd(&sh[p][(uint32_t)(key >> (8 * p)) & 0xFF], 1u);
         }
-#else
-        // warp-aggregated (Morton digits of a clustered system pile up in a
-        // few bins)
-#pragma unroll
-        for (int p = 0; p < 8; p++) {
-            const uint32_t d = (uint32_t)(key >> (8 * p)) & 0xFF;
-            const bool live = i < n;
-            const unsigned lm = __ballot_sync(0xFFFFFFFFu, live);
-            const unsigned peers = __match_any_sync(0xFFFFFFFFu, live ? d : 0x100u) & lm;
-            if (live && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][d], (uint32_t)__popc(peers));
-        }
-#endif
     }
     __syncthreads();
     for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) {

@@ -99,7 +99,16 @@ k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* 
 #pragma unroll
     for (int k = 0; k < kSortItems; k++) {
         uint32_t d = (uint32_t)(key[k] >> shift) & 0xFF;
+#ifdef NB_SORT_RANK_BALLOT
+        unsigned peers = 0xFFFFFFFFu;
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const unsigned bal = __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? bal : ~bal;
+        }
+#else
         unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+#endif
         uint32_t before = s_wcnt[warp][d];
         rank[k] = before + __popc(peers & lanemask_lt());
         __syncwarp();

@@ -24,6 +24,8 @@
 // down to level 21, with chains collapsed.
 #include "tree.cuh"
 
+#include <algorithm>
+
 namespace nb {
 
 constexpr int kMarkThreads = 256;
@@ -319,81 +321,96 @@ __global__ void __launch_bounds__(256)
 k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody,
             const float* __restrict__ srad, const double* __restrict__ cube,
             const uint64_t* __restrict__ skeys, const double* __restrict__ sys_half16) {
-    int w = blockIdx.x * blockDim.x + threadIdx.x;
-    int nn = *t.n_nodes;
-    if (w >= nn) return;
-    const int4 lk = __ldg(&t.link[w]);
-    if (lk.y != 0) return;  // internal nodes are reduced by their last child
+    const int nn = *t.n_nodes;
     auto root_half_of = [&](int first) {
         return sys_half16 ? sys_half16[skeys[first] >> kEnsSysShift] : cube[3];
     };
-    int pb = __ldg(&t.parent_bin[w]);
-    {
-        // leaf: moments straight from its bodies
-        const double half = ldexp(root_half_of(lk.z), -__ldg(&t.level[w]));
-        const double4 p0 = sbody[lk.z];
-        Moments mo;
-        float rmax = 0.f;
-        double lo[3] = {p0.x, p0.y, p0.z}, hi[3] = {p0.x, p0.y, p0.z};
+    // persistent grid-stride loop over the nodes: every block stays resident,
+    // so a climbing thread never holds back the start of another block's leaves
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nn; w += gridDim.x * blockDim.x) {
+        const int4 lk = __ldg(&t.link[w]);
+        if (lk.y != 0) continue;  // internal nodes are reduced by their last child
+        int pb = __ldg(&t.parent_bin[w]);
+        {
+            // leaf: moments straight from its bodies
+            const double half = ldexp(root_half_of(lk.z), -__ldg(&t.level[w]));
+            const double4 p0 = sbody[lk.z];
+            Moments mo;
+            float rmax = 0.f;
+            double lo[3] = {p0.x, p0.y, p0.z}, hi[3] = {p0.x, p0.y, p0.z};
 #pragma unroll 4
-        for (int b = lk.z; b < lk.z + lk.w; b++) {
-            const double4 p = sbody[b];
-            mo.add(p.w, p.x - p0.x, p.y - p0.y, p.z - p0.z);
-            if (srad) rmax = fmaxf(rmax, srad[b]);
-            lo[0] = fmin(lo[0], p.x); lo[1] = fmin(lo[1], p.y); lo[2] = fmin(lo[2], p.z);
-            hi[0] = fmax(hi[0], p.x); hi[1] = fmax(hi[1], p.y); hi[2] = fmax(hi[2], p.z);
+            for (int b = lk.z; b < lk.z + lk.w; b++) {
+                const double4 p = sbody[b];
+                mo.add(p.w, p.x - p0.x, p.y - p0.y, p.z - p0.z);
+                if (srad) rmax = fmaxf(rmax, srad[b]);
+                lo[0] = fmin(lo[0], p.x); lo[1] = fmin(lo[1], p.y); lo[2] = fmin(lo[2], p.z);
+                hi[0] = fmax(hi[0], p.x); hi[1] = fmax(hi[1], p.y); hi[2] = fmax(hi[2], p.z);
+            }
+            double4 com;
+            float4 q0;
+            float qyz;
+            mo.finish(p0.x, p0.y, p0.z, com, q0, qyz);
+            t.blo[w] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
+                                   __double2float_rd(lo[2]), 0.f);
+            t.bhi[w] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
+                                   __double2float_ru(hi[2]), 0.f);
+            t.com[w] = com;
+            t.q0[w] = q0;
+            t.q1[w] = make_float4(qyz, (float)half, rmax, 0.f);
         }
-        double4 com;
-        float4 q0;
-        float qyz;
-        mo.finish(p0.x, p0.y, p0.z, com, q0, qyz);
-        t.blo[w] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
-                               __double2float_rd(lo[2]), 0.f);
-        t.bhi[w] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
-                               __double2float_ru(hi[2]), 0.f);
-        t.com[w] = com;
-        t.q0[w] = q0;
-        t.q1[w] = make_float4(qyz, (float)half, rmax, 0.f);
-    }
-    // climb: the last child to arrive reduces the parent
-    for (int guard = 0; pb >= 0 && guard < 64; guard++) {  // <= 22 levels up
-        const int p = __ldg(&t.walk_index[pb]);
-        const int4 pl = __ldg(&t.link[p]);
-        const int plev = __ldg(&t.level[p]);
-        const int ppb = __ldg(&t.parent_bin[p]);
-        __threadfence();  // this thread's node words are visible before its arrival counts
-        if (atomicAdd(&t.counter[p], 1) != pl.y - 1) return;
-        __threadfence();
-        const double root_half = root_half_of(pl.z);
-        const double2 r0a = __ldcg((const double2*)&t.com[pl.x]);
-        const double r0z = __ldcg((const double*)&t.com[pl.x] + 2);
-        Moments mo;
-        float rmax = 0.f;
-        float4 blo = make_float4(3e38f, 3e38f, 3e38f, 0.f), bhi = make_float4(-3e38f, -3e38f, -3e38f, 0.f);
+        // climb: the last child to arrive reduces the parent
+        for (int guard = 0; pb >= 0 && guard < 64; guard++) {  // <= 22 levels up
+            const int p = __ldg(&t.walk_index[pb]);
+            const int4 pl = __ldg(&t.link[p]);
+            const int plev = __ldg(&t.level[p]);
+            const int ppb = __ldg(&t.parent_bin[p]);
+            __threadfence();  // this thread's node words are visible before its arrival counts
+            if (atomicAdd(&t.counter[p], 1) != pl.y - 1) break;
+            __threadfence();
+            const double root_half = root_half_of(pl.z);
+            const double2 r0a = __ldcg((const double2*)&t.com[pl.x]);
+            const double r0z = __ldcg((const double*)&t.com[pl.x] + 2);
+            Moments mo;
+            float rmax = 0.f;
+            float4 blo = make_float4(3e38f, 3e38f, 3e38f, 0.f), bhi = make_float4(-3e38f, -3e38f, -3e38f, 0.f);
 #pragma unroll 2
-        for (int c = pl.x; c < pl.x + pl.y; c++) {
-            const double2 a = __ldcg((const double2*)&t.com[c]);
-            const double2 b = __ldcg((const double2*)&t.com[c] + 1);
-            const float4 c0 = __ldcg(&t.q0[c]);
-            const float4 c1 = __ldcg(&t.q1[c]);
-            const float4 l = __ldcg(&t.blo[c]), h = __ldcg(&t.bhi[c]);
-            mo.add(b.y, a.x - r0a.x, a.y - r0a.y, b.x - r0z);
-            mo.qxx += c0.x; mo.qyy += c0.y; mo.qxy += c0.z; mo.qxz += c0.w; mo.qyz += c1.x;
-            rmax = fmaxf(rmax, c1.z);
-            blo.x = fminf(blo.x, l.x); blo.y = fminf(blo.y, l.y); blo.z = fminf(blo.z, l.z);
-            bhi.x = fmaxf(bhi.x, h.x); bhi.y = fmaxf(bhi.y, h.y); bhi.z = fmaxf(bhi.z, h.z);
+            for (int c = pl.x; c < pl.x + pl.y; c++) {
+                const double2 a = __ldcg((const double2*)&t.com[c]);
+                const double2 b = __ldcg((const double2*)&t.com[c] + 1);
+                const float4 c0 = __ldcg(&t.q0[c]);
+                const float4 c1 = __ldcg(&t.q1[c]);
+                const float4 l = __ldcg(&t.blo[c]), h = __ldcg(&t.bhi[c]);
+                mo.add(b.y, a.x - r0a.x, a.y - r0a.y, b.x - r0z);
+                mo.qxx += c0.x; mo.qyy += c0.y; mo.qxy += c0.z; mo.qxz += c0.w; mo.qyz += c1.x;
+                rmax = fmaxf(rmax, c1.z);
+                blo.x = fminf(blo.x, l.x); blo.y = fminf(blo.y, l.y); blo.z = fminf(blo.z, l.z);
+                bhi.x = fmaxf(bhi.x, h.x); bhi.y = fmaxf(bhi.y, h.y); bhi.z = fmaxf(bhi.z, h.z);
+            }
+            double4 com;
+            float4 q0;
+            float qyz;
+            mo.finish(r0a.x, r0a.y, r0z, com, q0, qyz);
+            t.blo[p] = blo;
+            t.bhi[p] = bhi;
+            t.com[p] = com;
+            t.q0[p] = q0;
+            t.q1[p] = make_float4(qyz, (float)ldexp(root_half, -plev), rmax, 0.f);
+            pb = ppb;
         }
-        double4 com;
-        float4 q0;
-        float qyz;
-        mo.finish(r0a.x, r0a.y, r0z, com, q0, qyz);
-        t.blo[p] = blo;
-        t.bhi[p] = bhi;
-        t.com[p] = com;
-        t.q0[p] = q0;
-        t.q1[p] = make_float4(qyz, (float)ldexp(root_half, -plev), rmax, 0.f);
-        pb = ppb;
     }
+}
+
+// Resident blocks of k_multipole on this device (its persistent grid).
+static int multipole_grid() {
+    static int blocks = 0;
+    if (blocks == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_multipole, 256, 0);
+        blocks = std::max(1, sms) * std::max(1, per_sm);
+    }
+    return blocks;
 }
 
 void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys,
@@ -414,7 +431,8 @@ void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys
     if (m > 0) k_octree_base<<<nblk, kMarkThreads, 0, st>>>(n, t);
     k_octree_emit<<<ceil_div(m > 0 ? m : 1, 256), 256, 0, st>>>(n, t, leaf_cap);
     cudaMemsetAsync(t.counter, 0, sizeof(int) * 2 * (size_t)n, st);
-    k_multipole<<<ceil_div(2 * n, 256), 256, 0, st>>>(n, t, sbody, srad, cube, skeys, sys_half16);
+    k_multipole<<<std::min(ceil_div(2 * n, 256), multipole_grid()), 256, 0, st>>>(
+        n, t, sbody, srad, cube, skeys, sys_half16);
 }
 
 }  // namespace nb
