@@ -19,10 +19,10 @@
 // identical to the CPU reference.
 //
 // Compaction: replaces the ~35-launch scan/scatter of compact_kernel.cu:
-// 191-407 (with a host scan above 262,144 bodies) by one kernel: warp ballot
-// / popc ranks, decoupled look-back across 4096-row tiles, and a scatter of
-// every state field.  Mask is_active && mass > 0 (compact_kernel.cu:39);
-// row order is preserved.
+// 191-407 (with a host scan above 262,144 bodies) by two kernels: warp ballot
+// / popc ranks with a decoupled look-back across 4096-row tiles give every
+// row its destination, then one thread per row moves every state field.
+// Mask is_active && mass > 0 (compact_kernel.cu:39); row order is preserved.
 #include <climits>
 
 #include "collide.cuh"
@@ -427,10 +427,11 @@ k_merge_rounds(State s, const uint64_t* __restrict__ pairs, int np, int max_fram
 
 // ---- compaction ---------------------------------------------------------
 
-template <bool SCATTER>
+// Destination row of every kept row (active with mass > 0), -1 for the rest:
+// a ballot count per warp, a warp-wide decoupled look-back across tiles.
 __global__ void __launch_bounds__(kCompThreads)
-k_compact(int n, State s, State d, int32_t* __restrict__ dest, uint32_t* look,
-          uint32_t* tile_ctr, int* n_kept, int* err) {
+k_compact(int n, State s, int32_t* __restrict__ dest, uint32_t* look, uint32_t* tile_ctr,
+          int* n_kept, int* err) {
     __shared__ int s_tile;
     __shared__ uint32_t s_wtot[kCompThreads / 32];
     __shared__ uint32_t s_base;
@@ -499,28 +500,35 @@ k_compact(int n, State s, State d, int32_t* __restrict__ dest, uint32_t* look,
         const bool keep = (ball[k] >> lane) & 1u;
         const uint32_t pos = off + __popc(ball[k] & lanemask_lt());
         off += __popc(ball[k]);
-        if (i >= n) continue;
-        if (!SCATTER) {
-            dest[i] = keep ? (int32_t)pos : -1;
-            continue;
-        }
-        if (!keep) continue;
-        d.px[pos] = s.px[i]; d.py[pos] = s.py[i]; d.pz[pos] = s.pz[i];
-        d.vx[pos] = s.vx[i]; d.vy[pos] = s.vy[i]; d.vz[pos] = s.vz[i];
-        d.ax[pos] = s.ax[i]; d.ay[pos] = s.ay[i]; d.az[pos] = s.az[i];
-        d.mass[pos] = s.mass[i]; d.radius[pos] = s.radius[i]; d.density[pos] = s.density[i];
-        d.active[pos] = s.active[i]; d.collidable[pos] = s.collidable[i];
-        d.ids[pos] = s.ids[i];
+        if (i < n) dest[i] = keep ? (int32_t)pos : -1;
     }
 }
 
-static void launch_compact(cudaStream_t st, CollideBufs& b, int n, const State& s, const State& d,
-                           int32_t* dest, bool scatter, int* n_kept, int* err) {
+// The kept rows' 15 fields moved to their destination rows: one thread per
+// row, so every field's loads and stores of a warp are in flight together
+// (the rows keep their order, so the stores of a warp are nearly contiguous).
+__global__ void k_scatter_rows(int n, State s, State d, const int32_t* __restrict__ dest) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int pos = dest[i];
+    if (pos < 0) return;
+    d.px[pos] = s.px[i]; d.py[pos] = s.py[i]; d.pz[pos] = s.pz[i];
+    d.vx[pos] = s.vx[i]; d.vy[pos] = s.vy[i]; d.vz[pos] = s.vz[i];
+    d.ax[pos] = s.ax[i]; d.ay[pos] = s.ay[i]; d.az[pos] = s.az[i];
+    d.mass[pos] = s.mass[i]; d.radius[pos] = s.radius[i]; d.density[pos] = s.density[i];
+    d.active[pos] = s.active[i]; d.collidable[pos] = s.collidable[i];
+    d.ids[pos] = s.ids[i];
+}
+
+// dest: n destination rows (-1: removed); with `d` the kept rows are moved
+// into d's rows 0 .. *n_kept - 1.
+static void launch_compact(cudaStream_t st, CollideBufs& b, int n, const State& s,
+                           const State* d, int32_t* dest, int* n_kept, int* err) {
     const int tiles = ceil_div(n, kCompTile);
     cudaMemsetAsync(b.look, 0, sizeof(uint32_t) * (size_t)tiles, st);
     cudaMemsetAsync(b.tile_ctr, 0, sizeof(uint32_t), st);
-    if (scatter) k_compact<true><<<tiles, kCompThreads, 0, st>>>(n, s, d, dest, b.look, b.tile_ctr, n_kept, err);
-    else k_compact<false><<<tiles, kCompThreads, 0, st>>>(n, s, d, dest, b.look, b.tile_ctr, n_kept, err);
+    k_compact<<<tiles, kCompThreads, 0, st>>>(n, s, dest, b.look, b.tile_ctr, n_kept, err);
+    if (d) k_scatter_rows<<<ceil_div(n, 256), 256, 0, st>>>(n, s, *d, dest);
 }
 
 int compact_indices(cudaStream_t st, CollideBufs& b, int n, const uint8_t* active,
@@ -529,7 +537,7 @@ int compact_indices(cudaStream_t st, CollideBufs& b, int n, const uint8_t* activ
     State s{};
     s.active = (uint8_t*)active;
     s.mass = (double*)mass;
-    launch_compact(st, b, n, s, s, dest, false, n_kept_dev, err);
+    launch_compact(st, b, n, s, nullptr, dest, n_kept_dev, err);
     return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 
@@ -548,7 +556,8 @@ int collide_step(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* npairs, i
                                                     a.max_body, a.density_merge, a.min_radius,
                                                     b.merge_count, b.owner, a.n_merges, a.err);
     }
-    launch_compact(st, b, a.n, a.s, a.s_alt, nullptr, true, a.n_kept, a.err);
+    // the merge's owner words are free again: they hold the destination rows
+    launch_compact(st, b, a.n, a.s, &a.s_alt, b.owner, a.n_kept, a.err);
     int host[2] = {0, 0};
     if (cudaMemcpyAsync(&host[0], a.n_kept, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(&host[1], a.n_merges, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
