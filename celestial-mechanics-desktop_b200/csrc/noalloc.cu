@@ -27,10 +27,11 @@ constexpr size_t kAltKeysOff = 0;
 constexpr size_t kAltValsOff = kAltKeysOff + sizeof(uint64_t) * kNoAllocMaxN;
 constexpr size_t kWsOff = kAltValsOff + sizeof(uint32_t) * kNoAllocMaxN;
 // sort workspace for kNoAllocMaxN keys: 8 x 256 histogram words, 8 tile
-// counters, 8 passes x 256 tiles x 256 look-back words (checked at set-up)
-constexpr size_t kWsBytes = sizeof(uint32_t) * (8 * 256 + 8 + 8 * 256 * 256) + 4096;
+// counters, 8 passes x 1024 tiles (of the smallest tile, 1024 keys) x 256
+// look-back words (checked at set-up)
+constexpr size_t kWsBytes = sizeof(uint32_t) * (8 * 256 + 8 + 8 * 1024 * 256) + 4096;
 constexpr size_t kErrOff = (kWsOff + kWsBytes + 255) & ~(size_t)255;
-constexpr size_t kScratchBytes = kErrOff + 256;  // about 14.7 MB
+constexpr size_t kScratchBytes = kErrOff + 256;  // about 21.0 MB
 
 __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 

@@ -5,7 +5,8 @@
 // an unstable shared-memory atomicAdd scatter) with a one-sweep design:
 //   * one histogram kernel computes the digit counts of all 8 passes at once
 //     (fused into the Morton kernel on the tree path);
-//   * each 8-bit pass is a single kernel: tiles of 4096 keys are ranked
+//   * each 8-bit pass is a single kernel: tiles of 4096, 2048 or 1024 keys
+//     (by n: at least two tiles per SM where possible) are ranked
 //     stably in shared memory with warp match/ballot, the per-digit tile
 //     offsets are chained across tiles by decoupled look-back, and keys are
 //     written out digit-run by digit-run from a shared-memory staging copy.
@@ -17,23 +18,31 @@ namespace nb {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+// Keys per thread: 16, 8 or 4 (tiles of 4096, 2048 or 1024 keys), the
+// largest that still gives two tiles per SM, so a pass over a few hundred
+// thousand keys is not left with fewer tiles than SMs.
+constexpr int kSortMinItems = 4;
+constexpr int kSortMinTile = kSortThreads * kSortMinItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPre = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1;
 constexpr int kLookBatch = 8;  // look-back words read per round trip
 
-constexpr int kSortDynSmem = kSortTile * 12;
+template <int ITEMS>
 const void* k_sort_pass_ptr();
 
 void sort_init() {
-    cudaFuncSetAttribute(k_sort_pass_ptr(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kSortDynSmem);
+    cudaFuncSetAttribute(k_sort_pass_ptr<16>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         16 * kSortThreads * 12);
+    cudaFuncSetAttribute(k_sort_pass_ptr<8>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         8 * kSortThreads * 12);
+    cudaFuncSetAttribute(k_sort_pass_ptr<4>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         4 * kSortThreads * 12);
 }
 
+// histograms, tile counters, and look-back words for the smallest tile
 size_t sort_workspace_bytes(int capacity) {
-    size_t tiles = (size_t)ceil_div(capacity > 0 ? capacity : 1, kSortTile);
+    size_t tiles = (size_t)ceil_div(capacity > 0 ? capacity : 1, kSortMinTile);
     return sizeof(uint32_t) * (8 * 256 + 8 + 8 * tiles * 256);
 }
 
@@ -60,12 +69,16 @@ __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
     return *(const volatile uint32_t*)p;
 }
 
-// One stable 8-bit pass.  hist: the 256 global counts of this digit;
-// look: tiles x 256 look-back words (zeroed); tile_ctr: dynamic tile index.
+// One stable 8-bit pass over tiles of ITEMS x 256 keys.  hist: the 256
+// global counts of this digit; look: tiles x 256 look-back words (zeroed);
+// tile_ctr: dynamic tile index.
+template <int ITEMS>
 __global__ void __launch_bounds__(kSortThreads)
 k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
             uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
             const uint32_t* __restrict__ hist, uint32_t* look, uint32_t* tile_ctr, int* err) {
+    constexpr int kSortItems = ITEMS;
+    constexpr int kSortTile = kSortThreads * ITEMS;
     extern __shared__ __align__(16) unsigned char s_dyn[];
     uint64_t* s_keys = (uint64_t*)s_dyn;                 // kSortTile keys
     uint32_t* s_vals = (uint32_t*)(s_dyn + 8 * kSortTile);  // kSortTile values
@@ -83,7 +96,7 @@ k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* 
     const int base = tile * kSortTile;
     const int valid = min(kSortTile, n - base);
 
-    // Load: warp w owns the contiguous segment [base + 512w, base + 512w + 512),
+    // Load: warp w owns the contiguous segment [base + 32 ITEMS w, + 32 ITEMS),
     // item k of lane l is element 32k + l of it, so (warp, k, lane) order is
     // index order and the ranking below is stable.
     uint64_t key[kSortItems];
@@ -220,7 +233,10 @@ k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* 
     }
 }
 
-const void* k_sort_pass_ptr() { return (const void*)k_sort_pass; }
+template <int ITEMS>
+const void* k_sort_pass_ptr() {
+    return (const void*)k_sort_pass<ITEMS>;
+}
 
 // Sort n pairs.  Data starts in (k0, v0); the result ends in (k0, v0) (8
 // passes, even count).  ws: sort_workspace_bytes(capacity) bytes.  When
@@ -236,7 +252,14 @@ cudaError_t sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint6
     uint32_t* hist = (uint32_t*)ws;
     uint32_t* ctr = hist + 8 * 256;
     uint32_t* look = ctr + 8;
-    const int tiles = ceil_div(n, kSortTile);
+#ifdef NB_SORT_ITEMS
+    const int items = NB_SORT_ITEMS;
+#else
+    const int items = ceil_div(n, 16 * kSortThreads) >= 2 * sms  ? 16
+                      : ceil_div(n, 8 * kSortThreads) >= 2 * sms ? 8
+                                                                 : 4;
+#endif
+    const int tiles = ceil_div(n, items * kSortThreads);
     cudaError_t e;
     cudaLaunchConfig_t cfg = {};
     cfg.stream = st;
@@ -258,9 +281,12 @@ cudaError_t sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint6
     uint32_t* vd = v1;
     cfg.gridDim = dim3(tiles);
     cfg.blockDim = dim3(kSortThreads);
-    cfg.dynamicSmemBytes = kSortDynSmem;
+    cfg.dynamicSmemBytes = (size_t)items * kSortThreads * 12;
+    using Pass = void (*)(int, int, const uint64_t*, const uint32_t*, uint64_t*, uint32_t*,
+                          const uint32_t*, uint32_t*, uint32_t*, int*);
+    const Pass pass = items == 16 ? k_sort_pass<16> : items == 8 ? k_sort_pass<8> : k_sort_pass<4>;
     for (int p = 0; p < 8; p++) {
-        if ((e = cudaLaunchKernelEx(&cfg, k_sort_pass, n, 8 * p, (const uint64_t*)ks,
+        if ((e = cudaLaunchKernelEx(&cfg, pass, n, 8 * p, (const uint64_t*)ks,
                                     (const uint32_t*)vs, kd, vd, (const uint32_t*)(hist + 256 * p),
                                     look + (size_t)p * tiles * 256, ctr + p, err)) != cudaSuccess)
             return e;

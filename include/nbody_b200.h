@@ -275,7 +275,7 @@ NB_API int32_t nb_sort_pairs(nb_engine* h, int32_t n, uint64_t* keys, int32_t* v
  * it serves callers that cannot call cudaMalloc - hosts whose device memory
  * is all owned by their own pool allocator, and latency-critical paths where
  * cudaMalloc's device-wide synchronisation is not acceptable.  The scratch is
- * a fixed 14.7 MB __device__ array inside the library, held by every GPU
+ * a fixed 21.0 MB __device__ array inside the library, held by every GPU
  * that loads it until the process exits; n above NB_NOALLOC_SORT_MAX is
  * rejected with NB_ERR_CAPACITY.  The first call on a device looks up that
  * array's address (make it before any stream capture).  All calls share the
