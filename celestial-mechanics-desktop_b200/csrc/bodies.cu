@@ -115,9 +115,14 @@ constexpr int kKeyItems = 8;  // keys per thread: one block's histograms cover 2
 // Cube-mode keys of kKeyItems keys per thread, plus the digit histograms of
 // all 8 sort passes; a block folds its 2048 keys into shared bins and adds
 // the non-zero bins to the global counts (fewer global atomics per key).
+// With `rows`, every row's (x, y, z, m) is also written there in row order,
+// and with `amag` its |a| (the acceleration buffer still holds the previous
+// step's), so the gather after the sort reads one 32-byte record and one
+// word per body instead of seven scattered 8-byte fields.
 __global__ void __launch_bounds__(kKeyThreads)
 k_keys_cube(int n, State s, const double* __restrict__ cube, uint64_t* __restrict__ keys,
-            uint32_t* __restrict__ vals, uint32_t* __restrict__ hist) {
+            uint32_t* __restrict__ vals, uint32_t* __restrict__ hist, double4* __restrict__ rows,
+            float* __restrict__ amag) {
     __shared__ uint32_t sh[8][256];
     for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) (&sh[0][0])[t] = 0;
     __syncthreads();
@@ -128,12 +133,17 @@ k_keys_cube(int n, State s, const double* __restrict__ cube, uint64_t* __restric
         const int i = (blockIdx.x * kKeyItems + k) * kKeyThreads + threadIdx.x;
         uint64_t key = kInactiveKey;
         if (i < n) {
+            const double x = s.px[i], y = s.py[i], z = s.pz[i];
             if (s.active[i])
-                key = (spread21(quant_cube(s.px[i], lx, inv2h)) << 2) |
-                      (spread21(quant_cube(s.py[i], ly, inv2h)) << 1) |
-                      spread21(quant_cube(s.pz[i], lz, inv2h));
+                key = (spread21(quant_cube(x, lx, inv2h)) << 2) |
+                      (spread21(quant_cube(y, ly, inv2h)) << 1) | spread21(quant_cube(z, lz, inv2h));
             keys[i] = key;
             vals[i] = (uint32_t)i;
+            if (rows) rows[i] = make_double4(x, y, z, s.mass[i]);
+            if (amag) {
+                const double ax = s.ax[i], ay = s.ay[i], az = s.az[i];
+                amag[i] = (float)sqrt(ax * ax + ay * ay + az * az);
+            }
         }
         // plain shared atomics: measured faster than warp-aggregating the
         // digits with match_any (whose issue cost exceeds the serialisation
@@ -180,10 +190,17 @@ __global__ void k_keys_aabb(int n, State s, const unsigned long long* __restrict
 
 __global__ void k_gather(int n, State s, const uint32_t* __restrict__ sidx,
                          double4* __restrict__ sbody, float* __restrict__ srad,
-                         float* __restrict__ samag) {
+                         float* __restrict__ samag, const double4* __restrict__ rows,
+                         const float* __restrict__ amag) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t i = sidx[k];
+    if (rows) {
+        sbody[k] = rows[i];
+        if (srad) srad[k] = s.radius ? (float)s.radius[i] : 0.f;
+        if (samag) samag[k] = amag[i];
+        return;
+    }
     sbody[k] = make_double4(s.px[i], s.py[i], s.pz[i], s.mass[i]);
     if (srad) srad[k] = s.radius ? (float)s.radius[i] : 0.f;
     if (samag) {  // |a| of the previous step (acceleration buffer before it is overwritten)
@@ -220,11 +237,12 @@ void launch_cube(cudaStream_t st, const unsigned long long* bbox_ord, const doub
 }
 
 void launch_keys_cube(cudaStream_t st, int n, const State& s, const double* cube,
-                      uint64_t* keys, uint32_t* vals, uint32_t* hist) {
+                      uint64_t* keys, uint32_t* vals, uint32_t* hist, double4* rows,
+                      float* amag) {
     cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, st);
     if (n > 0)
-        k_keys_cube<<<ceil_div(n, kKeyThreads * kKeyItems), kKeyThreads, 0, st>>>(n, s, cube, keys,
-                                                                                  vals, hist);
+        k_keys_cube<<<ceil_div(n, kKeyThreads * kKeyItems), kKeyThreads, 0, st>>>(
+            n, s, cube, keys, vals, hist, rows, amag);
 }
 
 void launch_keys_aabb(cudaStream_t st, int n, const State& s,
@@ -233,8 +251,10 @@ void launch_keys_aabb(cudaStream_t st, int n, const State& s,
 }
 
 void launch_gather(cudaStream_t st, int n, const State& s, const uint32_t* sidx,
-                   double4* sbody, float* srad, float* samag) {
-    if (n > 0) k_gather<<<ceil_div(n, 256), 256, 0, st>>>(n, s, sidx, sbody, srad, samag);
+                   double4* sbody, float* srad, float* samag, const double4* rows,
+                   const float* amag) {
+    if (n > 0)
+        k_gather<<<ceil_div(n, 256), 256, 0, st>>>(n, s, sidx, sbody, srad, samag, rows, amag);
 }
 
 void launch_zero_acc(cudaStream_t st, int n, State s) {

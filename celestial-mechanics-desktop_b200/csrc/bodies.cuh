@@ -25,15 +25,21 @@ void launch_kick(cudaStream_t st, int n, State s, double dt);
 void launch_cube(cudaStream_t st, const unsigned long long* bbox_ord, const double* given,
                  double* cube);
 // Octree-aligned keys in the cube + all 8 digit histograms (hist zeroed).
+// Optionally, by row: rows = (x, y, z, m) and amag = |acc| (the previous
+// step's acceleration), for launch_gather.
 void launch_keys_cube(cudaStream_t st, int n, const State& s, const double* cube,
-                      uint64_t* keys, uint32_t* vals, uint32_t* hist);
+                      uint64_t* keys, uint32_t* vals, uint32_t* hist, double4* rows = nullptr,
+                      float* amag = nullptr);
 // Reference keys: per-axis AABB, scale 2^21-1 (morton_kernel.cu:11-76).
 void launch_keys_aabb(cudaStream_t st, int n, const State& s,
                       const unsigned long long* bbox_ord, uint64_t* keys, uint32_t* vals);
 // Gather the first n sorted rows: sbody = (x, y, z, m), srad = radius,
-// samag = |acc| (optional; the previous step's acceleration).
+// samag = |acc| (optional; the previous step's acceleration).  With `rows`
+// (and `amag` for samag) from launch_keys_cube, each body's record is read
+// whole instead of field by field.
 void launch_gather(cudaStream_t st, int n, const State& s, const uint32_t* sidx,
-                   double4* sbody, float* srad, float* samag = nullptr);
+                   double4* sbody, float* srad, float* samag = nullptr,
+                   const double4* rows = nullptr, const float* amag = nullptr);
 // Zero acc of all rows (inactive rows keep 0).
 void launch_zero_acc(cudaStream_t st, int n, State s);
 

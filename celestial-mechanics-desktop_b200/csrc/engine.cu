@@ -114,6 +114,8 @@ struct nb_engine {
     uint32_t *vals0 = nullptr, *vals1 = nullptr;
     void* sort_ws = nullptr;
     double4* sbody = nullptr;
+    double4* rows4 = nullptr;             // (x, y, z, m) by row, for the gather
+    float* amag_rows = nullptr;           // |a| of the previous step by row
     float* srad = nullptr;
     void* tree_mem = nullptr;
     nb::TreeBufs tree{};
@@ -276,12 +278,14 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     if (learned && !h->mac_ready)
         return fail(h, NB_ERR_STATE, "the learned MAC has no trained parameters");
     nb::launch_cube(h->st, sc->bbox_ord, nullptr, sc->cube);
-    nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws);
+    // the keys kernel also writes each row's (x, y, z, m) record and, for the
+    // learned MAC, the previous step's |a| (before the buffer is zeroed)
+    nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws,
+                         h->rows4, learned ? h->amag_rows : nullptr);
     nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err,
                    h->sms);
-    // the gather reads the previous step's |a| before the buffer is zeroed
     nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, radii ? h->srad : nullptr,
-                      learned ? h->samag : nullptr);
+                      learned ? h->samag : nullptr, h->rows4, h->amag_rows);
     nb::launch_zero_acc(h->st, n, h->s);
     record(h, 1);
     if (mode == NB_MODE_DIRECT) {
@@ -491,6 +495,7 @@ NB_API int32_t nb_create(int32_t capacity, int32_t device, nb_engine** out) {
         if ((r = dalloc(h, &h->vals0, cap)) || (r = dalloc(h, &h->vals1, cap))) break;
         if ((r = dalloc(h, (char**)&h->sort_ws, nb::sort_workspace_bytes(capacity)))) break;
         if ((r = dalloc(h, &h->sbody, cap)) || (r = dalloc(h, &h->srad, cap))) break;
+        if ((r = dalloc(h, &h->rows4, cap)) || (r = dalloc(h, &h->amag_rows, cap))) break;
         if ((r = dalloc(h, (char**)&h->tree_mem, nb::tree_bytes(capacity)))) break;
         nb::tree_carve(h->tree, h->tree_mem, capacity);
         if ((r = dalloc(h, (char**)&h->front, nb::walk_front_bytes(h->wcfg)))) break;

@@ -7,7 +7,7 @@
 //     (fused into the Morton kernel on the tree path);
 //   * each 8-bit pass is a single kernel: tiles of 4096, 2048 or 1024 keys
 //     (by n: at least two tiles per SM where possible) are ranked
-//     stably in shared memory with warp match/ballot, the per-digit tile
+//     stably in shared memory with warp ballots, the per-digit tile
 //     offsets are chained across tiles by decoupled look-back, and keys are
 //     written out digit-run by digit-run from a shared-memory staging copy.
 // Every look-back spin is bounded (kSpinLimit); on expiry the kernel records
@@ -112,16 +112,14 @@ k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* 
 #pragma unroll
     for (int k = 0; k < kSortItems; k++) {
         uint32_t d = (uint32_t)(key[k] >> shift) & 0xFF;
-#ifdef NB_SORT_RANK_BALLOT
+        // lanes with this lane's digit: one ballot per digit bit (measured
+        // faster than match_any, whose issue cost stalls the low-digit passes)
         unsigned peers = 0xFFFFFFFFu;
 #pragma unroll
         for (int b = 0; b < 8; b++) {
             const unsigned bal = __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u);
             peers &= ((d >> b) & 1u) ? bal : ~bal;
         }
-#else
-        unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
-#endif
         uint32_t before = s_wcnt[warp][d];
         rank[k] = before + __popc(peers & lanemask_lt());
         __syncwarp();

@@ -16,9 +16,10 @@
 //      its <= 3-deep binary subtree inside the same cell, in key order.
 //   3. block scan of the child counts gives every walk-internal node a
 //      contiguous child slot range; k_octree_emit writes the nodes.
-//   4. k_multipole: bottom-up, the last child to arrive at a parent computes
-//      the parent (arrival counters), so each node is reduced exactly once
-//      from its children in child order: deterministic.
+//   4. k_multipole_leaves / k_multipole_climb: leaves from their bodies, then
+//      bottom-up, the last child to arrive at a parent computes the parent
+//      (arrival counters), so each node is reduced exactly once from its
+//      children in child order: deterministic.
 // With leaf_cap = 1 the walk tree is the reference's point-region octree
 // (OctreeBuilder::insert_body, engine/src/physics/octree_builder.cpp:50-105)
 // down to level 21, with chains collapsed.
@@ -41,6 +42,7 @@ size_t tree_bytes(int cap) {
     size_t w = 2 * c;
     b += w * 16 + w * 4 + w * 4 + w * 32 + w * 16 + w * 16 + w * 4 + 16;
     b += 2 * w * 16;                                                   // body boxes
+    b += c * 4 + 16;                                                   // leaf list
     return b + 16 * 64;
 }
 
@@ -65,6 +67,8 @@ void tree_carve(TreeBufs& t, void* base, int cap) {
     t.parent_bin = carve<int>(p, w);
     t.counter = carve<int>(p, w);
     t.n_nodes = carve<int>(p, 4);
+    t.leaves = carve<int>(p, c);
+    t.n_leaves = carve<int>(p, 4);
     t.bchild = carve<int>(p, 2 * c);
     t.bfirst = carve<int>(p, c);
     t.blast = carve<int>(p, c);
@@ -312,102 +316,124 @@ struct Moments {
 // sys_half16: batched systems (keys carry the system in their top bits): the
 // half-size of each system's cube times 2^4, the half-size its level-0 cell
 // would have; null for one system in `cube`.
-// One thread per walk node: a leaf reduces its bodies in one pass, then the
-// thread climbs; the last child to arrive at a parent reduces it from its
-// children in child order (deterministic).  Per level the climb makes three
-// dependent L2 trips: the parent's walk index; its link / level / parent words
-// together with the arrival atomic; every child word in one loop.
+// Multipoles in two kernels.  k_multipole_leaves: every leaf reduces its
+// bodies in one pass (a persistent grid-stride loop, nothing waits) and enters
+// the leaf list.  k_multipole_climb: one thread per leaf, all resident at
+// once, climbs; the last child to arrive at a parent reduces it from its
+// children in child order, so the result does not depend on which thread
+// arrives last (deterministic).  Per level a climb makes three dependent L2
+// trips: the parent's walk index; its link / level / parent words together
+// with the arrival atomic; every child word in one loop.  (Computing the
+// leaves inside the climbing threads left the last blocks' leaves waiting for
+// resident blocks to drain, so the root finished a whole wave of climbs late.)
 __global__ void __launch_bounds__(256)
-k_multipole(int n, TreeBufs t, const double4* __restrict__ sbody,
-            const float* __restrict__ srad, const double* __restrict__ cube,
-            const uint64_t* __restrict__ skeys, const double* __restrict__ sys_half16) {
+k_multipole_leaves(TreeBufs t, const double4* __restrict__ sbody,
+                   const float* __restrict__ srad, const double* __restrict__ cube,
+                   const uint64_t* __restrict__ skeys, const double* __restrict__ sys_half16) {
     const int nn = *t.n_nodes;
-    auto root_half_of = [&](int first) {
-        return sys_half16 ? sys_half16[skeys[first] >> kEnsSysShift] : cube[3];
-    };
-    // persistent grid-stride loop over the nodes: every block stays resident,
-    // so a climbing thread never holds back the start of another block's leaves
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nn; w += gridDim.x * blockDim.x) {
         const int4 lk = __ldg(&t.link[w]);
-        if (lk.y != 0) continue;  // internal nodes are reduced by their last child
-        int pb = __ldg(&t.parent_bin[w]);
-        {
-            // leaf: moments straight from its bodies
-            const double half = ldexp(root_half_of(lk.z), -__ldg(&t.level[w]));
-            const double4 p0 = sbody[lk.z];
-            Moments mo;
-            float rmax = 0.f;
-            double lo[3] = {p0.x, p0.y, p0.z}, hi[3] = {p0.x, p0.y, p0.z};
+        const bool leaf = lk.y == 0;
+        const unsigned am = __activemask();
+        const unsigned lm = __ballot_sync(am, leaf);
+        int slot = 0;
+        const int lead = __ffs(am) - 1;
+        if ((threadIdx.x & 31) == lead && lm) slot = atomicAdd(t.n_leaves, __popc(lm));
+        slot = __shfl_sync(am, slot, lead);
+        if (!leaf) continue;
+        t.leaves[slot + __popc(lm & lanemask_lt())] = w;
+        const double root_half =
+            sys_half16 ? sys_half16[skeys[lk.z] >> kEnsSysShift] : cube[3];
+        const double half = ldexp(root_half, -__ldg(&t.level[w]));
+        const double4 p0 = sbody[lk.z];
+        Moments mo;
+        float rmax = 0.f;
+        double lo[3] = {p0.x, p0.y, p0.z}, hi[3] = {p0.x, p0.y, p0.z};
 #pragma unroll 4
-            for (int b = lk.z; b < lk.z + lk.w; b++) {
-                const double4 p = sbody[b];
-                mo.add(p.w, p.x - p0.x, p.y - p0.y, p.z - p0.z);
-                if (srad) rmax = fmaxf(rmax, srad[b]);
-                lo[0] = fmin(lo[0], p.x); lo[1] = fmin(lo[1], p.y); lo[2] = fmin(lo[2], p.z);
-                hi[0] = fmax(hi[0], p.x); hi[1] = fmax(hi[1], p.y); hi[2] = fmax(hi[2], p.z);
-            }
-            double4 com;
-            float4 q0;
-            float qyz;
-            mo.finish(p0.x, p0.y, p0.z, com, q0, qyz);
-            t.blo[w] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
-                                   __double2float_rd(lo[2]), 0.f);
-            t.bhi[w] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
-                                   __double2float_ru(hi[2]), 0.f);
-            t.com[w] = com;
-            t.q0[w] = q0;
-            t.q1[w] = make_float4(qyz, (float)half, rmax, 0.f);
+        for (int b = lk.z; b < lk.z + lk.w; b++) {
+            const double4 p = sbody[b];
+            mo.add(p.w, p.x - p0.x, p.y - p0.y, p.z - p0.z);
+            if (srad) rmax = fmaxf(rmax, srad[b]);
+            lo[0] = fmin(lo[0], p.x); lo[1] = fmin(lo[1], p.y); lo[2] = fmin(lo[2], p.z);
+            hi[0] = fmax(hi[0], p.x); hi[1] = fmax(hi[1], p.y); hi[2] = fmax(hi[2], p.z);
         }
-        // climb: the last child to arrive reduces the parent
-        for (int guard = 0; pb >= 0 && guard < 64; guard++) {  // <= 22 levels up
-            const int p = __ldg(&t.walk_index[pb]);
-            const int4 pl = __ldg(&t.link[p]);
-            const int plev = __ldg(&t.level[p]);
-            const int ppb = __ldg(&t.parent_bin[p]);
-            __threadfence();  // this thread's node words are visible before its arrival counts
-            if (atomicAdd(&t.counter[p], 1) != pl.y - 1) break;
-            __threadfence();
-            const double root_half = root_half_of(pl.z);
-            const double2 r0a = __ldcg((const double2*)&t.com[pl.x]);
-            const double r0z = __ldcg((const double*)&t.com[pl.x] + 2);
-            Moments mo;
-            float rmax = 0.f;
-            float4 blo = make_float4(3e38f, 3e38f, 3e38f, 0.f), bhi = make_float4(-3e38f, -3e38f, -3e38f, 0.f);
-#pragma unroll 2
-            for (int c = pl.x; c < pl.x + pl.y; c++) {
-                const double2 a = __ldcg((const double2*)&t.com[c]);
-                const double2 b = __ldcg((const double2*)&t.com[c] + 1);
-                const float4 c0 = __ldcg(&t.q0[c]);
-                const float4 c1 = __ldcg(&t.q1[c]);
-                const float4 l = __ldcg(&t.blo[c]), h = __ldcg(&t.bhi[c]);
-                mo.add(b.y, a.x - r0a.x, a.y - r0a.y, b.x - r0z);
-                mo.qxx += c0.x; mo.qyy += c0.y; mo.qxy += c0.z; mo.qxz += c0.w; mo.qyz += c1.x;
-                rmax = fmaxf(rmax, c1.z);
-                blo.x = fminf(blo.x, l.x); blo.y = fminf(blo.y, l.y); blo.z = fminf(blo.z, l.z);
-                bhi.x = fmaxf(bhi.x, h.x); bhi.y = fmaxf(bhi.y, h.y); bhi.z = fmaxf(bhi.z, h.z);
-            }
-            double4 com;
-            float4 q0;
-            float qyz;
-            mo.finish(r0a.x, r0a.y, r0z, com, q0, qyz);
-            t.blo[p] = blo;
-            t.bhi[p] = bhi;
-            t.com[p] = com;
-            t.q0[p] = q0;
-            t.q1[p] = make_float4(qyz, (float)ldexp(root_half, -plev), rmax, 0.f);
-            pb = ppb;
-        }
+        double4 com;
+        float4 q0;
+        float qyz;
+        mo.finish(p0.x, p0.y, p0.z, com, q0, qyz);
+        t.blo[w] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]),
+                               __double2float_rd(lo[2]), 0.f);
+        t.bhi[w] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]),
+                               __double2float_ru(hi[2]), 0.f);
+        t.com[w] = com;
+        t.q0[w] = q0;
+        t.q1[w] = make_float4(qyz, (float)half, rmax, 0.f);
     }
 }
 
-// Resident blocks of k_multipole on this device (its persistent grid).
-static int multipole_grid() {
+#ifndef NB_CLIMB_THREADS
+#define NB_CLIMB_THREADS 128
+#endif
+#ifndef NB_CLIMB_MIN_BLOCKS
+#define NB_CLIMB_MIN_BLOCKS 6
+#endif
+constexpr int kClimbThreads = NB_CLIMB_THREADS;
+
+__global__ void __launch_bounds__(kClimbThreads, NB_CLIMB_MIN_BLOCKS)
+k_multipole_climb(TreeBufs t, const double* __restrict__ cube,
+                  const uint64_t* __restrict__ skeys, const double* __restrict__ sys_half16) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *t.n_leaves) return;
+    int pb = __ldg(&t.parent_bin[t.leaves[i]]);
+    for (int guard = 0; pb >= 0 && guard < 64; guard++) {  // <= 22 levels up
+        const int p = __ldg(&t.walk_index[pb]);
+        const int4 pl = __ldg(&t.link[p]);
+        const int plev = __ldg(&t.level[p]);
+        const int ppb = __ldg(&t.parent_bin[p]);
+        __threadfence();  // this thread's node words are visible before its arrival counts
+        if (atomicAdd(&t.counter[p], 1) != pl.y - 1) return;
+        __threadfence();
+        const double root_half = sys_half16 ? sys_half16[skeys[pl.z] >> kEnsSysShift] : cube[3];
+        const double2 r0a = __ldcg((const double2*)&t.com[pl.x]);
+        const double r0z = __ldcg((const double*)&t.com[pl.x] + 2);
+        Moments mo;
+        float rmax = 0.f;
+        float4 blo = make_float4(3e38f, 3e38f, 3e38f, 0.f);
+        float4 bhi = make_float4(-3e38f, -3e38f, -3e38f, 0.f);
+#pragma unroll 2
+        for (int c = pl.x; c < pl.x + pl.y; c++) {
+            const double2 a = __ldcg((const double2*)&t.com[c]);
+            const double2 b = __ldcg((const double2*)&t.com[c] + 1);
+            const float4 c0 = __ldcg(&t.q0[c]);
+            const float4 c1 = __ldcg(&t.q1[c]);
+            const float4 l = __ldcg(&t.blo[c]), h = __ldcg(&t.bhi[c]);
+            mo.add(b.y, a.x - r0a.x, a.y - r0a.y, b.x - r0z);
+            mo.qxx += c0.x; mo.qyy += c0.y; mo.qxy += c0.z; mo.qxz += c0.w; mo.qyz += c1.x;
+            rmax = fmaxf(rmax, c1.z);
+            blo.x = fminf(blo.x, l.x); blo.y = fminf(blo.y, l.y); blo.z = fminf(blo.z, l.z);
+            bhi.x = fmaxf(bhi.x, h.x); bhi.y = fmaxf(bhi.y, h.y); bhi.z = fmaxf(bhi.z, h.z);
+        }
+        double4 com;
+        float4 q0;
+        float qyz;
+        mo.finish(r0a.x, r0a.y, r0z, com, q0, qyz);
+        t.blo[p] = blo;
+        t.bhi[p] = bhi;
+        t.com[p] = com;
+        t.q0[p] = q0;
+        t.q1[p] = make_float4(qyz, (float)ldexp(root_half, -plev), rmax, 0.f);
+        pb = ppb;
+    }
+}
+
+// Resident blocks of k_multipole_leaves on this device (its persistent grid).
+static int leaves_grid() {
     static int blocks = 0;
     if (blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_multipole, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_multipole_leaves, 256, 0);
         blocks = std::max(1, sms) * std::max(1, per_sm);
     }
     return blocks;
@@ -431,8 +457,12 @@ void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys
     if (m > 0) k_octree_base<<<nblk, kMarkThreads, 0, st>>>(n, t);
     k_octree_emit<<<ceil_div(m > 0 ? m : 1, 256), 256, 0, st>>>(n, t, leaf_cap);
     cudaMemsetAsync(t.counter, 0, sizeof(int) * 2 * (size_t)n, st);
-    k_multipole<<<std::min(ceil_div(2 * n, 256), multipole_grid()), 256, 0, st>>>(
-        n, t, sbody, srad, cube, skeys, sys_half16);
+    cudaMemsetAsync(t.n_leaves, 0, sizeof(int), st);
+    k_multipole_leaves<<<std::min(ceil_div(2 * n, 256), leaves_grid()), 256, 0, st>>>(
+        t, sbody, srad, cube, skeys, sys_half16);
+    // at most n leaves (each holds a body); the threads past the count return
+    k_multipole_climb<<<ceil_div(n, kClimbThreads), kClimbThreads, 0, st>>>(t, cube, skeys,
+                                                                             sys_half16);
 }
 
 }  // namespace nb

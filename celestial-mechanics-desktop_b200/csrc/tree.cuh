@@ -28,6 +28,8 @@ struct TreeBufs {
     float4* blo;        // bounding box of the node's bodies (xyz, rounded outwards)
     float4* bhi;
     int* counter;       // bottom-up arrival counters
+    int* leaves;        // walk index of every leaf (multipole pass, any order)
+    int* n_leaves;      // device leaf count
     int* n_nodes;       // device node count
     int capacity;       // bodies
 };
