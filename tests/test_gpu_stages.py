@@ -44,10 +44,10 @@ def test_morton_degenerate_box(engine, oracle):
 
 
 @pytest.mark.parametrize("n,dup", [(0, 0), (1, 0), (2, 1), (4095, 0), (4097, 1), (300_001, 1),
-                                   (1_000_003, 1), (2_000_000, 0)])
+                                   (400_003, 0), (1_000_003, 1), (2_000_000, 0)])
 def test_stable_sort_bit_exact(engine, oracle, n, dup):
-    """Tiles of 1024 keys (4097, 300,001), 2048 (1,000,003) and 4096 (2M) on a
-    148-SM B200; duplicates and sentinel keys keep their input order."""
+    """Tiles of 1024 keys (4097, 300,001), 2048 (400,003) and 4096 (1,000,003,
+    2M) on a 148-SM B200; duplicates and sentinel keys keep their input order."""
     rng = np.random.Generator(np.random.PCG64(n))
     if dup:
         keys = rng.integers(0, 300, n).astype(np.uint64) * np.uint64(0x0123456789AB)
