@@ -240,7 +240,7 @@ def run_reference(args, ws, rank):
     err = oracle.force_error((acc[0][t], acc[1][t], acc[2][t]), want)
     sample = (f"N={args.n:,} Plummer seed 1: {steps} full force evaluations (serial tree build "
               f"+ parallel walk, theta 0.5, monopole), {warm} warm-up")
-    ref_gpu = reference_gpu_context(b)
+    ref_gpu = reference_gpu_context(b, t, want)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * total / steps,
@@ -259,13 +259,16 @@ def run_reference(args, ws, rank):
     }))
 
 
-def reference_gpu_context(b):
-    """Two of the reference's own CUDA kernels built for this GPU
+def reference_gpu_context(b, rows=None, want=None):
+    """The reference's own CUDA paths built for this GPU
     (oracle/_ref/libcelestial_ref_gpu.so), for context beside the CPU
     timing: the FP64 tiled gravity kernel on the FP64 direct-sum workload
-    (N = 1000) and on the headline sphere (one launch at N = 2^20), and the
-    radix sort on that sphere's 1,048,576 keys (its time, and whether its
-    output is sorted and stable).  None when the library or a GPU is absent."""
+    (N = 1000) and on the headline sphere (one launch at N = 2^20), the radix
+    sort on that sphere's 1,048,576 keys (its time, and whether its output is
+    sorted and stable), and GpuTreeSolver::compute_forces on the sphere (one
+    timed evaluation after an untimed one; its force error on `rows` against
+    the FP64 direct sum `want` when given).  None when the library or a GPU
+    is absent."""
     import oracle
     from nbody_b200 import scenarios
 
@@ -294,6 +297,16 @@ def reference_gpu_context(b):
     out["radix_sort_n1048576"] = {"ms": ms, "sorted": ok_sorted,
                                   "stable": bool(np.array_equal(v, want_v)),
                                   "keys_out_of_order": int(np.count_nonzero(k[1:] < k[:-1]))}
+    acc, ms, build, trav = oracle.ref_gpu_tree(b.px, b.py, b.pz, b.mass, b.active, EPS, THETA,
+                                               reps=1)
+    tree = {"ms_per_evaluation": ms, "steps_per_s": 1e3 / ms, "sort_build_ms": build,
+            "traversal_ms": trav,
+            "note": "GpuTreeSolver::compute_forces, theta 0.5 monopole FP64: single-thread tree "
+                    "insertion, per-body walk"}
+    if rows is not None and want is not None:
+        e = oracle.force_error((acc[0][rows], acc[1][rows], acc[2][rows]), want)
+        tree["force_error"] = {"mean": e[0], "max": e[1], "rms": e[2]}
+    out["gpu_tree_solver_n1048576"] = tree
     return out
 
 

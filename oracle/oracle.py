@@ -90,6 +90,7 @@ _REF_SIGS = {
 _REF_GPU_SIGS = {
     "ref_gpu_gravity": (i32, [i32, P, P, P, P, P, f64, i32, P, P, P, P]),
     "ref_gpu_radix_sort": (i32, [i32, P, P, P]),
+    "ref_gpu_tree": (i32, [i32, P, P, P, P, P, f64, f64, i32, P, P, P, P, P, P]),
 }
 
 _lib = None
@@ -137,6 +138,23 @@ def ref_gpu_gravity(px, py, pz, m, active, eps, reps=3):
     if r != 0:
         raise RuntimeError("reference gravity kernel failed")
     return (ax, ay, az), float(ms[0])
+
+
+def ref_gpu_tree(px, py, pz, m, active, eps, theta=0.5, reps=1):
+    """The reference's GpuTreeSolver::compute_forces on the current GPU (one
+    untimed evaluation, then `reps` timed ones): the accelerations, the mean
+    time per evaluation (ms, CUDA events) and the solver's own
+    sort+build / traversal split of the last one (ms, host clock)."""
+    n = len(px)
+    px, py, pz, m = map(_f, (px, py, pz, m))
+    act = _u8(active)
+    ax, ay, az = np.empty(n), np.empty(n), np.empty(n)
+    ms, build, trav = np.zeros(1), np.zeros(1), np.zeros(1)
+    r = ref_gpu().ref_gpu_tree(n, _p(px), _p(py), _p(pz), _p(m), _p(act), eps, theta, int(reps),
+                               _p(ax), _p(ay), _p(az), _p(ms), _p(build), _p(trav))
+    if r != 0:
+        raise RuntimeError("reference GPU tree solver failed")
+    return (ax, ay, az), float(ms[0]), float(build[0]), float(trav[0])
 
 
 def ref_gpu_radix_sort(keys, values):
