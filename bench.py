@@ -297,12 +297,10 @@ def reference_gpu_context(b, rows=None, want=None):
     out["radix_sort_n1048576"] = {"ms": ms, "sorted": ok_sorted,
                                   "stable": bool(np.array_equal(v, want_v)),
                                   "keys_out_of_order": int(np.count_nonzero(k[1:] < k[:-1]))}
-    acc, ms, build, trav = oracle.ref_gpu_tree(b.px, b.py, b.pz, b.mass, b.active, EPS, THETA,
-                                               reps=1)
-    tree = {"ms_per_evaluation": ms, "steps_per_s": 1e3 / ms, "sort_build_ms": build,
-            "traversal_ms": trav,
+    acc, ms, _, _ = oracle.ref_gpu_tree(b.px, b.py, b.pz, b.mass, b.active, EPS, THETA, reps=1)
+    tree = {"ms_per_evaluation": ms, "steps_per_s": 1e3 / ms,
             "note": "GpuTreeSolver::compute_forces, theta 0.5 monopole FP64: single-thread tree "
-                    "insertion, per-body walk"}
+                    "insertion, per-body walk; CUDA events around the whole call"}
     if rows is not None and want is not None:
         e = oracle.force_error((acc[0][rows], acc[1][rows], acc[2][rows]), want)
         tree["force_error"] = {"mean": e[0], "max": e[1], "rms": e[2]}
@@ -497,6 +495,8 @@ def run_b200(args, ws, rank, local, trained=None):
     eng = Engine(max(n, N_BODIES), device=dev)
     if args.group_span is not None:
         eng.set_param(N.PARAM_GROUP_SPAN, int(args.group_span))
+    if args.group_bodies is not None:
+        eng.set_param(N.PARAM_GROUP_BODIES, int(args.group_bodies))
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     geo, learned = MODE_BARNES_HUT, MODE_BARNES_HUT | FLAG_LEARNED_MAC
 
@@ -676,6 +676,8 @@ def run_theta05(args, ws, rank, local):
     eng = Engine(n, device=dev)
     if args.group_span is not None:
         eng.set_param(N.PARAM_GROUP_SPAN, int(args.group_span))
+    if args.group_bodies is not None:
+        eng.set_param(N.PARAM_GROUP_BODIES, int(args.group_bodies))
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     eng.set_param(N.PARAM_THETA, THETA)
     arm = timed_arm(eng, b, stream, args, ws, dev, mode, N, mode,
@@ -1208,6 +1210,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--group-bodies", type=int, default=None, choices=[32, 64],
+                    help="bodies per walk group (NB_PARAM_GROUP_BODIES; 64: two per lane)")
     ap.add_argument("--group-span", type=int, default=None,
                     help="walk groups: runs of 32 bodies cut from cells of at most this many "
                          "bodies (NB_PARAM_GROUP_SPAN; 0 = sibling packing)")

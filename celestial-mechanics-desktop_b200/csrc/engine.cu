@@ -137,12 +137,13 @@ struct nb_engine {
     // captured single step (CUDA graph) and the parameters it was captured with
     cudaGraphExec_t graph_exec = nullptr;
     struct GraphKey {
-        int flags, n, n_active, leaf_cap, span;
+        int flags, n, n_active, leaf_cap, span, bodies;
         double dt, eps, theta, pack, mac_lo, mac_hi, mac_budget;
         const double* state;  // the state arrays swap after a compaction
         bool operator==(const GraphKey& o) const {
             return flags == o.flags && n == o.n && n_active == o.n_active &&
-                   leaf_cap == o.leaf_cap && span == o.span && dt == o.dt && eps == o.eps && theta == o.theta &&
+                   leaf_cap == o.leaf_cap && span == o.span && bodies == o.bodies && dt == o.dt &&
+                   eps == o.eps && theta == o.theta &&
                    pack == o.pack && mac_lo == o.mac_lo && mac_hi == o.mac_hi &&
                    mac_budget == o.mac_budget && state == o.state;
         }
@@ -318,8 +319,8 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
         a.groups = h->groups;
         a.n_groups = &sc->n_groups;
         a.pack = h->group_pack;
-    a.group_span = h->group_span;
         a.group_span = h->group_span;
+        a.group_size = h->group_bodies;
         a.counters = sc->counters;
         a.err = sc->err;
         if (ref) {
@@ -371,7 +372,8 @@ int sub_steps(int flags, double dt, double* sub) {
 // timing events are not recorded inside the graph.
 int step_graph(nb_engine* h, int flags, double dt, double eps) {
     const nb_engine::GraphKey key{flags,           h->n,           h->n_active,
-                                  h->leaf_cap,     h->group_span,  dt,             eps,
+                                  h->leaf_cap,     h->group_span,  h->group_bodies,
+                                  dt,              eps,
                                   h->theta,        h->group_pack,  h->mac_theta_lo,
                                   h->mac_theta_hi, h->mac_budget,  h->s.px};
     if (h->graph_exec && key == h->graph_key) return NB_OK;
@@ -624,7 +626,7 @@ NB_API int32_t nb_set_param_i32(nb_engine* h, int32_t p, int32_t v) {
             h->group_span = v;
             return NB_OK;
         case NB_PARAM_GROUP_BODIES:
-            if (v != 32) return fail(h, NB_ERR_INVALID_ARG, "group size must be 32");
+            if (v != 32 && v != 64) return fail(h, NB_ERR_INVALID_ARG, "group size must be 32 or 64");
             h->group_bodies = v;
             return NB_OK;
         default: return fail(h, NB_ERR_INVALID_ARG, "unknown i32 parameter %d", p);
@@ -962,8 +964,8 @@ NB_API int32_t nb_diagnostics(nb_engine* h, double softening, int32_t pe_mode, d
         a.groups = h->groups;
         a.n_groups = &sc->n_groups;
         a.pack = h->group_pack;
-    a.group_span = h->group_span;
         a.group_span = h->group_span;
+        a.group_size = h->group_bodies;
         a.counters = nullptr;
         a.err = sc->err;
         nb::walk_group(h->st, h->wcfg, a, true, false, true);
@@ -1363,6 +1365,7 @@ NB_API int32_t nb_mac_harvest(nb_engine* h, int32_t max_records, double sample_f
     a.n_groups = &sc->n_groups;
     a.pack = h->group_pack;
     a.group_span = h->group_span;
+    a.group_size = h->group_bodies;
     a.counters = sc->counters;
     a.err = sc->err;
     a.theta2 = h->mac_theta_lo * h->mac_theta_lo;

@@ -22,6 +22,8 @@
 //     silently.
 #include "walk.cuh"
 
+#include <algorithm>
+
 namespace nb {
 
 constexpr int kWalkWarps = 8;
@@ -84,19 +86,41 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
 // blocks per SM, 1 = 4 warps x 6 blocks per SM (the same warps per SM in
 // smaller blocks; the ensembles' autotuner picks one).
 constexpr int kWalkWarpsSmall = 4;
-template <int MAC, int SHAPE>
+// GS = 64 (groups of up to 64 bodies, two per lane): more work per warp and
+// more live registers, so fewer and larger-register warps per SM.
+#ifndef NB_WALK64_WARPS
+#define NB_WALK64_WARPS 8
+#endif
+#ifndef NB_WALK64_BLOCKS
+#define NB_WALK64_BLOCKS 2
+#endif
+#ifndef NB_WALK64_MAC_WARPS
+#define NB_WALK64_MAC_WARPS 4
+#endif
+#ifndef NB_WALK64_MAC_BLOCKS
+#define NB_WALK64_MAC_BLOCKS 4
+#endif
+constexpr int kMacWarps64 = NB_WALK64_MAC_WARPS;
+constexpr int kWalkSmemMac64 = kMacWarps64 * (kWarpFloats + kMacWarpWords) * 4;
+constexpr int kWalkSmem64 = NB_WALK64_WARPS * kWarpFloats * 4;
+static_assert(NB_WALK64_MAC_BLOCKS * (kWalkSmemMac64 + 1024) <= 228 * 1024, "learned walk blocks");
+static_assert(kMacWarps64 <= kWalkWarps && NB_WALK64_WARPS <= kWalkWarps,
+              "the stacks are sized for the geometric block shape");
+template <int MAC, int SHAPE, int GS = 32>
 struct WalkShape {
     static constexpr int warps =
-        MAC == kMacLearned ? kMacWarps : (SHAPE == 1 ? kWalkWarpsSmall : kWalkWarps);
+        GS == 64 ? (MAC == kMacLearned ? kMacWarps64 : NB_WALK64_WARPS)
+                 : (MAC == kMacLearned ? kMacWarps : (SHAPE == 1 ? kWalkWarpsSmall : kWalkWarps));
     static constexpr int min_blocks =
-        MAC == kMacLearned ? NB_WALK_MAC_BLOCKS : (SHAPE == 1 ? 6 : 3);
+        GS == 64 ? (MAC == kMacLearned ? NB_WALK64_MAC_BLOCKS : NB_WALK64_BLOCKS)
+                 : (MAC == kMacLearned ? NB_WALK_MAC_BLOCKS : (SHAPE == 1 ? 6 : 3));
 };
 
-template <bool QUAD, bool SHELL, bool POT, bool GUARD, int MAC, int SHAPE = 0>
-__global__ void __launch_bounds__(WalkShape<MAC, SHAPE>::warps * 32,
-                                  WalkShape<MAC, SHAPE>::min_blocks)
+template <bool QUAD, bool SHELL, bool POT, bool GUARD, int MAC, int SHAPE = 0, int GS = 32>
+__global__ void __launch_bounds__(WalkShape<MAC, SHAPE, GS>::warps * 32,
+                                  WalkShape<MAC, SHAPE, GS>::min_blocks)
 k_walk_group(WalkArgs a) {
-    constexpr int WARPS = WalkShape<MAC, SHAPE>::warps;
+    constexpr int WARPS = WalkShape<MAC, SHAPE, GS>::warps;
     extern __shared__ __align__(16) float s_walk[];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -132,25 +156,35 @@ k_walk_group(WalkArgs a) {
         if (lane == 0) g = (int)atomicAdd(a.group_ctr, 1u);
         g = __shfl_sync(FULL, g, 0);
         if (g >= ngroups) break;
-        const int2 grp = a.groups[g];  // body_first, body_count (<= 32)
+        const int2 grp = a.groups[g];  // body_first, body_count (<= 64)
         const int nvalid = grp.y;
+        // A group of 33..64 bodies gives every lane two: body `lane` (A) and
+        // body `32 + lane` (B, when present); the warp walks once for both and
+        // evaluates each interaction list for A and then for B.
+        const bool two = GS == 64 && nvalid > 32;
         // A group of nvalid <= 16 bodies is replicated over the warp: lane
         // (rep, slot) holds body `slot` and evaluates every nrep-th list entry
         // starting at `rep`; the replicas' sums are combined at the end.
-        const int lw = (nvalid <= 1) ? 0 : 32 - __clz(nvalid - 1);  // log2(width)
+        const int lw = (nvalid <= 1) ? 0 : two ? 5 : 32 - __clz(nvalid - 1);  // log2(width)
         const int slot = lane & ((1 << lw) - 1);
         const int rep = lane >> lw, nrep = 32 >> lw;
         const int s = grp.x + slot;
         const bool valid = slot < nvalid;
+        const int s2 = s + 32;
+        const bool valid2 = two && 32 + lane < nvalid;
         const double4 b = a.sbody[valid ? s : grp.x];
-        const double mnx = warp_min(b.x), mny = warp_min(b.y), mnz = warp_min(b.z);
-        const double mxx = warp_max(b.x), mxy = warp_max(b.y), mxz = warp_max(b.z);
+        const double4 b2 = valid2 ? a.sbody[s2] : b;
+        const double mnx = warp_min(fmin(b.x, b2.x)), mny = warp_min(fmin(b.y, b2.y));
+        const double mnz = warp_min(fmin(b.z, b2.z));
+        const double mxx = warp_max(fmax(b.x, b2.x)), mxy = warp_max(fmax(b.y, b2.y));
+        const double mxz = warp_max(fmax(b.z, b2.z));
         const double gcx = 0.5 * (mnx + mxx), gcy = 0.5 * (mny + mxy), gcz = 0.5 * (mnz + mxz);
         // half extents, rounded outwards so the FP32 box contains every body
         const float ghx = (float)(0.5 * (mxx - mnx)) * 1.000001f + 1e-30f;
         const float ghy = (float)(0.5 * (mxy - mny)) * 1.000001f + 1e-30f;
         const float ghz = (float)(0.5 * (mxz - mnz)) * 1.000001f + 1e-30f;
         const float bx = (float)(b.x - gcx), by = (float)(b.y - gcy), bz = (float)(b.z - gcz);
+        const float bx2 = (float)(b2.x - gcx), by2 = (float)(b2.y - gcy), bz2 = (float)(b2.z - gcz);
         // smallest / largest |a| of the group's bodies (previous step), and
         // whether this group's candidates are recorded (harvest)
         float a_min = 0.f, a_max = 0.f, r_grp = 0.f;
@@ -158,8 +192,9 @@ k_walk_group(WalkArgs a) {
         bool sampled = false;
         if (MAC != kMacGeometric) {
             const float am = a.samag[valid ? s : grp.x];
-            a_min = am;
-            a_max = am;
+            const float am2 = valid2 ? a.samag[s2] : am;
+            a_min = fminf(am, am2);
+            a_max = fmaxf(am, am2);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 a_min = fminf(a_min, __shfl_xor_sync(FULL, a_min, o));
@@ -193,18 +228,17 @@ k_walk_group(WalkArgs a) {
 
         float sax = 0.f, say = 0.f, saz = 0.f, cax = 0.f, cay = 0.f, caz = 0.f;
         float spot = 0.f, cpot = 0.f;
+        // body B's accumulators (groups of more than 32 bodies)
+        float sbx = 0.f, sby = 0.f, sbz = 0.f, cbx = 0.f, cby = 0.f, cbz = 0.f;
+        float spot2 = 0.f, cpot2 = 0.f;
         int nc = 0, np = 0;
         unsigned long long grp_entries = 0;  // list entries of this group (load-balance record)
 
-        auto flush_cells = [&]() {
-            float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
+        // The cell list's terms on the body at (bx, by, bz) (group-centred).
+        auto eval_cells = [&](float bx, float by, float bz, float& tx, float& ty, float& tz,
+                              float& tp) {
+            tx = ty = tz = tp = 0.f;
             if constexpr (!POT) {
-                // an odd count is padded with a massless, quadrupole-free entry
-                // far away, whose terms are exactly zero
-                if (nc & 1) {
-                    if (lane < 10) cbuf[(nc >> 1) * 20 + lane * 2 + 1] = lane < 3 ? 1e15f : 0.f;
-                    __syncwarp();
-                }
                 const int npair = (nc + 1) >> 1;
                 const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
                 const f32x2 E2 = pk2(eps2, eps2), M25 = pk2(-2.5f, -2.5f);
@@ -284,22 +318,39 @@ k_walk_group(WalkArgs a) {
                     }
                 }
             }
+        };
+        auto flush_cells = [&]() {
+            if constexpr (!POT) {
+                // an odd count is padded with a massless, quadrupole-free entry
+                // far away, whose terms are exactly zero
+                if (nc & 1) {
+                    if (lane < 10) cbuf[(nc >> 1) * 20 + lane * 2 + 1] = lane < 3 ? 1e15f : 0.f;
+                    __syncwarp();
+                }
+            }
+            float tx, ty, tz, tp;
+            eval_cells(bx, by, bz, tx, ty, tz, tp);
             kahan(sax, cax, tx);
             kahan(say, cay, ty);
             kahan(saz, caz, tz);
             if (POT) kahan(spot, cpot, tp);
+            if (two) {
+                eval_cells(bx2, by2, bz2, tx, ty, tz, tp);
+                kahan(sbx, cbx, tx);
+                kahan(sby, cby, ty);
+                kahan(sbz, cbz, tz);
+                if (POT) kahan(spot2, cpot2, tp);
+            }
             cnt_cell += (unsigned long long)nc * nvalid;
             grp_entries += nc;
             nc = 0;
             __syncwarp();
         };
-        auto flush_parts = [&]() {
-            float tx = 0.f, ty = 0.f, tz = 0.f, tp = 0.f;
+        // The body list's terms on body `self` at (bx, by, bz).
+        auto eval_parts = [&](float bx, float by, float bz, int self, float& tx, float& ty,
+                              float& tz, float& tp) {
+            tx = ty = tz = tp = 0.f;
             if constexpr (!SHELL && !POT) {
-                if (np & 1) {  // pad: a massless body far away
-                    if (lane < 4) pbuf[(np >> 1) * 8 + lane * 2 + 1] = lane < 3 ? 1e15f : 0.f;
-                    __syncwarp();
-                }
                 const int npair = (np + 1) >> 1;
                 const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
                 const f32x2 E2 = pk2(eps2, eps2);
@@ -348,14 +399,31 @@ k_walk_group(WalkArgs a) {
                     ty = fmaf(-f, dy, ty);
                     tz = fmaf(-f, dz, tz);
                     if (POT) {
-                        if (p2[j] != s) tp = fmaf(-pm, inv, tp);
+                        if (p2[j] != self) tp = fmaf(-pm, inv, tp);
                     }
                 }
             }
+        };
+        auto flush_parts = [&]() {
+            if constexpr (!SHELL && !POT) {
+                if (np & 1) {  // pad: a massless body far away
+                    if (lane < 4) pbuf[(np >> 1) * 8 + lane * 2 + 1] = lane < 3 ? 1e15f : 0.f;
+                    __syncwarp();
+                }
+            }
+            float tx, ty, tz, tp;
+            eval_parts(bx, by, bz, s, tx, ty, tz, tp);
             kahan(sax, cax, tx);
             kahan(say, cay, ty);
             kahan(saz, caz, tz);
             if (POT) kahan(spot, cpot, tp);
+            if (two) {
+                eval_parts(bx2, by2, bz2, s2, tx, ty, tz, tp);
+                kahan(sbx, cbx, tx);
+                kahan(sby, cby, ty);
+                kahan(sbz, cbz, tz);
+                if (POT) kahan(spot2, cpot2, tp);
+            }
             cnt_body += (unsigned long long)np * nvalid;
             grp_entries += np;
             np = 0;
@@ -640,6 +708,13 @@ k_walk_group(WalkArgs a) {
             a.az[row] = fz;
             if (POT) a.pot[row] = fp;
         }
+        if (valid2) {
+            const uint32_t row = a.sidx[s2];
+            a.ax[row] = (double)sbx - (double)cbx;
+            a.ay[row] = (double)sby - (double)cby;
+            a.az[row] = (double)sbz - (double)cbz;
+            if (POT) a.pot[row] = (double)spot2 - (double)cpot2;
+        }
     }
     if (lane == 0 && a.counters) {
         atomicAdd(&a.counters[0], cnt_cell);
@@ -836,14 +911,13 @@ __global__ void k_find_groups(TreeBufs t, int2* __restrict__ groups, int* __rest
 
 // Span grouping: the walk-tree nodes holding at most `span` bodies whose
 // parent holds more ("span cells"; the root when it holds at most span, and
-// leaf buckets of coincident keys that hold more) are cut into runs of 32
-// consecutive sorted bodies, the last run taking the rest.  Every warp lane
-// then holds a body (a full group, or a short tail group that the walk
-// replicates over the warp), while a group's box stays inside its span
-// cell, which holds at most `span` bodies: a group can never enclose a dense
-// region it does not belong to.
+// leaf buckets of coincident keys that hold more) are cut into runs of `size`
+// (32 or 64) consecutive sorted bodies, the last run taking the rest.  Every
+// warp lane then holds a body (or two), while a group's box stays inside its
+// span cell, which holds at most `span` bodies: a group can never enclose a
+// dense region it does not belong to.
 __global__ void k_find_groups_span(TreeBufs t, int2* __restrict__ groups,
-                                   int* __restrict__ n_groups, int span) {
+                                   int* __restrict__ n_groups, int span, int size) {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= *t.n_nodes) return;
     const int4 lk = t.link[w];
@@ -853,16 +927,17 @@ __global__ void k_find_groups_span(TreeBufs t, int2* __restrict__ groups,
         const int pw = t.walk_index[pb];
         if (t.link[pw].w <= span) return;  // inside a span cell: its ancestor cuts it
     }
-    for (int off = 0; off < lk.w; off += 32)
-        groups[atomicAdd(n_groups, 1)] = make_int2(lk.z + off, min(32, lk.w - off));
+    for (int off = 0; off < lk.w; off += size)
+        groups[atomicAdd(n_groups, 1)] = make_int2(lk.z + off, min(size, lk.w - off));
 }
 
 void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n, int2* groups,
-                 int* n_groups, double pack, int span) {
+                 int* n_groups, double pack, int span, int size) {
     cudaMemsetAsync(n_groups, 0, sizeof(int), st);
     if (n <= 0) return;
     if (span >= 32)
-        k_find_groups_span<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, groups, n_groups, span);
+        k_find_groups_span<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, groups, n_groups, span,
+                                                                 size == 64 ? 64 : 32);
     else
         k_find_groups<<<ceil_div(2 * n, 256), 256, 0, st>>>(t, groups, n_groups, pack);
 }
@@ -926,6 +1001,27 @@ void walk_init(int sms, WalkConfig& cfg) {
     cfg.blocks_small = sms * per_sm_small;
     if (cfg.blocks_small * kWalkWarpsSmall > cfg.blocks * kWalkWarps)
         cfg.blocks_small = cfg.blocks * kWalkWarps / kWalkWarpsSmall;
+    // the 64-body-group variants
+    const void* g64[4] = {(const void*)k_walk_group<true, false, false, false, kMacGeometric, 0, 64>,
+                          (const void*)k_walk_group<true, false, false, true, kMacGeometric, 0, 64>,
+                          (const void*)k_walk_group<true, false, false, false, kMacHarvest, 0, 64>,
+                          (const void*)k_walk_group<true, false, false, false, kMacLearned, 0, 64>};
+    for (int k = 0; k < 4; k++)
+        cudaFuncSetAttribute(g64[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             k == 3 ? kWalkSmemMac64 : kWalkSmem64);
+    int per_sm64 = 0, per_sm_mac64 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm64, k_walk_group<true, false, false, false, kMacGeometric, 0, 64>,
+        NB_WALK64_WARPS * 32, kWalkSmem64);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm_mac64, k_walk_group<true, false, false, false, kMacLearned, 0, 64>,
+        kMacWarps64 * 32, kWalkSmemMac64);
+    cfg.blocks64 = sms * std::max(per_sm64, 1);
+    if (cfg.blocks64 * NB_WALK64_WARPS > cfg.blocks * kWalkWarps)
+        cfg.blocks64 = cfg.blocks * kWalkWarps / NB_WALK64_WARPS;
+    cfg.blocks_mac64 = sms * std::max(per_sm_mac64, 1);
+    if (cfg.blocks_mac64 * kMacWarps64 > cfg.blocks * kWalkWarps)
+        cfg.blocks_mac64 = cfg.blocks * kWalkWarps / kMacWarps64;
     cfg.front_cap = 16384;
 }
 
@@ -937,8 +1033,28 @@ void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, b
                 bool pot, int mac, int shape) {
     if (a.n <= 0) return;
     a.front_cap = cfg.front_cap;
-    find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack, a.group_span);
+    // groups of up to 64 bodies: span groups of span >= 64, for the
+    // quadrupole walks without the shell theorem or potentials
+    const bool g64 = a.group_size == 64 && a.group_span >= 64 && quad && !shell && !pot &&
+                     (mac != kMacGeometric || shape == 0);
+    find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack, a.group_span,
+                g64 ? 64 : 32);
     cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
+    if (g64) {
+        if (mac == kMacHarvest)
+            k_walk_group<true, false, false, false, kMacHarvest, 0, 64>
+                <<<cfg.blocks64, NB_WALK64_WARPS * 32, kWalkSmem64, st>>>(a);
+        else if (mac == kMacLearned)
+            k_walk_group<true, false, false, false, kMacLearned, 0, 64>
+                <<<cfg.blocks_mac64, kMacWarps64 * 32, kWalkSmemMac64, st>>>(a);
+        else if (a.eps2 > 0.0)
+            k_walk_group<true, false, false, false, kMacGeometric, 0, 64>
+                <<<cfg.blocks64, NB_WALK64_WARPS * 32, kWalkSmem64, st>>>(a);
+        else
+            k_walk_group<true, false, false, true, kMacGeometric, 0, 64>
+                <<<cfg.blocks64, NB_WALK64_WARPS * 32, kWalkSmem64, st>>>(a);
+        return;
+    }
     if (mac == kMacHarvest) {
         k_walk_group<true, false, false, false, kMacHarvest>
             <<<cfg.blocks, kWalkThreads, kWalkSmem, st>>>(a);

@@ -20,11 +20,12 @@ struct WalkArgs {
     double* pot;                // potential by body row (may be null)
     int* front;                 // per-warp node stacks, front_cap ints each
     int front_cap;
-    int2* groups;               // walk groups: body_first, body_count (<= 32)
+    int2* groups;               // walk groups: body_first, body_count (<= group_size)
     int* n_groups;
     double pack;                // sibling packing box-growth limit (0: no packing)
-    int group_span;             // >= 32: runs of 32 bodies inside cells of <= group_span
-                                // bodies (find_groups); otherwise sibling packing
+    int group_span;             // >= 32: runs of group_size bodies inside cells of <=
+                                // group_span bodies (find_groups); otherwise sibling packing
+    int group_size;             // 32, or 64 with span groups: a lane holds two bodies
     // learned MAC / harvest
     const float* samag;         // |a| of each sorted body from the previous step
     const MacDev* mac;          // network image (learned mode)
@@ -47,6 +48,8 @@ struct WalkConfig {
     int blocks;        // persistent grid size
     int blocks_mac;    // persistent grid size of the learned-MAC walk
     int blocks_small;  // persistent grid size of the small-block geometric walk (shape 1)
+    int blocks64;      // persistent grid sizes of the 64-body-group walks
+    int blocks_mac64;
     int front_cap;
 };
 
@@ -59,7 +62,7 @@ void walk_init(int sms, WalkConfig& cfg);
 // times the larger part's (0: no packing), plus 32-body slices of level-21
 // buckets that hold more than 32.
 void find_groups(cudaStream_t st, const TreeBufs& t, const double4* sbody, int n, int2* groups,
-                 int* n_groups, double pack, int span);
+                 int* n_groups, double pack, int span, int size = 32);
 size_t walk_front_bytes(const WalkConfig& cfg);
 // Group walk, FP32 monopole(+quadrupole) on FP64-differenced coordinates.
 // mac: 0 geometric, 1 harvest, 2 learned (1 and 2 need quad, no shell, no
