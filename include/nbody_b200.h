@@ -107,7 +107,9 @@ enum nb_param {
     NB_PARAM_DENSITY_MERGE = 6,    /* i32, 1 = density-preserving merge radius (default 1)     */
     NB_PARAM_TIMING = 7,           /* i32, 1 = record per-stage CUDA events (default 1)        */
     NB_PARAM_MAC_BUDGET = 8,       /* f64, learned MAC: max predicted log10 rel. error         */
-    NB_PARAM_GROUP_BODIES = 9,     /* i32, bodies per walk group (32)                          */
+    NB_PARAM_GROUP_BODIES = 9,     /* i32, bodies per walk group with span groups: 64 (default;
+                                      each warp lane holds two bodies) or 32; the shell-theorem,
+                                      potential and small-block walks use 32                  */
     NB_PARAM_GROUP_PACK = 10,      /* f64, pack sibling cells into one walk group while the
                                       packed box is at most this many times the larger part's
                                       box; 0 = no packing (default 2.25)                       */

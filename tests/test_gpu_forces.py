@@ -198,6 +198,32 @@ def test_bh_group_walk_error_budget(engine, oracle, n):
     assert c[N.C_CELL_INTERACTIONS] > 0 and c[N.C_BODY_INTERACTIONS] > 0
 
 
+@pytest.mark.parametrize("n", [50_001, 200_000])
+def test_bh_group_sizes_32_and_64(engine, oracle, n):
+    """Walk groups of up to 32 bodies (one per lane) and of up to 64 (two per
+    lane, the default): both within the theta = 0.5 error budget, each run to
+    run bit-identical, and the larger group (a looser group box) never less
+    accurate by more than a few percent."""
+    b = scenarios.plummer(n, seed=6)
+    t = np.arange(0, n, max(1, n // 2048))
+    want = oracle.direct_forces_targets(b.px, b.py, b.pz, b.mass, b.active, 1e-4, t)
+    errs = {}
+    try:
+        for gb in (32, 64):
+            engine.set_param(N.PARAM_GROUP_BODIES, gb)
+            got = _forces(engine, b, 1e-4, MODE_BARNES_HUT, theta=0.5)
+            again = _forces(engine, b, 1e-4, MODE_BARNES_HUT, theta=0.5)
+            for x, y in zip(got, again):
+                np.testing.assert_array_equal(x, y)
+            errs[gb] = np.sqrt(np.mean(rel_err([g[t] for g in got], want) ** 2))
+            assert errs[gb] < 1e-3, (gb, errs[gb])
+            groups = engine.counters()[N.C_GROUPS]
+            assert groups >= -(-n // gb)
+    finally:
+        engine.set_param(N.PARAM_GROUP_BODIES, 64)
+    assert errs[64] < errs[32] * 1.05
+
+
 def test_bh_group_walk_theta_monotone(engine, oracle):
     b = scenarios.plummer(30_000, seed=2)
     t = np.arange(0, 30_000, 29)
