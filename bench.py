@@ -348,11 +348,17 @@ def train_learned_mac(eng, N, scenarios, log):
         frac = min(1.0, per / (60.0 * n))
         rows.append(eng.mac_harvest(per * 2, frac, seed, EPS))
     harvest_s = time.perf_counter() - t0
+    t1 = time.perf_counter()
     losses = eng.mac_train(6, 4096, 2e-3, seed=3)
+    train_s = time.perf_counter() - t1
     log(f"learned MAC: {sum(rows)} rows in {harvest_s:.1f} s, losses {np.round(losses, 4)}")
     return {"rows": int(sum(rows)), "systems": len(rows), "epochs": 6, "batch": 4096, "lr": 2e-3,
             "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
-            "harvest_s": harvest_s, "total_s": time.perf_counter() - t0,
+            "harvest_s": harvest_s, "train_s": train_s,
+            # tcgen05 gradient + Adam + weight image per 4096-row batch, host
+            # shuffle per epoch included
+            "train_rows_per_s": 6 * int(sum(rows)) / train_s,
+            "total_s": time.perf_counter() - t0,
             "screen_margin": float(eng.mac_get_screen()[-1])}
 
 
