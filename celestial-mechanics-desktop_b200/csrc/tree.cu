@@ -41,6 +41,7 @@ size_t tree_bytes(int cap) {
     b += 256;                                                          // align slack
     size_t w = 2 * c;
     b += w * 16 + w * 4 + w * 4 + w * 32 + w * 16 + w * 16 + w * 4 + 16;
+    b += w * 4 + 16;                                                   // parent walk index
     b += 2 * w * 16;                                                   // body boxes
     b += c * 4 + 16;                                                   // leaf list
     return b + 16 * 64;
@@ -65,6 +66,7 @@ void tree_carve(TreeBufs& t, void* base, int cap) {
     t.bhi = carve<float4>(p, w);
     t.level = carve<int>(p, w);
     t.parent_bin = carve<int>(p, w);
+    t.parent_walk = carve<int>(p, w);
     t.counter = carve<int>(p, w);
     t.n_nodes = carve<int>(p, 4);
     t.leaves = carve<int>(p, c);
@@ -316,14 +318,23 @@ struct Moments {
 // sys_half16: batched systems (keys carry the system in their top bits): the
 // half-size of each system's cube times 2^4, the half-size its level-0 cell
 // would have; null for one system in `cube`.
+__device__ __forceinline__ int atomic_add_acq_rel(int* p, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;"
+                 : "=r"(old)
+                 : "l"(p), "r"(v)
+                 : "memory");
+    return old;
+}
+
 // Multipoles in two kernels.  k_multipole_leaves: every leaf reduces its
 // bodies in one pass (a persistent grid-stride loop, nothing waits) and enters
 // the leaf list.  k_multipole_climb: one thread per leaf, all resident at
 // once, climbs; the last child to arrive at a parent reduces it from its
 // children in child order, so the result does not depend on which thread
-// arrives last (deterministic).  Per level a climb makes three dependent L2
-// trips: the parent's walk index; its link / level / parent words together
-// with the arrival atomic; every child word in one loop.  (Computing the
+// arrives last (deterministic).  Per level a climb makes two dependent L2
+// trips: the parent's link / level / parent words together with the
+// acquire-release arrival atomic, then every child word in one loop.  (Computing the
 // leaves inside the climbing threads left the last blocks' leaves waiting for
 // resident blocks to drain, so the root finished a whole wave of climbs late.)
 __global__ void __launch_bounds__(256)
@@ -334,6 +345,9 @@ k_multipole_leaves(TreeBufs t, const double4* __restrict__ sbody,
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nn; w += gridDim.x * blockDim.x) {
         const int4 lk = __ldg(&t.link[w]);
         const bool leaf = lk.y == 0;
+        // every node's parent as a walk index, for the climb and the groups
+        const int pbin = __ldg(&t.parent_bin[w]);
+        t.parent_walk[w] = pbin >= 0 ? __ldg(&t.walk_index[pbin]) : -1;
         const unsigned am = __activemask();
         const unsigned lm = __ballot_sync(am, leaf);
         int slot = 0;
@@ -384,15 +398,14 @@ k_multipole_climb(TreeBufs t, const double* __restrict__ cube,
                   const uint64_t* __restrict__ skeys, const double* __restrict__ sys_half16) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= *t.n_leaves) return;
-    int pb = __ldg(&t.parent_bin[t.leaves[i]]);
-    for (int guard = 0; pb >= 0 && guard < 64; guard++) {  // <= 22 levels up
-        const int p = __ldg(&t.walk_index[pb]);
+    int p = __ldg(&t.parent_walk[t.leaves[i]]);
+    for (int guard = 0; p >= 0 && guard < 64; guard++) {  // <= 22 levels up
         const int4 pl = __ldg(&t.link[p]);
         const int plev = __ldg(&t.level[p]);
-        const int ppb = __ldg(&t.parent_bin[p]);
-        __threadfence();  // this thread's node words are visible before its arrival counts
-        if (atomicAdd(&t.counter[p], 1) != pl.y - 1) return;
-        __threadfence();
+        const int pp = __ldg(&t.parent_walk[p]);
+        // arrival: release orders this thread's node words before it, acquire
+        // orders the children's words (released by their own arrivals) after
+        if (atomic_add_acq_rel(&t.counter[p], 1) != pl.y - 1) return;
         const double root_half = sys_half16 ? sys_half16[skeys[pl.z] >> kEnsSysShift] : cube[3];
         const double2 r0a = __ldcg((const double2*)&t.com[pl.x]);
         const double r0z = __ldcg((const double*)&t.com[pl.x] + 2);
@@ -422,7 +435,7 @@ k_multipole_climb(TreeBufs t, const double* __restrict__ cube,
         t.com[p] = com;
         t.q0[p] = q0;
         t.q1[p] = make_float4(qyz, (float)ldexp(root_half, -plev), rmax, 0.f);
-        pb = ppb;
+        p = pp;
     }
 }
 

@@ -22,6 +22,7 @@ struct TreeBufs {
     int4* link;         // first_child (-1 leaf), n_child, body_first, body_count
     int* level;         // octree level of the node's (deepest) cell
     int* parent_bin;    // binary id of the parent octree node (-1 root)
+    int* parent_walk;   // walk index of the parent node (-1 root; set by the multipole pass)
     double4* com;       // centre of mass (FP64) and mass
     float4* q0;         // Qxx, Qyy, Qxy, Qxz (traceless, about the COM)
     float4* q1;         // Qyz, cell half-size, max body radius, 0

@@ -922,11 +922,8 @@ __global__ void k_find_groups_span(TreeBufs t, int2* __restrict__ groups,
     if (w >= *t.n_nodes) return;
     const int4 lk = t.link[w];
     if (lk.w > span && lk.y != 0) return;  // an internal node above the span cells
-    const int pb = t.parent_bin[w];
-    if (pb >= 0) {
-        const int pw = t.walk_index[pb];
-        if (t.link[pw].w <= span) return;  // inside a span cell: its ancestor cuts it
-    }
+    const int pw = t.parent_walk[w];
+    if (pw >= 0 && t.link[pw].w <= span) return;  // inside a span cell: its ancestor cuts it
     for (int off = 0; off < lk.w; off += size)
         groups[atomicAdd(n_groups, 1)] = make_int2(lk.z + off, min(size, lk.w - off));
 }
