@@ -713,7 +713,9 @@ def run_theta05(args, ws, rank, local):
                              "frac": achieved / fp32_peak, "flop_per_pair": FLOPS_BODY,
                              "traffic": (walk_traffic_per_launch()
                                          if n == N_BODIES and not direct else None)},
-                "gpu_launches": (15 if direct else launches_per_step()) * args.steps,
+                # direct: kick-drift, cube, keys, 8 passes, gather, zero-acc,
+                # the direct sum, its chunk reduction, kick
+                "gpu_launches": (16 if direct else launches_per_step()) * args.steps,
                 "clocks": arm["clocks"]}
         if direct and ws == 1 and not args.no_cpu_baseline:
             # the CpuParallelBackend restatement (FP64, OpenMP over targets) on
@@ -956,10 +958,12 @@ def run_compact(args, ws, rank, local):
 
 
 def launches_per_step() -> int:
-    """Kernels of one device step: kick-drift-bbox, cube, keys, 8 sort passes,
-    gather, zero-acc, radix tree, octree mark, block scan, octree base,
-    octree emit, multipoles, walk groups, walk, kick."""
-    return 1 + 1 + 1 + 8 + 1 + 1 + 6 + 1 + 1 + 1
+    """Kernels of one geometric device step: kick-drift-bbox, cube, keys, 8
+    sort passes, gather, zero-acc, radix tree, octree mark, block scan,
+    octree base, octree emit, multipole leaves (which also cut the walk
+    groups), multipole climb, walk, kick (the learned MAC adds its per-node
+    screen terms)."""
+    return 1 + 1 + 1 + 8 + 1 + 1 + 5 + 2 + 1 + 1
 
 
 def _timed_steps(eng, stream, steps, dt, eps, flags, dev, ws):
