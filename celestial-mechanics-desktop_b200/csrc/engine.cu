@@ -300,14 +300,8 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
                         &sc->group_ctr, h->sms);
     } else if (mode == NB_MODE_BARNES_HUT || mode == NB_MODE_BARNES_HUT_REF) {
         const bool ref = mode == NB_MODE_BARNES_HUT_REF;
-        // span groups are cut by the tree build's leaf pass (no separate launch)
-        const bool quad = learned || (flags & NB_FLAG_NO_QUADRUPOLE) == 0;
-        const bool span_groups = !ref && h->group_span >= 32;
-        const nb::SpanGroups sg{h->groups, &sc->n_groups, h->group_span,
-                                nb::walk_group_bodies(h->group_bodies, h->group_span, quad, shell,
-                                                      false, learned ? 2 : 0, 0)};
         nb::tree_build(h->st, h->tree, na, h->keys0, h->sbody, radii ? h->srad : nullptr, sc->cube,
-                       ref ? 1 : h->leaf_cap, sc->err, nullptr, span_groups ? &sg : nullptr);
+                       ref ? 1 : h->leaf_cap, sc->err);
         h->ev_tree = true;
         h->tree_current = radii;
         record(h, 2);
@@ -330,7 +324,6 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
         a.pack = h->group_pack;
         a.group_span = h->group_span;
         a.group_size = h->group_bodies;
-        a.groups_ready = span_groups;
         a.counters = sc->counters;
         a.err = sc->err;
         if (ref) {

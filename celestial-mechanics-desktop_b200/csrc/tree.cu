@@ -340,21 +340,14 @@ __device__ __forceinline__ int atomic_add_acq_rel(int* p, int v) {
 __global__ void __launch_bounds__(256)
 k_multipole_leaves(TreeBufs t, const double4* __restrict__ sbody,
                    const float* __restrict__ srad, const double* __restrict__ cube,
-                   const uint64_t* __restrict__ skeys, const double* __restrict__ sys_half16,
-                   SpanGroups sg) {
+                   const uint64_t* __restrict__ skeys, const double* __restrict__ sys_half16) {
     const int nn = *t.n_nodes;
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nn; w += gridDim.x * blockDim.x) {
         const int4 lk = __ldg(&t.link[w]);
         const bool leaf = lk.y == 0;
         // every node's parent as a walk index, for the climb and the groups
         const int pbin = __ldg(&t.parent_bin[w]);
-        const int pw = pbin >= 0 ? __ldg(&t.walk_index[pbin]) : -1;
-        t.parent_walk[w] = pw;
-        // span groups: a node holding at most `span` bodies (or a leaf bucket
-        // that holds more) whose parent holds more is cut into runs
-        if (sg.groups && (lk.w <= sg.span || leaf) && (pw < 0 || __ldg(&t.link[pw]).w > sg.span))
-            for (int off = 0; off < lk.w; off += sg.size)
-                sg.groups[atomicAdd(sg.n_groups, 1)] = make_int2(lk.z + off, min(sg.size, lk.w - off));
+        t.parent_walk[w] = pbin >= 0 ? __ldg(&t.walk_index[pbin]) : -1;
         const unsigned am = __activemask();
         const unsigned lm = __ballot_sync(am, leaf);
         int slot = 0;
@@ -461,9 +454,8 @@ static int leaves_grid() {
 
 void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys,
                 const double4* sbody, const float* srad, const double* cube, int leaf_cap,
-                int* err, const double* sys_half16, const SpanGroups* sg) {
+                int* err, const double* sys_half16) {
     (void)err;
-    if (sg) cudaMemsetAsync(sg->n_groups, 0, sizeof(int), st);
     if (n <= 0) {
         cudaMemsetAsync(t.n_nodes, 0, sizeof(int), st);
         return;
@@ -480,7 +472,7 @@ void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys
     cudaMemsetAsync(t.counter, 0, sizeof(int) * 2 * (size_t)n, st);
     cudaMemsetAsync(t.n_leaves, 0, sizeof(int), st);
     k_multipole_leaves<<<std::min(ceil_div(2 * n, 256), leaves_grid()), 256, 0, st>>>(
-        t, sbody, srad, cube, skeys, sys_half16, sg ? *sg : SpanGroups{nullptr, nullptr, 0, 32});
+        t, sbody, srad, cube, skeys, sys_half16);
     // at most n leaves (each holds a body); the threads past the count return
     k_multipole_climb<<<ceil_div(n, kClimbThreads), kClimbThreads, 0, st>>>(t, cube, skeys,
                                                                              sys_half16);

@@ -44,18 +44,8 @@ void tree_carve(TreeBufs& t, void* base, int capacity);
 // the system index in bits 62..51 (four octree levels) and a 17-bit-per-axis
 // Morton code in that system's own cube below; sys_half16[s] = that cube's
 // half-size x 16 (cube is then unused).
-// Walk groups found during the build (span groups, see find_groups in
-// walk.cuh): runs of `size` bodies cut from the nodes holding at most `span`
-// bodies whose parent holds more.
-struct SpanGroups {
-    int2* groups;
-    int* n_groups;
-    int span;
-    int size;
-};
-
 void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys,
                 const double4* sbody, const float* srad, const double* cube, int leaf_cap,
-                int* err, const double* sys_half16 = nullptr, const SpanGroups* sg = nullptr);
+                int* err, const double* sys_half16 = nullptr);
 
 }  // namespace nb

@@ -1026,23 +1026,16 @@ size_t walk_front_bytes(const WalkConfig& cfg) {
     return (size_t)cfg.blocks * kWalkWarps * cfg.front_cap * sizeof(int);
 }
 
-int walk_group_bodies(int group_size, int span, bool quad, bool shell, bool pot, int mac,
-                      int shape) {
-    return group_size == 64 && span >= 64 && quad && !shell && !pot &&
-                   (mac != kMacGeometric || shape == 0)
-               ? 64
-               : 32;
-}
-
 void walk_group(cudaStream_t st, const WalkConfig& cfg, WalkArgs a, bool quad, bool shell,
                 bool pot, int mac, int shape) {
     if (a.n <= 0) return;
     a.front_cap = cfg.front_cap;
-    const bool g64 =
-        walk_group_bodies(a.group_size, a.group_span, quad, shell, pot, mac, shape) == 64;
-    if (!a.groups_ready)
-        find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack, a.group_span,
-                    g64 ? 64 : 32);
+    // groups of up to 64 bodies: span groups of span >= 64, for the
+    // quadrupole walks without the shell theorem or potentials
+    const bool g64 = a.group_size == 64 && a.group_span >= 64 && quad && !shell && !pot &&
+                     (mac != kMacGeometric || shape == 0);
+    find_groups(st, a.t, a.sbody, a.n, a.groups, a.n_groups, a.pack, a.group_span,
+                g64 ? 64 : 32);
     cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
     if (g64) {
         if (mac == kMacHarvest)

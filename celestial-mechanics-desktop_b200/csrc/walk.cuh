@@ -26,7 +26,6 @@ struct WalkArgs {
     int group_span;             // >= 32: runs of group_size bodies inside cells of <=
                                 // group_span bodies (find_groups); otherwise sibling packing
     int group_size;             // 32, or 64 with span groups: a lane holds two bodies
-    int groups_ready;           // the span groups were found by tree_build (SpanGroups)
     // learned MAC / harvest
     const float* samag;         // |a| of each sorted body from the previous step
     const MacDev* mac;          // network image (learned mode)
@@ -55,11 +54,6 @@ struct WalkConfig {
 };
 
 void walk_init(int sms, WalkConfig& cfg);
-// Bodies per group the walk uses for these settings: `group_size` (64) only
-// with span groups (span >= 64) and the quadrupole walks without the shell
-// theorem or potentials (and the default block shape); otherwise 32.
-int walk_group_bodies(int group_size, int span, bool quad, bool shell, bool pot, int mac,
-                      int shape);
 // Walk groups (sets of at most 32 consecutive sorted bodies), groups: >= n
 // entries.  span >= 32: every walk-tree node holding at most `span` bodies
 // whose parent holds more is cut into runs of 32 consecutive bodies.
