@@ -960,10 +960,9 @@ def run_compact(args, ws, rank, local):
 def launches_per_step() -> int:
     """Kernels of one geometric device step: kick-drift-bbox, cube, keys, 8
     sort passes, gather, zero-acc, radix tree, octree mark, block scan,
-    octree base, octree emit, multipole leaves (which also cut the walk
-    groups), multipole climb, walk, kick (the learned MAC adds its per-node
-    screen terms)."""
-    return 1 + 1 + 1 + 8 + 1 + 1 + 5 + 2 + 1 + 1
+    octree base, octree emit, multipole leaves, multipole climb, walk
+    groups, walk, kick (the learned MAC adds its per-node screen terms)."""
+    return 1 + 1 + 1 + 8 + 1 + 1 + 5 + 2 + 1 + 1 + 1
 
 
 def _timed_steps(eng, stream, steps, dt, eps, flags, dev, ws):
