@@ -880,7 +880,7 @@ def run_ensemble(args, ws, rank, local):
                          "tree": {"choice": list(__import__("nbody_b200")._native
                                                  .ENS_TREE_CHOICES[tree_choice]),
                                   "choices": "(walk block shape 0: 8 warps x 3, 1: 4 warps x 6; "
-                                             "walk-group span)",
+                                             "walk-group span; bodies per group)",
                                   "ms_per_choice": [round(float(x), 4) for x in tree_ms]}},
             "force_error": {"direct_rms_max": float(rms[small].max()),
                             "direct_rms_median": float(np.median(rms[small])),

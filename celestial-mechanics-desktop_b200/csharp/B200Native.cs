@@ -44,7 +44,7 @@ internal static unsafe class B200Native
         CPairs = 4, CMerges = 5, COverflows = 6, CGroups = 7, CMaxGroupWork = 8, CMacEvals = 9,
         CMacAudits = 10, CMacFallback = 11, CCount = 12;
 
-    public const int MacParams = 4801, MacNorm = 18, MacScreen = 10, EnsTreeChoices = 8;
+    public const int MacParams = 4801, MacNorm = 18, MacScreen = 10, EnsTreeChoices = 11;
     public const int NoAllocSortMax = 1048576;
 
     // ---- lifetime ---------------------------------------------------------

@@ -393,6 +393,7 @@ struct nb_ensemble {
     int leaf_cap = 8;
     int walk_shape = 0;                   // tree branch: walk block shape (0: 8 warps, 1: 4)
     int group_span = 0;                   // tree branch: walk-group span (0: sibling packing)
+    int group_bodies = 32;                // tree branch: bodies per walk group (64 with span >= 64)
     int shape = 4;                        // direct tile shape (128 x 2 until tuned)
     int shape_blocks[nb::kNumShapes] = {0};  // resident blocks per SM of each shape
     // device
@@ -422,7 +423,7 @@ struct nb_ensemble {
     // graph of one step
     cudaGraphExec_t graph = nullptr;
     double g_dt = 0, g_eps = -1, g_theta = -1;
-    int g_shape = -1, g_walk = -1, g_span = -1;
+    int g_shape = -1, g_walk = -1, g_span = -1, g_bodies = -1;
     // counters of the last evaluation
     long long ds_pairs = 0;
     long long bh_cell = 0, bh_body = 0;
@@ -569,6 +570,7 @@ void launch_tree(nb_ensemble* h, cudaStream_t st, double eps) {
         a.n_groups = &sc->n_groups;
         a.pack = 2.25;
         a.group_span = h->group_span;
+        a.group_size = h->group_bodies;
         a.counters = sc->counters;
         a.err = sc->err;
         a.sys_root = h->d_root;
@@ -590,9 +592,17 @@ void enqueue_forces(nb_ensemble* h, double eps) {
     cudaStreamWaitEvent(h->st, h->ev_join, 0);
 }
 
-// Walk-group spans the tree autotuner tries (0: sibling packing); choice k
-// is walk shape k / 4 with span kEnsSpans[k % 4].
+// Walk-group spans the tree autotuner tries (0: sibling packing).  Choices
+// 0..7 are walk shape k / 4 with span kEnsSpans[k % 4] and 32-body groups;
+// choices 8..10 are shape 0 with span kEnsSpans[k - 7] and 64-body groups.
 constexpr int kEnsSpans[4] = {0, 256, 512, 1024};
+struct EnsTreeChoice {
+    int shape, span, bodies;
+};
+static EnsTreeChoice ens_tree_choice(int k) {
+    if (k < 8) return {k / 4, kEnsSpans[k % 4], 32};
+    return {0, kEnsSpans[k - 7], 64};
+}
 
 // A span cell must lie inside one system: with span below the smallest tree
 // system's body count, a walk-tree node holding at most `span` bodies can
@@ -602,7 +612,7 @@ int smallest_tree_system(const nb_ensemble* h) {
     for (int k = h->nds; k < h->nsys; k++) m = std::min(m, h->off[k + 1] - h->off[k]);
     return m;
 }
-static_assert(NB_ENS_TREE_CHOICES == 8, "two walk shapes x four spans");
+static_assert(NB_ENS_TREE_CHOICES == 11, "two walk shapes x four spans, and three spans of 64-body groups");
 
 void collect(nb_ensemble* h) {
     unsigned long long c[4] = {0, 0, 0, 0};
@@ -614,7 +624,8 @@ void collect(nb_ensemble* h) {
 
 int ens_graph(nb_ensemble* h, double dt, double eps) {
     if (h->graph && h->g_dt == dt && h->g_eps == eps && h->g_theta == h->theta &&
-        h->g_shape == h->shape && h->g_walk == h->walk_shape && h->g_span == h->group_span)
+        h->g_shape == h->shape && h->g_walk == h->walk_shape && h->g_span == h->group_span &&
+        h->g_bodies == h->group_bodies)
         return NB_OK;
     if (h->graph) {
         cudaGraphExecDestroy(h->graph);
@@ -643,6 +654,7 @@ int ens_graph(nb_ensemble* h, double dt, double eps) {
     h->g_shape = h->shape;
     h->g_walk = h->walk_shape;
     h->g_span = h->group_span;
+    h->g_bodies = h->group_bodies;
     return NB_OK;
 }
 
@@ -844,6 +856,11 @@ NB_API int32_t nb_ens_set_param_i32(nb_ensemble* h, int32_t p, int32_t v) {
         h->group_span = v;
         return NB_OK;
     }
+    if (p == NB_PARAM_GROUP_BODIES) {
+        if (v != 32 && v != 64) return efail(h, NB_ERR_INVALID_ARG, "group size must be 32 or 64");
+        h->group_bodies = v;
+        return NB_OK;
+    }
     if (p == NB_PARAM_ENS_WALK_SHAPE) {
         if (v < 0 || v > 1) return efail(h, NB_ERR_INVALID_ARG, "walk shape must be 0 or 1");
         h->walk_shape = v;
@@ -984,9 +1001,11 @@ NB_API int32_t nb_ens_autotune_tree(nb_ensemble* h, double softening, int32_t* c
         const int smallest = smallest_tree_system(h);
         for (int k = 0; k < NB_ENS_TREE_CHOICES; k++) {
             if (ms_per_choice) ms_per_choice[k] = -1.0;
-            if (kEnsSpans[k % 4] >= smallest) continue;  // could cross systems
-            h->walk_shape = k / 4;
-            h->group_span = kEnsSpans[k % 4];
+            const EnsTreeChoice c = ens_tree_choice(k);
+            if (c.span >= smallest) continue;  // could cross systems
+            h->walk_shape = c.shape;
+            h->group_span = c.span;
+            h->group_bodies = c.bodies;
             launch_tree(h, h->st, softening);  // warm-up
             float t = 1e30f;
             for (int rep = 0; rep < 3; rep++) {
@@ -1008,8 +1027,10 @@ NB_API int32_t nb_ens_autotune_tree(nb_ensemble* h, double softening, int32_t* c
     } else if (ms_per_choice) {
         for (int k = 0; k < NB_ENS_TREE_CHOICES; k++) ms_per_choice[k] = -1.0;
     }
-    h->walk_shape = best / 4;
-    h->group_span = kEnsSpans[best % 4];
+    const EnsTreeChoice c = ens_tree_choice(best);
+    h->walk_shape = c.shape;
+    h->group_span = c.span;
+    h->group_bodies = c.bodies;
     if (choice) *choice = best;
     // the accelerations of the tree systems come from the chosen configuration
     if (h->n_bh > 0) {

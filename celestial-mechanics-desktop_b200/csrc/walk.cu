@@ -121,6 +121,14 @@ __global__ void __launch_bounds__(WalkShape<MAC, SHAPE, GS>::warps * 32,
                                   WalkShape<MAC, SHAPE, GS>::min_blocks)
 k_walk_group(WalkArgs a) {
     constexpr int WARPS = WalkShape<MAC, SHAPE, GS>::warps;
+    // two-body lanes evaluate each cell-list block for both bodies in one
+    // pass (one shared-memory read of the block for the two); the learned
+    // walk, at its register limit, evaluates the list once per body
+#ifdef NB_WALK_FUSE2_LEARNED
+    constexpr bool FUSE2 = true;
+#else
+    constexpr bool FUSE2 = MAC == kMacGeometric;
+#endif
     extern __shared__ __align__(16) float s_walk[];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -235,57 +243,77 @@ k_walk_group(WalkArgs a) {
         unsigned long long grp_entries = 0;  // list entries of this group (load-balance record)
 
         // The cell list's terms on the body at (bx, by, bz) (group-centred).
+        // The terms of list entries 2m, 2m+1 (the pair block at cbuf + 20m)
+        // on one body, packed two entries per instruction.
+        auto cell_pair = [&](const float* blk_f, f32x2 BX, f32x2 BY, f32x2 BZ, f32x2& TX,
+                             f32x2& TY, f32x2& TZ) {
+            const float4* blk = (const float4*)blk_f;
+            const f32x2 E2 = pk2(eps2, eps2), M25 = pk2(-2.5f, -2.5f);
+            const float4 v0 = blk[0], v1 = blk[1];
+            const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
+            const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
+            const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
+            const f32x2 nm = pk2(v1.z, v1.w);  // -mass
+            const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+            float ra, rb;
+            upk2(r2, ra, rb);
+            const f32x2 inv = pk2(rsqrt_ftz(ra), rsqrt_ftz(rb));
+            const f32x2 inv2 = mul2(inv, inv);
+            const f32x2 inv3 = mul2(inv, inv2);
+            if constexpr (QUAD) {
+                const float4 v2 = blk[2], v3 = blk[3], v4 = blk[4];
+                const f32x2 qxx = pk2(v2.x, v2.y), qyy = pk2(v2.z, v2.w);
+                const f32x2 qzz = pk2(v3.x, v3.y), qxy = pk2(v3.z, v3.w);
+                const f32x2 qxz = pk2(v4.x, v4.y), qyz = pk2(v4.z, v4.w);
+                const f32x2 qx = fma2(qxx, dx, fma2(qxy, dy, mul2(qxz, dz)));
+                const f32x2 qy = fma2(qxy, dx, fma2(qyy, dy, mul2(qyz, dz)));
+                const f32x2 qz = fma2(qxz, dx, fma2(qyz, dy, mul2(qzz, dz)));
+                const f32x2 rqr = fma2(dx, qx, fma2(dy, qy, mul2(dz, qz)));
+                const f32x2 inv5 = mul2(inv3, inv2);
+                // a = -M r / r^3 + Q r / r^5 - (5/2) (r.Q.r) r / r^7
+                const f32x2 f = fma2(mul2(M25, rqr), mul2(inv5, inv2), mul2(nm, inv3));
+                TX = fma2(f, dx, fma2(qx, inv5, TX));
+                TY = fma2(f, dy, fma2(qy, inv5, TY));
+                TZ = fma2(f, dz, fma2(qz, inv5, TZ));
+            } else {
+                const f32x2 f = mul2(nm, inv3);
+                TX = fma2(f, dx, TX);
+                TY = fma2(f, dy, TY);
+                TZ = fma2(f, dz, TZ);
+            }
+        };
+        auto fold = [](f32x2 T) {
+            float a0, a1;
+            upk2(T, a0, a1);
+            return a0 + a1;
+        };
+        // Both bodies of a two-body lane in one pass over the cell list: each
+        // pair block is read from shared memory once for the two.
+        auto eval_cells2 = [&](float& tx, float& ty, float& tz, float& ux, float& uy, float& uz) {
+            const int npair = (nc + 1) >> 1;
+            const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
+            const f32x2 CX = pk2(bx2, bx2), CY = pk2(by2, by2), CZ = pk2(bz2, bz2);
+            f32x2 TX = 0ull, TY = 0ull, TZ = 0ull, UX = 0ull, UY = 0ull, UZ = 0ull;
+            for (int m = 0; m < npair; m++) {
+                cell_pair(cbuf + m * 20, BX, BY, BZ, TX, TY, TZ);
+                cell_pair(cbuf + m * 20, CX, CY, CZ, UX, UY, UZ);
+            }
+            tx = fold(TX); ty = fold(TY); tz = fold(TZ);
+            ux = fold(UX); uy = fold(UY); uz = fold(UZ);
+        };
         auto eval_cells = [&](float bx, float by, float bz, float& tx, float& ty, float& tz,
                               float& tp) {
             tx = ty = tz = tp = 0.f;
             if constexpr (!POT) {
                 const int npair = (nc + 1) >> 1;
                 const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
-                const f32x2 E2 = pk2(eps2, eps2), M25 = pk2(-2.5f, -2.5f);
                 f32x2 TX = 0ull, TY = 0ull, TZ = 0ull;
 #pragma unroll 2
-                for (int m = rep; m < npair; m += nrep) {
-                    const float4* blk = (const float4*)(cbuf + m * 20);
-                    const float4 v0 = blk[0], v1 = blk[1];
-                    const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
-                    const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
-                    const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
-                    const f32x2 nm = pk2(v1.z, v1.w);  // -mass
-                    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
-                    float ra, rb;
-                    upk2(r2, ra, rb);
-                    const f32x2 inv = pk2(rsqrt_ftz(ra), rsqrt_ftz(rb));
-                    const f32x2 inv2 = mul2(inv, inv);
-                    const f32x2 inv3 = mul2(inv, inv2);
-                    if constexpr (QUAD) {
-                        const float4 v2 = blk[2], v3 = blk[3], v4 = blk[4];
-                        const f32x2 qxx = pk2(v2.x, v2.y), qyy = pk2(v2.z, v2.w);
-                        const f32x2 qzz = pk2(v3.x, v3.y), qxy = pk2(v3.z, v3.w);
-                        const f32x2 qxz = pk2(v4.x, v4.y), qyz = pk2(v4.z, v4.w);
-                        const f32x2 qx = fma2(qxx, dx, fma2(qxy, dy, mul2(qxz, dz)));
-                        const f32x2 qy = fma2(qxy, dx, fma2(qyy, dy, mul2(qyz, dz)));
-                        const f32x2 qz = fma2(qxz, dx, fma2(qyz, dy, mul2(qzz, dz)));
-                        const f32x2 rqr = fma2(dx, qx, fma2(dy, qy, mul2(dz, qz)));
-                        const f32x2 inv5 = mul2(inv3, inv2);
-                        // a = -M r / r^3 + Q r / r^5 - (5/2) (r.Q.r) r / r^7
-                        const f32x2 f = fma2(mul2(M25, rqr), mul2(inv5, inv2), mul2(nm, inv3));
-                        TX = fma2(f, dx, fma2(qx, inv5, TX));
-                        TY = fma2(f, dy, fma2(qy, inv5, TY));
-                        TZ = fma2(f, dz, fma2(qz, inv5, TZ));
-                    } else {
-                        const f32x2 f = mul2(nm, inv3);
-                        TX = fma2(f, dx, TX);
-                        TY = fma2(f, dy, TY);
-                        TZ = fma2(f, dz, TZ);
-                    }
-                }
-                float a0, a1;
-                upk2(TX, a0, a1);
-                tx = a0 + a1;
-                upk2(TY, a0, a1);
-                ty = a0 + a1;
-                upk2(TZ, a0, a1);
-                tz = a0 + a1;
+                for (int m = rep; m < npair; m += nrep)
+                    cell_pair(cbuf + m * 20, BX, BY, BZ, TX, TY, TZ);
+                tx = fold(TX);
+                ty = fold(TY);
+                tz = fold(TZ);
             } else {
 #pragma unroll 4
                 for (int j = rep; j < nc; j += nrep) {
@@ -329,18 +357,27 @@ k_walk_group(WalkArgs a) {
                 }
             }
             float tx, ty, tz, tp;
-            eval_cells(bx, by, bz, tx, ty, tz, tp);
+            if (!POT && FUSE2 && two) {
+                float ux, uy, uz;
+                eval_cells2(tx, ty, tz, ux, uy, uz);
+                kahan(sbx, cbx, ux);
+                kahan(sby, cby, uy);
+                kahan(sbz, cbz, uz);
+            } else {
+                eval_cells(bx, by, bz, tx, ty, tz, tp);
+                if (two) {
+                    float ux, uy, uz, up;
+                    eval_cells(bx2, by2, bz2, ux, uy, uz, up);
+                    kahan(sbx, cbx, ux);
+                    kahan(sby, cby, uy);
+                    kahan(sbz, cbz, uz);
+                    if (POT) kahan(spot2, cpot2, up);
+                }
+            }
             kahan(sax, cax, tx);
             kahan(say, cay, ty);
             kahan(saz, caz, tz);
             if (POT) kahan(spot, cpot, tp);
-            if (two) {
-                eval_cells(bx2, by2, bz2, tx, ty, tz, tp);
-                kahan(sbx, cbx, tx);
-                kahan(sby, cby, ty);
-                kahan(sbz, cbz, tz);
-                if (POT) kahan(spot2, cpot2, tp);
-            }
             cnt_cell += (unsigned long long)nc * nvalid;
             grp_entries += nc;
             nc = 0;

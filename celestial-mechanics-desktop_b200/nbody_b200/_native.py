@@ -63,7 +63,9 @@ PARAM_ADAPTIVE_DT_MAX = 20
 PARAM_GROUP_SPAN = 21
 PARAM_ENS_WALK_SHAPE = 22
 # nb_ens_autotune_tree choices: (walk block shape, walk-group span)
-ENS_TREE_CHOICES = [(w, sp) for w in (0, 1) for sp in (0, 256, 512, 1024)]
+# (walk block shape, walk-group span, bodies per group) of each tree autotune choice
+ENS_TREE_CHOICES = ([(w, sp, 32) for w in (0, 1) for sp in (0, 256, 512, 1024)] +
+                    [(0, sp, 64) for sp in (256, 512, 1024)])
 ENS_SHAPES = [(64, 1), (64, 2), (64, 4), (128, 1), (128, 2), (128, 4), (256, 1), (256, 2), (256, 4)]
 # timings / counters
 T_BUILD, T_TRAVERSAL, T_TOTAL, T_SORT, T_TREE, T_COLLIDE, T_COUNT = range(7)

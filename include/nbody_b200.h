@@ -400,7 +400,8 @@ NB_API int32_t nb_ens_destroy(nb_ensemble* h);
 NB_API const char* nb_ens_last_error(const nb_ensemble* h);
 /* systems, direct systems, tree systems, bodies, direct bodies, tree bodies */
 NB_API int32_t nb_ens_info(const nb_ensemble* h, int64_t* out, int32_t n);
-/* NB_PARAM_THETA (f64); NB_PARAM_LEAF_CAPACITY, NB_PARAM_ENS_DIRECT_SHAPE (i32) */
+/* NB_PARAM_THETA (f64); NB_PARAM_LEAF_CAPACITY, NB_PARAM_ENS_DIRECT_SHAPE,
+ * NB_PARAM_ENS_WALK_SHAPE, NB_PARAM_GROUP_SPAN, NB_PARAM_GROUP_BODIES (i32) */
 NB_API int32_t nb_ens_set_param_f64(nb_ensemble* h, int32_t param, double value);
 NB_API int32_t nb_ens_set_param_i32(nb_ensemble* h, int32_t param, int32_t value);
 /* Positions, velocities, masses; accelerations are unknown until the first
@@ -423,11 +424,15 @@ NB_API int32_t nb_ens_autotune(nb_ensemble* h, double softening, int32_t* shape,
                                double* ms_per_shape);
 /* Times the tree branch (keys, sort, tree, walk of every tree system) on the
  * current state for each walk block shape (NB_PARAM_ENS_WALK_SHAPE 0, 1) and
- * walk-group span (NB_PARAM_GROUP_SPAN 0, 256, 512, 1024), 3 runs each with
- * CUDA events, and keeps the fastest: choice k is shape k / 4 with the k % 4-th
- * span.  ms_per_choice (NB_ENS_TREE_CHOICES entries, may be NULL) gets the
- * times.  The tree systems' accelerations are then those of the choice. */
-#define NB_ENS_TREE_CHOICES 8
+ * walk-group span (NB_PARAM_GROUP_SPAN 0, 256, 512, 1024) with 32-body groups,
+ * and for shape 0 with spans 256, 512, 1024 and 64-body groups
+ * (NB_PARAM_GROUP_BODIES), 3 runs each with CUDA events, and keeps the
+ * fastest: choice k < 8 is shape k / 4 with the k % 4-th span, choice 8 + j
+ * is shape 0 with the (j + 1)-th span and 64-body groups.  Spans at or above
+ * the smallest tree system's body count are skipped (time -1).
+ * ms_per_choice (NB_ENS_TREE_CHOICES entries, may be NULL) gets the times.
+ * The tree systems' accelerations are then those of the choice. */
+#define NB_ENS_TREE_CHOICES 11
 NB_API int32_t nb_ens_autotune_tree(nb_ensemble* h, double softening, int32_t* choice,
                                     double* ms_per_choice);
 /* Per system (in `sizes` order): rms and max relative error of the current

@@ -170,8 +170,8 @@ def test_rejects_bad_input():
 
 
 def test_tree_autotune_choices_keep_systems_apart_and_accurate():
-    """nb_ens_autotune_tree times every (walk block shape, walk-group span)
-    it may use on the current state and keeps the fastest.  A span at or
+    """nb_ens_autotune_tree times every (walk block shape, walk-group span,
+    group size) it may use on the current state and keeps the fastest.  A span at or
     above the smallest tree system's size is never tried (its groups could
     take bodies of two systems) and is refused as a parameter; every tried
     configuration gives each tree system its theta = 0.5 accuracy."""
@@ -184,9 +184,10 @@ def test_tree_autotune_choices_keep_systems_apart_and_accurate():
         assert ms[choice] > 0 and ms[choice] == min(m for m in ms if m > 0)
         # every span below 2049 is tried for both block shapes
         assert np.all(ms > 0)
-        for k, (shape, span) in enumerate(N.ENS_TREE_CHOICES):
+        for k, (shape, span, bodies) in enumerate(N.ENS_TREE_CHOICES):
             ens.set_param(N.PARAM_ENS_WALK_SHAPE, shape)
             ens.set_param(N.PARAM_GROUP_SPAN, span)
+            ens.set_param(N.PARAM_GROUP_BODIES, bodies)
             ens.compute_forces(EPS)
             errs = _per_system_errors(ens, systems)
             for s, (rms, mx) in enumerate(errs):
@@ -201,4 +202,4 @@ def test_tree_autotune_choices_keep_systems_apart_and_accurate():
         choice, ms = small.autotune_tree(EPS)
         # only sibling packing (span 0) is tried, for both block shapes
         assert choice in (0, 4) and ms[0] > 0 and ms[4] > 0
-        assert all(ms[k] == -1 for k in (1, 2, 3, 5, 6, 7))
+        assert all(ms[k] == -1 for k in (1, 2, 3, 5, 6, 7, 8, 9, 10))
