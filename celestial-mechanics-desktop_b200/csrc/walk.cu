@@ -383,6 +383,41 @@ k_walk_group(WalkArgs a) {
             nc = 0;
             __syncwarp();
         };
+        // The terms of body-list entries 2m, 2m+1 (the pair block at pbuf + 8m)
+        // on one body, packed two entries per instruction.
+        auto body_pair = [&](const float* blk_f, f32x2 BX, f32x2 BY, f32x2 BZ, f32x2& TX,
+                             f32x2& TY, f32x2& TZ) {
+            const float4* blk = (const float4*)blk_f;
+            const f32x2 E2 = pk2(eps2, eps2);
+            const float4 v0 = blk[0], v1 = blk[1];
+            const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
+            const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
+            const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
+            const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+            float ra, rb;
+            upk2(r2, ra, rb);
+            const float ia = (GUARD && !(ra > 0.f)) ? 0.f : rsqrt_ftz(ra);
+            const float ib = (GUARD && !(rb > 0.f)) ? 0.f : rsqrt_ftz(rb);
+            const f32x2 inv = pk2(ia, ib);
+            // -(m / r^3); the term is -(m/r^3) (b - p), as fmaf(-f, dx, t)
+            const f32x2 f = mul2(pk2(v1.z, v1.w), mul2(mul2(inv, inv), inv));
+            TX = fma2(f, dx, TX);
+            TY = fma2(f, dy, TY);
+            TZ = fma2(f, dz, TZ);
+        };
+        auto eval_parts2 = [&](float& tx, float& ty, float& tz, float& ux, float& uy, float& uz) {
+            const int npair = (np + 1) >> 1;
+            const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
+            const f32x2 CX = pk2(bx2, bx2), CY = pk2(by2, by2), CZ = pk2(bz2, bz2);
+            f32x2 TX = 0ull, TY = 0ull, TZ = 0ull, UX = 0ull, UY = 0ull, UZ = 0ull;
+#pragma unroll 2
+            for (int m = 0; m < npair; m++) {
+                body_pair(pbuf + m * 8, BX, BY, BZ, TX, TY, TZ);
+                body_pair(pbuf + m * 8, CX, CY, CZ, UX, UY, UZ);
+            }
+            tx = fold(TX); ty = fold(TY); tz = fold(TZ);
+            ux = fold(UX); uy = fold(UY); uz = fold(UZ);
+        };
         // The body list's terms on body `self` at (bx, by, bz).
         auto eval_parts = [&](float bx, float by, float bz, int self, float& tx, float& ty,
                               float& tz, float& tp) {
@@ -390,34 +425,13 @@ k_walk_group(WalkArgs a) {
             if constexpr (!SHELL && !POT) {
                 const int npair = (np + 1) >> 1;
                 const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
-                const f32x2 E2 = pk2(eps2, eps2);
                 f32x2 TX = 0ull, TY = 0ull, TZ = 0ull;
 #pragma unroll 4
-                for (int m = rep; m < npair; m += nrep) {
-                    const float4* blk = (const float4*)(pbuf + m * 8);
-                    const float4 v0 = blk[0], v1 = blk[1];
-                    const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
-                    const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
-                    const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
-                    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
-                    float ra, rb;
-                    upk2(r2, ra, rb);
-                    const float ia = (GUARD && !(ra > 0.f)) ? 0.f : rsqrt_ftz(ra);
-                    const float ib = (GUARD && !(rb > 0.f)) ? 0.f : rsqrt_ftz(rb);
-                    const f32x2 inv = pk2(ia, ib);
-                    // -(m / r^3); the term is -(m/r^3) (b - p), as fmaf(-f, dx, t)
-                    const f32x2 f = mul2(pk2(v1.z, v1.w), mul2(mul2(inv, inv), inv));
-                    TX = fma2(f, dx, TX);
-                    TY = fma2(f, dy, TY);
-                    TZ = fma2(f, dz, TZ);
-                }
-                float a0, a1;
-                upk2(TX, a0, a1);
-                tx = a0 + a1;
-                upk2(TY, a0, a1);
-                ty = a0 + a1;
-                upk2(TZ, a0, a1);
-                tz = a0 + a1;
+                for (int m = rep; m < npair; m += nrep)
+                    body_pair(pbuf + m * 8, BX, BY, BZ, TX, TY, TZ);
+                tx = fold(TX);
+                ty = fold(TY);
+                tz = fold(TZ);
             } else {
 #pragma unroll 4
                 for (int j = rep; j < np; j += nrep) {
@@ -449,18 +463,27 @@ k_walk_group(WalkArgs a) {
                 }
             }
             float tx, ty, tz, tp;
-            eval_parts(bx, by, bz, s, tx, ty, tz, tp);
+            if (!SHELL && !POT && FUSE2 && two) {
+                float ux, uy, uz;
+                eval_parts2(tx, ty, tz, ux, uy, uz);
+                kahan(sbx, cbx, ux);
+                kahan(sby, cby, uy);
+                kahan(sbz, cbz, uz);
+            } else {
+                eval_parts(bx, by, bz, s, tx, ty, tz, tp);
+                if (two) {
+                    float ux, uy, uz, up;
+                    eval_parts(bx2, by2, bz2, s2, ux, uy, uz, up);
+                    kahan(sbx, cbx, ux);
+                    kahan(sby, cby, uy);
+                    kahan(sbz, cbz, uz);
+                    if (POT) kahan(spot2, cpot2, up);
+                }
+            }
             kahan(sax, cax, tx);
             kahan(say, cay, ty);
             kahan(saz, caz, tz);
             if (POT) kahan(spot, cpot, tp);
-            if (two) {
-                eval_parts(bx2, by2, bz2, s2, tx, ty, tz, tp);
-                kahan(sbx, cbx, tx);
-                kahan(sby, cby, ty);
-                kahan(sbz, cbz, tz);
-                if (POT) kahan(spot2, cpot2, tp);
-            }
             cnt_body += (unsigned long long)np * nvalid;
             grp_entries += np;
             np = 0;
