@@ -28,7 +28,10 @@ constexpr int kSortMinTile = kSortThreads * kSortMinItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPre = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1;
-constexpr int kLookBatch = 8;  // look-back words read per round trip
+#ifndef NB_SORT_LOOK
+#define NB_SORT_LOOK 8
+#endif
+constexpr int kLookBatch = NB_SORT_LOOK;  // look-back words read per round trip
 
 template <int ITEMS>
 const void* k_sort_pass_ptr();
