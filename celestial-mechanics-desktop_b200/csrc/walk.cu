@@ -116,6 +116,145 @@ struct WalkShape {
                  : (MAC == kMacLearned ? NB_WALK_MAC_BLOCKS : (SHAPE == 1 ? 6 : 3));
 };
 
+// ---- interaction-list evaluation ---------------------------------------------
+//
+// Lists live in shared memory pair-blocked: field f of entry e at
+// [(e / 2) * W + 2 f + e % 2] (cells W = 20: rel x, y, z, -mass, Qxx, Qyy,
+// Qzz, Qxy, Qxz, Qyz; bodies W = 8: rel x, y, z, -mass), so one 16-byte load
+// gives two fields of two entries as a register pair for the packed f32x2
+// arithmetic.  The list loops are out-of-line functions (NB_WALK_NOINLINE):
+// the learned walk reaches them from three places and inlining every copy
+// cost it instruction-cache misses.
+#ifdef NB_WALK_NOINLINE
+#define NB_WALK_EVAL __device__ __noinline__
+#else
+#define NB_WALK_EVAL __device__ __forceinline__
+#endif
+
+__device__ __forceinline__ float fold2(f32x2 T) {
+    float a0, a1;
+    upk2(T, a0, a1);
+    return a0 + a1;
+}
+
+// Terms of cell entries 2m, 2m+1 (the block at blk) on one body.
+template <bool QUAD>
+__device__ __forceinline__ void cell_pair_terms(const float* blk_f, float eps2, f32x2 BX, f32x2 BY,
+                                                f32x2 BZ, f32x2& TX, f32x2& TY, f32x2& TZ) {
+    const float4* blk = (const float4*)blk_f;
+    const f32x2 E2 = pk2(eps2, eps2), M25 = pk2(-2.5f, -2.5f);
+    const float4 v0 = blk[0], v1 = blk[1];
+    const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
+    const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
+    const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
+    const f32x2 nm = pk2(v1.z, v1.w);  // -mass
+    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+    float ra, rb;
+    upk2(r2, ra, rb);
+    const f32x2 inv = pk2(rsqrt_ftz(ra), rsqrt_ftz(rb));
+    const f32x2 inv2 = mul2(inv, inv);
+    const f32x2 inv3 = mul2(inv, inv2);
+    if constexpr (QUAD) {
+        const float4 v2 = blk[2], v3 = blk[3], v4 = blk[4];
+        const f32x2 qxx = pk2(v2.x, v2.y), qyy = pk2(v2.z, v2.w);
+        const f32x2 qzz = pk2(v3.x, v3.y), qxy = pk2(v3.z, v3.w);
+        const f32x2 qxz = pk2(v4.x, v4.y), qyz = pk2(v4.z, v4.w);
+        const f32x2 qx = fma2(qxx, dx, fma2(qxy, dy, mul2(qxz, dz)));
+        const f32x2 qy = fma2(qxy, dx, fma2(qyy, dy, mul2(qyz, dz)));
+        const f32x2 qz = fma2(qxz, dx, fma2(qyz, dy, mul2(qzz, dz)));
+        const f32x2 rqr = fma2(dx, qx, fma2(dy, qy, mul2(dz, qz)));
+        const f32x2 inv5 = mul2(inv3, inv2);
+        // a = -M r / r^3 + Q r / r^5 - (5/2) (r.Q.r) r / r^7
+        const f32x2 f = fma2(mul2(M25, rqr), mul2(inv5, inv2), mul2(nm, inv3));
+        TX = fma2(f, dx, fma2(qx, inv5, TX));
+        TY = fma2(f, dy, fma2(qy, inv5, TY));
+        TZ = fma2(f, dz, fma2(qz, inv5, TZ));
+    } else {
+        const f32x2 f = mul2(nm, inv3);
+        TX = fma2(f, dx, TX);
+        TY = fma2(f, dy, TY);
+        TZ = fma2(f, dz, TZ);
+    }
+}
+
+// Terms of body entries 2m, 2m+1 (the block at blk) on one body.  GUARD
+// (softening 0 only): 1/r is taken as 0 at r = 0.
+template <bool GUARD>
+__device__ __forceinline__ void body_pair_terms(const float* blk_f, float eps2, f32x2 BX, f32x2 BY,
+                                                f32x2 BZ, f32x2& TX, f32x2& TY, f32x2& TZ) {
+    const float4* blk = (const float4*)blk_f;
+    const f32x2 E2 = pk2(eps2, eps2);
+    const float4 v0 = blk[0], v1 = blk[1];
+    const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
+    const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
+    const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
+    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
+    float ra, rb;
+    upk2(r2, ra, rb);
+    const float ia = (GUARD && !(ra > 0.f)) ? 0.f : rsqrt_ftz(ra);
+    const float ib = (GUARD && !(rb > 0.f)) ? 0.f : rsqrt_ftz(rb);
+    const f32x2 inv = pk2(ia, ib);
+    // -(m / r^3); the term is -(m/r^3) (b - p), as fmaf(-f, dx, t)
+    const f32x2 f = mul2(pk2(v1.z, v1.w), mul2(mul2(inv, inv), inv));
+    TX = fma2(f, dx, TX);
+    TY = fma2(f, dy, TY);
+    TZ = fma2(f, dz, TZ);
+}
+
+// A cell list's terms on one body: pair blocks rep, rep + nrep, ... < npair.
+template <bool QUAD>
+NB_WALK_EVAL float3 cells_one(const float* cbuf, int npair, int rep, int nrep, float bx, float by,
+                              float bz, float eps2) {
+    const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
+    f32x2 TX = 0ull, TY = 0ull, TZ = 0ull;
+#pragma unroll 2
+    for (int m = rep; m < npair; m += nrep)
+        cell_pair_terms<QUAD>(cbuf + m * 20, eps2, BX, BY, BZ, TX, TY, TZ);
+    return make_float3(fold2(TX), fold2(TY), fold2(TZ));
+}
+
+// A cell list's terms on both bodies of a two-body lane, each pair block
+// read once for the two.
+template <bool QUAD>
+NB_WALK_EVAL void cells_two(const float* cbuf, int npair, float bx, float by, float bz, float cx,
+                            float cy, float cz, float eps2, float3& a, float3& b) {
+    const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
+    const f32x2 CX = pk2(cx, cx), CY = pk2(cy, cy), CZ = pk2(cz, cz);
+    f32x2 TX = 0ull, TY = 0ull, TZ = 0ull, UX = 0ull, UY = 0ull, UZ = 0ull;
+    for (int m = 0; m < npair; m++) {
+        cell_pair_terms<QUAD>(cbuf + m * 20, eps2, BX, BY, BZ, TX, TY, TZ);
+        cell_pair_terms<QUAD>(cbuf + m * 20, eps2, CX, CY, CZ, UX, UY, UZ);
+    }
+    a = make_float3(fold2(TX), fold2(TY), fold2(TZ));
+    b = make_float3(fold2(UX), fold2(UY), fold2(UZ));
+}
+
+template <bool GUARD>
+NB_WALK_EVAL float3 parts_one(const float* pbuf, int npair, int rep, int nrep, float bx, float by,
+                              float bz, float eps2) {
+    const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
+    f32x2 TX = 0ull, TY = 0ull, TZ = 0ull;
+#pragma unroll 4
+    for (int m = rep; m < npair; m += nrep)
+        body_pair_terms<GUARD>(pbuf + m * 8, eps2, BX, BY, BZ, TX, TY, TZ);
+    return make_float3(fold2(TX), fold2(TY), fold2(TZ));
+}
+
+template <bool GUARD>
+NB_WALK_EVAL void parts_two(const float* pbuf, int npair, float bx, float by, float bz, float cx,
+                            float cy, float cz, float eps2, float3& a, float3& b) {
+    const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
+    const f32x2 CX = pk2(cx, cx), CY = pk2(cy, cy), CZ = pk2(cz, cz);
+    f32x2 TX = 0ull, TY = 0ull, TZ = 0ull, UX = 0ull, UY = 0ull, UZ = 0ull;
+#pragma unroll 2
+    for (int m = 0; m < npair; m++) {
+        body_pair_terms<GUARD>(pbuf + m * 8, eps2, BX, BY, BZ, TX, TY, TZ);
+        body_pair_terms<GUARD>(pbuf + m * 8, eps2, CX, CY, CZ, UX, UY, UZ);
+    }
+    a = make_float3(fold2(TX), fold2(TY), fold2(TZ));
+    b = make_float3(fold2(UX), fold2(UY), fold2(UZ));
+}
+
 template <bool QUAD, bool SHELL, bool POT, bool GUARD, int MAC, int SHAPE = 0, int GS = 32>
 __global__ void __launch_bounds__(WalkShape<MAC, SHAPE, GS>::warps * 32,
                                   WalkShape<MAC, SHAPE, GS>::min_blocks)
@@ -243,77 +382,22 @@ k_walk_group(WalkArgs a) {
         unsigned long long grp_entries = 0;  // list entries of this group (load-balance record)
 
         // The cell list's terms on the body at (bx, by, bz) (group-centred).
-        // The terms of list entries 2m, 2m+1 (the pair block at cbuf + 20m)
-        // on one body, packed two entries per instruction.
-        auto cell_pair = [&](const float* blk_f, f32x2 BX, f32x2 BY, f32x2 BZ, f32x2& TX,
-                             f32x2& TY, f32x2& TZ) {
-            const float4* blk = (const float4*)blk_f;
-            const f32x2 E2 = pk2(eps2, eps2), M25 = pk2(-2.5f, -2.5f);
-            const float4 v0 = blk[0], v1 = blk[1];
-            const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
-            const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
-            const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
-            const f32x2 nm = pk2(v1.z, v1.w);  // -mass
-            const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
-            float ra, rb;
-            upk2(r2, ra, rb);
-            const f32x2 inv = pk2(rsqrt_ftz(ra), rsqrt_ftz(rb));
-            const f32x2 inv2 = mul2(inv, inv);
-            const f32x2 inv3 = mul2(inv, inv2);
-            if constexpr (QUAD) {
-                const float4 v2 = blk[2], v3 = blk[3], v4 = blk[4];
-                const f32x2 qxx = pk2(v2.x, v2.y), qyy = pk2(v2.z, v2.w);
-                const f32x2 qzz = pk2(v3.x, v3.y), qxy = pk2(v3.z, v3.w);
-                const f32x2 qxz = pk2(v4.x, v4.y), qyz = pk2(v4.z, v4.w);
-                const f32x2 qx = fma2(qxx, dx, fma2(qxy, dy, mul2(qxz, dz)));
-                const f32x2 qy = fma2(qxy, dx, fma2(qyy, dy, mul2(qyz, dz)));
-                const f32x2 qz = fma2(qxz, dx, fma2(qyz, dy, mul2(qzz, dz)));
-                const f32x2 rqr = fma2(dx, qx, fma2(dy, qy, mul2(dz, qz)));
-                const f32x2 inv5 = mul2(inv3, inv2);
-                // a = -M r / r^3 + Q r / r^5 - (5/2) (r.Q.r) r / r^7
-                const f32x2 f = fma2(mul2(M25, rqr), mul2(inv5, inv2), mul2(nm, inv3));
-                TX = fma2(f, dx, fma2(qx, inv5, TX));
-                TY = fma2(f, dy, fma2(qy, inv5, TY));
-                TZ = fma2(f, dz, fma2(qz, inv5, TZ));
-            } else {
-                const f32x2 f = mul2(nm, inv3);
-                TX = fma2(f, dx, TX);
-                TY = fma2(f, dy, TY);
-                TZ = fma2(f, dz, TZ);
-            }
-        };
-        auto fold = [](f32x2 T) {
-            float a0, a1;
-            upk2(T, a0, a1);
-            return a0 + a1;
-        };
         // Both bodies of a two-body lane in one pass over the cell list: each
         // pair block is read from shared memory once for the two.
         auto eval_cells2 = [&](float& tx, float& ty, float& tz, float& ux, float& uy, float& uz) {
-            const int npair = (nc + 1) >> 1;
-            const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
-            const f32x2 CX = pk2(bx2, bx2), CY = pk2(by2, by2), CZ = pk2(bz2, bz2);
-            f32x2 TX = 0ull, TY = 0ull, TZ = 0ull, UX = 0ull, UY = 0ull, UZ = 0ull;
-            for (int m = 0; m < npair; m++) {
-                cell_pair(cbuf + m * 20, BX, BY, BZ, TX, TY, TZ);
-                cell_pair(cbuf + m * 20, CX, CY, CZ, UX, UY, UZ);
-            }
-            tx = fold(TX); ty = fold(TY); tz = fold(TZ);
-            ux = fold(UX); uy = fold(UY); uz = fold(UZ);
+            float3 a3, b3;
+            cells_two<QUAD>(cbuf, (nc + 1) >> 1, bx, by, bz, bx2, by2, bz2, eps2, a3, b3);
+            tx = a3.x; ty = a3.y; tz = a3.z;
+            ux = b3.x; uy = b3.y; uz = b3.z;
         };
         auto eval_cells = [&](float bx, float by, float bz, float& tx, float& ty, float& tz,
                               float& tp) {
             tx = ty = tz = tp = 0.f;
             if constexpr (!POT) {
-                const int npair = (nc + 1) >> 1;
-                const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
-                f32x2 TX = 0ull, TY = 0ull, TZ = 0ull;
-#pragma unroll 2
-                for (int m = rep; m < npair; m += nrep)
-                    cell_pair(cbuf + m * 20, BX, BY, BZ, TX, TY, TZ);
-                tx = fold(TX);
-                ty = fold(TY);
-                tz = fold(TZ);
+                const float3 t3 = cells_one<QUAD>(cbuf, (nc + 1) >> 1, rep, nrep, bx, by, bz, eps2);
+                tx = t3.x;
+                ty = t3.y;
+                tz = t3.z;
             } else {
 #pragma unroll 4
                 for (int j = rep; j < nc; j += nrep) {
@@ -383,55 +467,21 @@ k_walk_group(WalkArgs a) {
             nc = 0;
             __syncwarp();
         };
-        // The terms of body-list entries 2m, 2m+1 (the pair block at pbuf + 8m)
-        // on one body, packed two entries per instruction.
-        auto body_pair = [&](const float* blk_f, f32x2 BX, f32x2 BY, f32x2 BZ, f32x2& TX,
-                             f32x2& TY, f32x2& TZ) {
-            const float4* blk = (const float4*)blk_f;
-            const f32x2 E2 = pk2(eps2, eps2);
-            const float4 v0 = blk[0], v1 = blk[1];
-            const f32x2 dx = sub2(BX, pk2(v0.x, v0.y));
-            const f32x2 dy = sub2(BY, pk2(v0.z, v0.w));
-            const f32x2 dz = sub2(BZ, pk2(v1.x, v1.y));
-            const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, E2)));
-            float ra, rb;
-            upk2(r2, ra, rb);
-            const float ia = (GUARD && !(ra > 0.f)) ? 0.f : rsqrt_ftz(ra);
-            const float ib = (GUARD && !(rb > 0.f)) ? 0.f : rsqrt_ftz(rb);
-            const f32x2 inv = pk2(ia, ib);
-            // -(m / r^3); the term is -(m/r^3) (b - p), as fmaf(-f, dx, t)
-            const f32x2 f = mul2(pk2(v1.z, v1.w), mul2(mul2(inv, inv), inv));
-            TX = fma2(f, dx, TX);
-            TY = fma2(f, dy, TY);
-            TZ = fma2(f, dz, TZ);
-        };
         auto eval_parts2 = [&](float& tx, float& ty, float& tz, float& ux, float& uy, float& uz) {
-            const int npair = (np + 1) >> 1;
-            const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
-            const f32x2 CX = pk2(bx2, bx2), CY = pk2(by2, by2), CZ = pk2(bz2, bz2);
-            f32x2 TX = 0ull, TY = 0ull, TZ = 0ull, UX = 0ull, UY = 0ull, UZ = 0ull;
-#pragma unroll 2
-            for (int m = 0; m < npair; m++) {
-                body_pair(pbuf + m * 8, BX, BY, BZ, TX, TY, TZ);
-                body_pair(pbuf + m * 8, CX, CY, CZ, UX, UY, UZ);
-            }
-            tx = fold(TX); ty = fold(TY); tz = fold(TZ);
-            ux = fold(UX); uy = fold(UY); uz = fold(UZ);
+            float3 a3, b3;
+            parts_two<GUARD>(pbuf, (np + 1) >> 1, bx, by, bz, bx2, by2, bz2, eps2, a3, b3);
+            tx = a3.x; ty = a3.y; tz = a3.z;
+            ux = b3.x; uy = b3.y; uz = b3.z;
         };
         // The body list's terms on body `self` at (bx, by, bz).
         auto eval_parts = [&](float bx, float by, float bz, int self, float& tx, float& ty,
                               float& tz, float& tp) {
             tx = ty = tz = tp = 0.f;
             if constexpr (!SHELL && !POT) {
-                const int npair = (np + 1) >> 1;
-                const f32x2 BX = pk2(bx, bx), BY = pk2(by, by), BZ = pk2(bz, bz);
-                f32x2 TX = 0ull, TY = 0ull, TZ = 0ull;
-#pragma unroll 4
-                for (int m = rep; m < npair; m += nrep)
-                    body_pair(pbuf + m * 8, BX, BY, BZ, TX, TY, TZ);
-                tx = fold(TX);
-                ty = fold(TY);
-                tz = fold(TZ);
+                const float3 t3 = parts_one<GUARD>(pbuf, (np + 1) >> 1, rep, nrep, bx, by, bz, eps2);
+                tx = t3.x;
+                ty = t3.y;
+                tz = t3.z;
             } else {
 #pragma unroll 4
                 for (int j = rep; j < np; j += nrep) {
