@@ -28,10 +28,13 @@ constexpr int kSortMinTile = kSortThreads * kSortMinItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPre = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1;
+// Look-back words read per round trip: 8, 16 and 32 measured the same
+// (sort stage 0.260 / 0.260 / 0.264 ms at 2^20): past 8 the chain is not
+// what bounds a pass.
 #ifndef NB_SORT_LOOK
 #define NB_SORT_LOOK 8
 #endif
-constexpr int kLookBatch = NB_SORT_LOOK;  // look-back words read per round trip
+constexpr int kLookBatch = NB_SORT_LOOK;
 
 template <int ITEMS>
 const void* k_sort_pass_ptr();
