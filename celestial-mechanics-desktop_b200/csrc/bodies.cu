@@ -10,9 +10,11 @@ namespace nb {
 // round-to-nearest operations: v += (dt/2) a, x += dt v, exactly as the
 // reference rounds them.
 __global__ void k_kick_drift_bbox(int n, State s, int kick, double dt,
-                                  unsigned long long* bbox_ord, int* n_active, int* err) {
+                                  unsigned long long* bbox_ord, int* n_active, int* err,
+                                  const int* dn) {
     __shared__ double sh[6][8];
     __shared__ int sa[8];
+    n = dev_rows(n, dn);
     const double half = 0.5 * dt;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double lo[3] = {1.0e308 * 10, 1.0e308 * 10, 1.0e308 * 10};
@@ -72,9 +74,9 @@ __global__ void k_kick_drift_bbox(int n, State s, int kick, double dt,
 
 // Phases 4-5 (SoAVerletIntegrator.cs:95-116): v += (dt/2) a for active rows;
 // the acceleration buffer itself is the next step's "old" acceleration.
-__global__ void k_kick(int n, State s, double dt) {
+__global__ void k_kick(int n, State s, double dt, const int* dn) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !s.active[i]) return;
+    if (i >= dev_rows(n, dn) || !s.active[i]) return;
     const double half = 0.5 * dt;
     s.vx[i] = __dadd_rn(s.vx[i], __dmul_rn(half, s.ax[i]));
     s.vy[i] = __dadd_rn(s.vy[i], __dmul_rn(half, s.ay[i]));
@@ -122,8 +124,9 @@ constexpr int kKeyItems = 8;  // keys per thread: one block's histograms cover 2
 __global__ void __launch_bounds__(kKeyThreads)
 k_keys_cube(int n, State s, const double* __restrict__ cube, uint64_t* __restrict__ keys,
             uint32_t* __restrict__ vals, uint32_t* __restrict__ hist, double4* __restrict__ rows,
-            float* __restrict__ amag) {
+            float* __restrict__ amag, const int* dn) {
     __shared__ uint32_t sh[8][256];
+    n = dev_rows(n, dn);
     for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) (&sh[0][0])[t] = 0;
     __syncthreads();
     const double h = cube[3];
@@ -191,9 +194,9 @@ __global__ void k_keys_aabb(int n, State s, const unsigned long long* __restrict
 __global__ void k_gather(int n, State s, const uint32_t* __restrict__ sidx,
                          double4* __restrict__ sbody, float* __restrict__ srad,
                          float* __restrict__ samag, const double4* __restrict__ rows,
-                         const float* __restrict__ amag) {
+                         const float* __restrict__ amag, const int* dn) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= dev_rows(n, dn)) return;
     const uint32_t i = sidx[k];
     if (rows) {
         sbody[k] = rows[i];
@@ -209,26 +212,27 @@ __global__ void k_gather(int n, State s, const uint32_t* __restrict__ sidx,
     }
 }
 
-__global__ void k_zero_acc(int n, State s) {
+__global__ void k_zero_acc(int n, State s, const int* dn) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= dev_rows(n, dn)) return;
     s.ax[i] = 0.0;
     s.ay[i] = 0.0;
     s.az[i] = 0.0;
 }
 
 void launch_kick_drift_bbox(cudaStream_t st, int n, State s, bool kick, double dt,
-                            unsigned long long* bbox_ord, int* n_active, int* err) {
+                            unsigned long long* bbox_ord, int* n_active, int* err,
+                            const int* dn) {
     cudaMemsetAsync(bbox_ord, 0xFF, 3 * sizeof(unsigned long long), st);
     cudaMemsetAsync(bbox_ord + 3, 0, 3 * sizeof(unsigned long long), st);
     cudaMemsetAsync(n_active, 0, sizeof(int), st);
     if (n <= 0) return;
     k_kick_drift_bbox<<<ceil_div(n, 256), 256, 0, st>>>(n, s, kick ? 1 : 0, dt, bbox_ord,
-                                                        n_active, err);
+                                                        n_active, err, dn);
 }
 
-void launch_kick(cudaStream_t st, int n, State s, double dt) {
-    if (n > 0) k_kick<<<ceil_div(n, 256), 256, 0, st>>>(n, s, dt);
+void launch_kick(cudaStream_t st, int n, State s, double dt, const int* dn) {
+    if (n > 0) k_kick<<<ceil_div(n, 256), 256, 0, st>>>(n, s, dt, dn);
 }
 
 void launch_cube(cudaStream_t st, const unsigned long long* bbox_ord, const double* given,
@@ -238,11 +242,11 @@ void launch_cube(cudaStream_t st, const unsigned long long* bbox_ord, const doub
 
 void launch_keys_cube(cudaStream_t st, int n, const State& s, const double* cube,
                       uint64_t* keys, uint32_t* vals, uint32_t* hist, double4* rows,
-                      float* amag) {
+                      float* amag, const int* dn) {
     cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, st);
     if (n > 0)
         k_keys_cube<<<ceil_div(n, kKeyThreads * kKeyItems), kKeyThreads, 0, st>>>(
-            n, s, cube, keys, vals, hist, rows, amag);
+            n, s, cube, keys, vals, hist, rows, amag, dn);
 }
 
 void launch_keys_aabb(cudaStream_t st, int n, const State& s,
@@ -252,13 +256,14 @@ void launch_keys_aabb(cudaStream_t st, int n, const State& s,
 
 void launch_gather(cudaStream_t st, int n, const State& s, const uint32_t* sidx,
                    double4* sbody, float* srad, float* samag, const double4* rows,
-                   const float* amag) {
+                   const float* amag, const int* dn) {
     if (n > 0)
-        k_gather<<<ceil_div(n, 256), 256, 0, st>>>(n, s, sidx, sbody, srad, samag, rows, amag);
+        k_gather<<<ceil_div(n, 256), 256, 0, st>>>(n, s, sidx, sbody, srad, samag, rows, amag,
+                                                   dn);
 }
 
-void launch_zero_acc(cudaStream_t st, int n, State s) {
-    if (n > 0) k_zero_acc<<<ceil_div(n, 256), 256, 0, st>>>(n, s);
+void launch_zero_acc(cudaStream_t st, int n, State s, const int* dn) {
+    if (n > 0) k_zero_acc<<<ceil_div(n, 256), 256, 0, st>>>(n, s, dn);
 }
 
 }  // namespace nb

@@ -364,12 +364,111 @@ __device__ __forceinline__ int block_excl_count(bool flag, int* s_warp, int* tot
     return off + __popc(m & lanemask_lt());
 }
 
+// Ascending sort of the w pair keys (distinct) by the merge block itself,
+// so that the pair count never has to reach the host: up to kBitonicMax keys
+// a bitonic network in shared memory, above that a stable LSD radix sort of
+// 8 passes over the block in global memory (alt as the other buffer; the
+// result ends in keys).  The large case needs more than kBitonicMax pairs in
+// one step, over 100 times the disk workload's usual count.
+constexpr int kBitonicMax = 2048;
+
+__device__ void block_sort_pairs(uint64_t* keys, uint64_t* alt, int w) {
+    __shared__ uint64_t s_b[kBitonicMax];
+    __shared__ uint16_t s_wc[kMergeThreads / 32][256];  // per-warp digit counts, then offsets
+    __shared__ uint32_t s_base[256], s_tot[256];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (w <= 1) return;
+    if (w <= kBitonicMax) {
+        int n2 = 2;
+        while (n2 < w) n2 <<= 1;
+        for (int i = t; i < n2; i += kMergeThreads) s_b[i] = i < w ? keys[i] : ~0ull;
+        __syncthreads();
+        for (int k = 2; k <= n2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = t; i < n2; i += kMergeThreads) {
+                    const int ixj = i ^ j;
+                    if (ixj > i) {
+                        const uint64_t a = s_b[i], b = s_b[ixj];
+                        if ((a > b) == ((i & k) == 0)) {
+                            s_b[i] = b;
+                            s_b[ixj] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (int i = t; i < w; i += kMergeThreads) keys[i] = s_b[i];
+        __syncthreads();
+        return;
+    }
+    uint64_t* src = keys;
+    uint64_t* dst = alt;
+    for (int p = 0; p < 8; p++) {
+        const int shift = 8 * p;
+        if (t < 256) s_tot[t] = 0;
+        __syncthreads();
+        for (int i = t; i < w; i += kMergeThreads) atomicAdd(&s_tot[(src[i] >> shift) & 0xFF], 1u);
+        __syncthreads();
+        if (t == 0) {
+            uint32_t run = 0;
+            for (int d = 0; d < 256; d++) {
+                s_base[d] = run;
+                run += s_tot[d];
+            }
+        }
+        __syncthreads();
+        for (int c = 0; c < w; c += kMergeThreads) {
+            const int i = c + t;
+            const bool valid = i < w;
+            const uint64_t key = valid ? src[i] : 0ull;
+            const uint32_t d = (uint32_t)(key >> shift) & 0xFF;
+            for (int x = t; x < (kMergeThreads / 32) * 256; x += kMergeThreads) (&s_wc[0][0])[x] = 0;
+            __syncthreads();
+            unsigned peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                const unsigned bal = __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u);
+                peers &= ((d >> b) & 1u) ? bal : ~bal;
+            }
+            const int rank = __popc(peers & lanemask_lt());
+            if (valid && rank == 0) s_wc[warp][d] = (uint16_t)__popc(peers);
+            __syncthreads();
+            if (t < 256) {
+                uint32_t run = 0;
+                for (int x = 0; x < kMergeThreads / 32; x++) {
+                    const uint32_t v = s_wc[x][t];
+                    s_wc[x][t] = (uint16_t)run;
+                    run += v;
+                }
+                s_tot[t] = run;
+            }
+            __syncthreads();
+            if (valid) dst[s_base[d] + s_wc[warp][d] + rank] = key;
+            __syncthreads();
+            if (t < 256) s_base[t] += s_tot[t];
+            __syncthreads();
+        }
+        uint64_t* tmp = src;
+        src = dst;
+        dst = tmp;
+    }
+}
+
+// np_dev: with it the pair count is read on the device (the broad phase's
+// count, capped at np), the pairs are still unsorted and the block sorts them
+// first (pairs_alt: its second buffer); without it np pairs are sorted.
 __global__ void __launch_bounds__(kMergeThreads)
-k_merge_rounds(State s, const uint64_t* __restrict__ pairs, int np, int max_frame, int max_body,
-               int density_merge, double min_radius, int* __restrict__ counts,
-               int* __restrict__ owner, int* __restrict__ n_merges, int* err) {
+k_merge_rounds(State s, uint64_t* __restrict__ pairs, uint64_t* __restrict__ pairs_alt, int np,
+               const int* np_dev, int max_frame, int max_body, int density_merge,
+               double min_radius, int* __restrict__ counts, int* __restrict__ owner,
+               int* __restrict__ n_merges, int* err) {
     __shared__ int s_warp[kMergeThreads / 32];
     const int t = threadIdx.x;
+    if (np_dev) {
+        np = min(*np_dev, np);
+        block_sort_pairs(pairs, pairs_alt, np);
+    }
     int merged = 0;  // merges of the finished windows (the same in every thread)
     for (int base = 0; base < np && merged < max_frame; base += kMergeThreads) {
         const int k = base + t;
@@ -431,8 +530,9 @@ k_merge_rounds(State s, const uint64_t* __restrict__ pairs, int np, int max_fram
 // a ballot count per warp, a warp-wide decoupled look-back across tiles.
 __global__ void __launch_bounds__(kCompThreads)
 k_compact(int n, State s, int32_t* __restrict__ dest, uint32_t* look, uint32_t* tile_ctr,
-          int* n_kept, int* err) {
+          int* n_kept, int* err, const int* dn) {
     __shared__ int s_tile;
+    n = dev_rows(n, dn);  // tiles past the rows keep nothing
     __shared__ uint32_t s_wtot[kCompThreads / 32];
     __shared__ uint32_t s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -507,9 +607,10 @@ k_compact(int n, State s, int32_t* __restrict__ dest, uint32_t* look, uint32_t* 
 // The kept rows' 15 fields moved to their destination rows: one thread per
 // row, so every field's loads and stores of a warp are in flight together
 // (the rows keep their order, so the stores of a warp are nearly contiguous).
-__global__ void k_scatter_rows(int n, State s, State d, const int32_t* __restrict__ dest) {
+__global__ void k_scatter_rows(int n, State s, State d, const int32_t* __restrict__ dest,
+                               const int* dn) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= dev_rows(n, dn)) return;
     const int pos = dest[i];
     if (pos < 0) return;
     d.px[pos] = s.px[i]; d.py[pos] = s.py[i]; d.pz[pos] = s.pz[i];
@@ -521,14 +622,15 @@ __global__ void k_scatter_rows(int n, State s, State d, const int32_t* __restric
 }
 
 // dest: n destination rows (-1: removed); with `d` the kept rows are moved
-// into d's rows 0 .. *n_kept - 1.
+// into d's rows 0 .. *n_kept - 1.  dn: optional device row count (<= n).
 static void launch_compact(cudaStream_t st, CollideBufs& b, int n, const State& s,
-                           const State* d, int32_t* dest, int* n_kept, int* err) {
+                           const State* d, int32_t* dest, int* n_kept, int* err,
+                           const int* dn = nullptr) {
     const int tiles = ceil_div(n, kCompTile);
     cudaMemsetAsync(b.look, 0, sizeof(uint32_t) * (size_t)tiles, st);
     cudaMemsetAsync(b.tile_ctr, 0, sizeof(uint32_t), st);
-    k_compact<<<tiles, kCompThreads, 0, st>>>(n, s, dest, b.look, b.tile_ctr, n_kept, err);
-    if (d) k_scatter_rows<<<ceil_div(n, 256), 256, 0, st>>>(n, s, *d, dest);
+    k_compact<<<tiles, kCompThreads, 0, st>>>(n, s, dest, b.look, b.tile_ctr, n_kept, err, dn);
+    if (d) k_scatter_rows<<<ceil_div(n, 256), 256, 0, st>>>(n, s, *d, dest, dn);
 }
 
 int compact_indices(cudaStream_t st, CollideBufs& b, int n, const uint8_t* active,
@@ -539,6 +641,32 @@ int compact_indices(cudaStream_t st, CollideBufs& b, int n, const uint8_t* activ
     s.mass = (double*)mass;
     launch_compact(st, b, n, s, nullptr, dest, n_kept_dev, err);
     return cudaGetLastError() == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+// The collision stage with no host round trip, for a captured step: the
+// pair count stays on the device (the merge block sorts the pairs itself)
+// and the rows are counted by *dn, which the compaction's count replaces at
+// the end.  It queries the force evaluation's tree (a.reuse_tree); a.n and
+// a.n_active only bound the launches.
+int collide_step_device(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* dn) {
+    if (!a.reuse_tree) return NB_ERR_INVALID_ARG;
+    cudaMemsetAsync(a.n_pairs, 0, sizeof(int), st);
+    if (a.n <= 0) return NB_OK;
+    if (a.n_active > 0) {
+        find_groups(st, a.tree, a.sbody, a.n_active, a.groups, a.n_groups, 2.25, 0);
+        cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
+        k_broad_phase_groups<<<a.sms * 4, kBpWarps * 32, 0, st>>>(
+            a.s, a.keys0, a.vals0, a.tree, a.cube, a.groups, a.n_groups, a.group_ctr,
+            b.pair_keys, b.pair_cap, a.n_pairs, a.err);
+    }
+    cudaMemsetAsync(b.merge_count, 0, sizeof(int) * (size_t)a.n, st);
+    k_merge_rounds<<<1, kMergeThreads, 0, st>>>(a.s, b.pair_keys, b.pair_keys_alt, b.pair_cap,
+                                                a.n_pairs, a.max_frame, a.max_body,
+                                                a.density_merge, a.min_radius, b.merge_count,
+                                                b.owner, a.n_merges, a.err);
+    launch_compact(st, b, a.n, a.s, &a.s_alt, b.owner, a.n_kept, a.err, dn);
+    cudaMemcpyAsync(dn, a.n_kept, sizeof(int), cudaMemcpyDeviceToDevice, st);
+    return NB_OK;
 }
 
 int collide_step(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* npairs, int* nmerge,
@@ -552,9 +680,10 @@ int collide_step(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* npairs, i
     cudaMemsetAsync(a.n_merges, 0, sizeof(int), st);
     if (w > 0) {
         cudaMemsetAsync(b.merge_count, 0, sizeof(int) * (size_t)a.n, st);
-        k_merge_rounds<<<1, kMergeThreads, 0, st>>>(a.s, b.pair_keys, w, a.max_frame,
-                                                    a.max_body, a.density_merge, a.min_radius,
-                                                    b.merge_count, b.owner, a.n_merges, a.err);
+        k_merge_rounds<<<1, kMergeThreads, 0, st>>>(a.s, b.pair_keys, b.pair_keys_alt, w, nullptr,
+                                                    a.max_frame, a.max_body, a.density_merge,
+                                                    a.min_radius, b.merge_count, b.owner,
+                                                    a.n_merges, a.err);
     }
     // the merge's owner words are free again: they hold the destination rows
     launch_compact(st, b, a.n, a.s, &a.s_alt, b.owner, a.n_kept, a.err);

@@ -58,6 +58,10 @@ int broad_phase(cudaStream_t st, CollideBufs& b, CollideArgs& a, bool build_tree
 // Broad phase + merges + compaction of c.s into c.s_alt.
 int collide_step(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* npairs, int* nmerge,
                  int* nkept);
+// The same stage with every count kept on the device, for a captured step:
+// the rows are counted by *dn (replaced by the kept count at the end); needs
+// a.reuse_tree; a.n / a.n_active bound the launches.
+int collide_step_device(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* dn);
 // Destination rows of the order-preserving compaction (mask active && mass > 0).
 int compact_indices(cudaStream_t st, CollideBufs& b, int n, const uint8_t* active,
                     const double* mass, int32_t* dest, int* n_kept_dev, int* err);

@@ -134,4 +134,9 @@ __host__ __device__ __forceinline__ uint32_t compact21(uint64_t v) {
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// Rows of a launch sized on the host for n rows: with a device count `dn`
+// (a count that only shrinks inside a captured multi-step graph, e.g. the
+// rows left by the last compaction) the smaller of the two.
+__device__ __forceinline__ int dev_rows(int n, const int* dn) { return dn ? min(n, *dn) : n; }
+
 }  // namespace nb

@@ -45,7 +45,7 @@ struct Scal {
     int n_pairs;
     int n_kept;
     int n_merges;
-    int pad;
+    int n_rows;  // current row count of a captured collisional step
     unsigned long long amax2;  // bits of the largest |a|^2 (adaptive dt)
 };
 
@@ -151,6 +151,20 @@ struct nb_engine {
                    mac_budget == o.mac_budget && state == o.state;
         }
     } graph_key{};
+    // the collisional step captured twice, from each state buffer into the
+    // other (compaction alternates them): cstate[k] is graph k's source
+    // buffer; n and n_active in ckey are the launch bounds of the capture
+    cudaGraphExec_t cgraph[2] = {nullptr, nullptr};
+    GraphKey ckey{};
+    const double* cstate[2] = {nullptr, nullptr};
+    struct MergeKey {
+        int max_frame, max_body, density;
+        double min_radius;
+        bool operator==(const MergeKey& o) const {
+            return max_frame == o.max_frame && max_body == o.max_body && density == o.density &&
+                   min_radius == o.min_radius;
+        }
+    } cmerge{};
     bool ev_valid = false;
     bool ev_tree = false;
     bool ev_collide = false;   // ev[4], ev[5] bracket the last collision stage
@@ -244,8 +258,12 @@ void record(nb_engine* h, int k) {
 }
 
 // Forces for the current device rows.  kick: fuse the first half kick and
-// the drift of a Verlet step into the bounding-box pass.
-int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
+// the drift of a Verlet step into the bounding-box pass.  dn (Barnes-Hut
+// modes only): the rows are counted on the device (a captured collisional
+// step); h->n and h->n_active then only bound the launches, and the sorted
+// stages take the active count the bounding-box pass writes.
+int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt,
+                   const int* dn = nullptr) {
     const int mode = flags & NB_MODE_MASK;
     const bool shell = (flags & NB_FLAG_SHELL_THEOREM) != 0;
     // the collision broad phase reuses this evaluation's tree, which then
@@ -255,9 +273,13 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     Scal* sc = h->scal;
     h->tree_current = false;
     record(h, 0);
-    nb::launch_kick_drift_bbox(h->st, n, h->s, kick, dt, sc->bbox_ord, &sc->n_active, sc->err);
+    nb::launch_kick_drift_bbox(h->st, n, h->s, kick, dt, sc->bbox_ord, &sc->n_active, sc->err,
+                               dn);
     cudaMemsetAsync(sc->counters, 0, sizeof(sc->counters), h->st);
     h->ev_tree = false;
+    const int* dna = dn ? &sc->n_active : nullptr;
+    if (dn && mode != NB_MODE_BARNES_HUT)
+        return fail(h, NB_ERR_INVALID_ARG, "device row counts need NB_MODE_BARNES_HUT");
     if (mode == NB_MODE_DIRECT_FP64) {
         record(h, 1);
         record(h, 2);
@@ -285,12 +307,12 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     // the keys kernel also writes each row's (x, y, z, m) record and, for the
     // learned MAC, the previous step's |a| (before the buffer is zeroed)
     nb::launch_keys_cube(h->st, n, h->s, sc->cube, h->keys0, h->vals0, (uint32_t*)h->sort_ws,
-                         h->rows4, learned ? h->amag_rows : nullptr);
+                         h->rows4, learned ? h->amag_rows : nullptr, dn);
     nb::sort_pairs(h->st, n, h->keys0, h->vals0, h->keys1, h->vals1, h->sort_ws, true, sc->err,
-                   h->sms);
+                   h->sms, dn);
     nb::launch_gather(h->st, na, h->s, h->vals0, h->sbody, radii ? h->srad : nullptr,
-                      learned ? h->samag : nullptr, h->rows4, h->amag_rows);
-    nb::launch_zero_acc(h->st, n, h->s);
+                      learned ? h->samag : nullptr, h->rows4, h->amag_rows, dna);
+    nb::launch_zero_acc(h->st, n, h->s, dn);
     record(h, 1);
     if (mode == NB_MODE_DIRECT) {
         record(h, 2);
@@ -301,7 +323,7 @@ int force_pipeline(nb_engine* h, int flags, double eps, bool kick, double dt) {
     } else if (mode == NB_MODE_BARNES_HUT || mode == NB_MODE_BARNES_HUT_REF) {
         const bool ref = mode == NB_MODE_BARNES_HUT_REF;
         nb::tree_build(h->st, h->tree, na, h->keys0, h->sbody, radii ? h->srad : nullptr, sc->cube,
-                       ref ? 1 : h->leaf_cap, sc->err);
+                       ref ? 1 : h->leaf_cap, sc->err, nullptr, dna);
         h->ev_tree = true;
         h->tree_current = radii;
         record(h, 2);
@@ -544,6 +566,8 @@ NB_API int32_t nb_destroy(nb_engine* h) {
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    for (auto& g : h->cgraph)
+        if (g) cudaGraphExecDestroy(g);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
     return NB_OK;
@@ -776,10 +800,149 @@ namespace {
 int force_error_stats(nb_engine* h, int32_t n_samples, uint64_t seed, double softening,
                       double* out3, bool sorted = false);
 
+// The collision stage's arguments for the current state.
+nb::CollideArgs collide_args(nb_engine* h) {
+    nb::CollideArgs c{};
+    c.n = h->n;
+    c.n_active = h->n_active;
+    c.s = h->s;
+    c.s_alt = h->s_alt;
+    c.keys0 = h->keys0; c.keys1 = h->keys1; c.vals0 = h->vals0; c.vals1 = h->vals1;
+    c.sort_ws = h->sort_ws;
+    c.tree = h->tree;
+    c.sbody = h->sbody;
+    c.srad = h->srad;
+    c.cube = h->scal->cube;
+    c.leaf_cap = h->leaf_cap;
+    c.max_frame = h->max_merges_frame;
+    c.max_body = h->max_merges_body;
+    c.density_merge = h->density_merge;
+    c.min_radius = h->min_radius;
+    c.n_pairs = &h->scal->n_pairs;
+    c.n_kept = &h->scal->n_kept;
+    c.n_merges = &h->scal->n_merges;
+    c.err = h->scal->err;
+    c.sms = h->sms;
+    c.bbox_ord = h->scal->bbox_ord;
+    c.n_active_dev = &h->scal->n_active;
+    // the second half kick moved no body: the force evaluation's tree
+    // (Barnes-Hut modes) still describes the positions
+    c.reuse_tree = h->tree_current;
+    c.groups = h->groups;
+    c.n_groups = &h->scal->n_groups;
+    c.group_ctr = &h->scal->group_ctr;
+    return c;
+}
+
+// Capture one collisional step (sub-steps, kicks, collision stage) from the
+// current state buffer into the other, every count on the device.
+int capture_collide_step(nb_engine* h, int flags, double dt, double eps, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    NB_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int* dn = &h->scal->n_rows;
+    double sub[3];
+    const int ns = sub_steps(flags, dt, sub);
+    int r = NB_OK;
+    for (int k = 0; k < ns && r == NB_OK; k++) {
+        r = force_pipeline(h, flags, eps, true, sub[k], dn);
+        if (r == NB_OK) nb::launch_kick(h->st, h->n, h->s, sub[k], dn);
+    }
+    if (r == NB_OK) {
+        nb::CollideArgs c = collide_args(h);
+        if (nb::collide_step_device(h->st, h->col, c, dn) != NB_OK)
+            r = fail(h, NB_ERR_INVALID_ARG, "captured collision stage needs the step's tree");
+    }
+    h->tree_current = false;
+    const cudaError_t e = cudaStreamEndCapture(h->st, &g);
+    if (r != NB_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(h, NB_ERR_CUDA, "collision step capture: %s", cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        *out = nullptr;
+        return fail(h, NB_ERR_CUDA, "collision step graph: %s", cudaGetErrorString(ei));
+    }
+    return NB_OK;
+}
+
+// n_steps collisional Barnes-Hut steps (geometric MAC) as replays of the two
+// captured steps: nothing returns to the host between steps.  The captures
+// are kept while the parameters match and the rows stay within 1/32 below
+// the bounds they were captured with (the launches are sized by the bounds).
+int run_collide_graphs(nb_engine* h, int n_steps, double dt, double eps, int flags) {
+    nb_engine::GraphKey key{flags,           h->n,           h->n_active,
+                            h->leaf_cap,     h->group_span,  h->group_bodies,
+                            dt,              eps,
+                            h->theta,        h->group_pack,  h->mac_theta_lo,
+                            h->mac_theta_hi, h->mac_budget,  nullptr};
+    const nb_engine::MergeKey mk{h->max_merges_frame, h->max_merges_body, h->density_merge,
+                                 h->min_radius};
+    nb_engine::GraphKey have = h->ckey;
+    const bool fits = h->cgraph[0] && h->cgraph[1] && h->n <= have.n &&
+                      h->n >= have.n - have.n / 32 && h->n_active <= have.n_active &&
+                      (h->s.px == h->cstate[0] || h->s.px == h->cstate[1]) && mk == h->cmerge;
+    have.n = key.n;
+    have.n_active = key.n_active;
+    int r = NB_OK;
+    if (!(fits && have == key)) {
+        for (auto& g : h->cgraph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        NB_CUDA(h, cudaStreamSynchronize(h->st));
+        const int timing = h->timing;
+        h->timing = 0;
+        // capture from buffer A into B, then from B into A; the two swaps
+        // leave the state where it was
+        for (int k = 0; k < 2; k++) {
+            h->cstate[k] = h->s.px;
+            if (r == NB_OK) r = capture_collide_step(h, flags, dt, eps, &h->cgraph[k]);
+            std::swap(h->s, h->s_alt);
+        }
+        h->timing = timing;
+        if (r) {
+            for (auto& g : h->cgraph)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+            return r;
+        }
+        h->ckey = key;
+        h->cmerge = mk;
+    }
+    NB_CUDA(h, cudaMemcpyAsync(&h->scal->n_rows, &h->n, sizeof(int), cudaMemcpyHostToDevice,
+                               h->st));
+    const int first = h->s.px == h->cstate[0] ? 0 : 1;
+    for (int k = 0; k < n_steps; k++)
+        NB_CUDA(h, cudaGraphLaunch(h->cgraph[(first + k) & 1], h->st));
+    if (n_steps & 1) std::swap(h->s, h->s_alt);
+    h->tree_current = false;
+    h->ev_valid = false;
+    h->ev_collide = false;
+    int cnt[4] = {0, 0, 0, 0};  // n_pairs, n_kept, n_merges, n_rows
+    if ((r = download(h, cnt, &h->scal->n_pairs, sizeof(cnt)))) return r;
+    r = check_device(h);  // synchronises: cnt holds the last step's counts
+    h->n = cnt[3];
+    h->n_active = cnt[3];  // compaction keeps exactly the active rows
+    h->counters[NB_C_PAIRS] = cnt[0];
+    h->counters[NB_C_MERGES] = cnt[2];
+    if (r) return r;
+    collect_counters(h);
+    return NB_OK;
+}
+
 // n_steps Verlet steps with one flag set (no audits).
 int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags) {
     const bool collide = (flags & NB_FLAG_COLLISIONS) != 0;
     int r;
+    if (collide && n_steps > 1 && (flags & NB_MODE_MASK) == NB_MODE_BARNES_HUT &&
+        !(flags & NB_FLAG_LEARNED_MAC))
+        return run_collide_graphs(h, n_steps, dt, softening, flags);
     if (!collide && n_steps > 1) {
         // Multi-step calls replay one captured step (a CUDA graph) n times;
         // the row and active counts do not change without collisions.
@@ -802,35 +965,7 @@ int run_steps(nb_engine* h, int n_steps, double dt, double softening, int flags)
         // (NBodySolver.cs:408-430) and the reference engine's GPU paths after
         // the last sub-step (engine.cpp:1160-1190)
         if (collide && k % ns == ns - 1) {
-            nb::CollideArgs c{};
-            c.n = h->n;
-            c.n_active = h->n_active;
-            c.s = h->s;
-            c.s_alt = h->s_alt;
-            c.keys0 = h->keys0; c.keys1 = h->keys1; c.vals0 = h->vals0; c.vals1 = h->vals1;
-            c.sort_ws = h->sort_ws;
-            c.tree = h->tree;
-            c.sbody = h->sbody;
-            c.srad = h->srad;
-            c.cube = h->scal->cube;
-            c.leaf_cap = h->leaf_cap;
-            c.max_frame = h->max_merges_frame;
-            c.max_body = h->max_merges_body;
-            c.density_merge = h->density_merge;
-            c.min_radius = h->min_radius;
-            c.n_pairs = &h->scal->n_pairs;
-            c.n_kept = &h->scal->n_kept;
-            c.n_merges = &h->scal->n_merges;
-            c.err = h->scal->err;
-            c.sms = h->sms;
-            c.bbox_ord = h->scal->bbox_ord;
-            c.n_active_dev = &h->scal->n_active;
-            // the second half kick moved no body: the force evaluation's tree
-            // (Barnes-Hut modes) still describes the positions
-            c.reuse_tree = h->tree_current;
-            c.groups = h->groups;
-            c.n_groups = &h->scal->n_groups;
-            c.group_ctr = &h->scal->group_ctr;
+            nb::CollideArgs c = collide_args(h);
             int npairs = 0, nmerge = 0, nkept = 0;
             record(h, 4);
             if ((r = nb::collide_step(h->st, h->col, c, &npairs, &nmerge, &nkept)))

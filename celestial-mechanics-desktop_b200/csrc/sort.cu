@@ -58,8 +58,9 @@ size_t sort_workspace_bytes(int capacity) {
 // Digit histograms of all 8 passes (used when the keys were not produced by a
 // kernel that already counted them).
 __global__ void k_sort_histogram(int n, const uint64_t* __restrict__ keys,
-                                 uint32_t* __restrict__ hist) {
+                                 uint32_t* __restrict__ hist, const int* dn) {
     __shared__ uint32_t sh[8][256];
+    n = dev_rows(n, dn);
     for (int t = threadIdx.x; t < 8 * 256; t += blockDim.x) (&sh[0][0])[t] = 0;
     __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -111,7 +112,8 @@ template <int ITEMS>
 __global__ void __launch_bounds__(kSortThreads, 3)
 k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin,
             uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
-            const uint32_t* __restrict__ hist, uint32_t* look, uint32_t* tile_ctr, int* err) {
+            const uint32_t* __restrict__ hist, uint32_t* look, uint32_t* tile_ctr, int* err,
+            const int* dn) {
     constexpr int kSortItems = ITEMS;
     constexpr int kSortTile = kSortThreads * ITEMS;
     extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -130,6 +132,10 @@ k_sort_pass(int n, int shift, const uint64_t* __restrict__ kin, const uint32_t* 
     __syncthreads();
     const int tile = s_tile;
     const int base = tile * kSortTile;
+    n = dev_rows(n, dn);
+    // tiles past a device count that shrank: nothing to sort, and no later
+    // tile looks back at them
+    if (base >= n && tile > 0) return;
     const int valid = min(kSortTile, n - base);
 
     // Load: warp w owns the contiguous segment [base + 32 ITEMS w, + 32 ITEMS),
@@ -263,7 +269,7 @@ const void* k_sort_pass_ptr() {
 // launch alone, so an error left pending by earlier unrelated work is
 // neither reported nor cleared here).
 cudaError_t sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint64_t* k1,
-                       uint32_t* v1, void* ws, bool hist_ready, int* err, int sms) {
+                       uint32_t* v1, void* ws, bool hist_ready, int* err, int sms, const int* dn) {
     if (n <= 1) return cudaSuccess;
     uint32_t* hist = (uint32_t*)ws;
     uint32_t* ctr = hist + 8 * 256;
@@ -284,7 +290,7 @@ cudaError_t sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint6
         cfg.gridDim = dim3(min(ceil_div(n, 256 * 8), sms * 8));
         cfg.blockDim = dim3(256);
         cfg.dynamicSmemBytes = 0;
-        if ((e = cudaLaunchKernelEx(&cfg, k_sort_histogram, n, (const uint64_t*)k0, hist)) !=
+        if ((e = cudaLaunchKernelEx(&cfg, k_sort_histogram, n, (const uint64_t*)k0, hist, dn)) !=
             cudaSuccess)
             return e;
     }
@@ -299,12 +305,13 @@ cudaError_t sort_pairs(cudaStream_t st, int n, uint64_t* k0, uint32_t* v0, uint6
     cfg.blockDim = dim3(kSortThreads);
     cfg.dynamicSmemBytes = (size_t)items * kSortThreads * 16;
     using Pass = void (*)(int, int, const uint64_t*, const uint32_t*, uint64_t*, uint32_t*,
-                          const uint32_t*, uint32_t*, uint32_t*, int*);
+                          const uint32_t*, uint32_t*, uint32_t*, int*, const int*);
     const Pass pass = items == 16 ? k_sort_pass<16> : items == 8 ? k_sort_pass<8> : k_sort_pass<4>;
     for (int p = 0; p < 8; p++) {
         if ((e = cudaLaunchKernelEx(&cfg, pass, n, 8 * p, (const uint64_t*)ks,
                                     (const uint32_t*)vs, kd, vd, (const uint32_t*)(hist + 256 * p),
-                                    look + (size_t)p * tiles * 256, ctr + p, err)) != cudaSuccess)
+                                    look + (size_t)p * tiles * 256, ctr + p, err, dn)) !=
+            cudaSuccess)
             return e;
         uint64_t* tk = ks; ks = kd; kd = tk;
         uint32_t* tv = vs; vs = vd; vd = tv;

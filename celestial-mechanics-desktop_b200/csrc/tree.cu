@@ -92,7 +92,8 @@ __device__ __forceinline__ int prefix_len(const uint64_t* __restrict__ k, int n,
     return 63 + __clz(i ^ j);
 }
 
-__global__ void k_radix_tree(int n, const uint64_t* __restrict__ keys, TreeBufs t) {
+__global__ void k_radix_tree(int n, const uint64_t* __restrict__ keys, TreeBufs t, const int* dn) {
+    n = dev_rows(n, dn);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int dl = prefix_len(keys, n, i, i - 1);
@@ -159,9 +160,9 @@ __device__ __forceinline__ bool walk_internal(const TreeBufs& t, int x, int leaf
 }
 
 __global__ void __launch_bounds__(kMarkThreads)
-k_octree_mark(int n, TreeBufs t, int leaf_cap) {
+k_octree_mark(int n, TreeBufs t, int leaf_cap, const int* dn) {
     __shared__ int s_red[kMarkThreads / 32];
-    const int m = n - 1;  // internal nodes
+    const int m = dev_rows(n, dn) - 1;  // internal nodes (blocks past them sum 0)
     int local = 0;
     for (int k = 0; k < kMarkItems; k++) {
         int i = blockIdx.x * kMarkTile + k * kMarkThreads + threadIdx.x;
@@ -194,8 +195,9 @@ k_octree_mark(int n, TreeBufs t, int leaf_cap) {
 }
 
 // Exclusive scan of the block sums in one block; writes the node count.
-__global__ void k_scan_block_sums(int nblocks, TreeBufs t, int n) {
+__global__ void k_scan_block_sums(int nblocks, TreeBufs t, int n, const int* dn) {
     __shared__ int s[1024];
+    n = dev_rows(n, dn);
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
@@ -219,9 +221,9 @@ __global__ void k_scan_block_sums(int nblocks, TreeBufs t, int n) {
 }
 
 // Child slot of every walk-internal node: 1 + exclusive scan of bnchild.
-__global__ void __launch_bounds__(kMarkThreads) k_octree_base(int n, TreeBufs t) {
+__global__ void __launch_bounds__(kMarkThreads) k_octree_base(int n, TreeBufs t, const int* dn) {
     __shared__ int s_w[kMarkThreads / 32];
-    const int m = n - 1;
+    const int m = dev_rows(n, dn) - 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int off = 1 + t.block_sums[blockIdx.x];
     for (int k = 0; k < kMarkItems; k++) {
@@ -242,7 +244,8 @@ __global__ void __launch_bounds__(kMarkThreads) k_octree_base(int n, TreeBufs t)
     }
 }
 
-__global__ void k_octree_emit(int n, TreeBufs t, int leaf_cap) {
+__global__ void k_octree_emit(int n, TreeBufs t, int leaf_cap, const int* dn) {
+    n = dev_rows(n, dn);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (n == 1) {
         if (i == 0) {
@@ -454,7 +457,7 @@ static int leaves_grid() {
 
 void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys,
                 const double4* sbody, const float* srad, const double* cube, int leaf_cap,
-                int* err, const double* sys_half16) {
+                int* err, const double* sys_half16, const int* dn) {
     (void)err;
     if (n <= 0) {
         cudaMemsetAsync(t.n_nodes, 0, sizeof(int), st);
@@ -463,12 +466,12 @@ void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys
     const int m = n - 1;
     const int nblk = ceil_div(m > 0 ? m : 1, kMarkTile);
     if (m > 0) {
-        k_radix_tree<<<ceil_div(m, 256), 256, 0, st>>>(n, skeys, t);
-        k_octree_mark<<<nblk, kMarkThreads, 0, st>>>(n, t, leaf_cap);
+        k_radix_tree<<<ceil_div(m, 256), 256, 0, st>>>(n, skeys, t, dn);
+        k_octree_mark<<<nblk, kMarkThreads, 0, st>>>(n, t, leaf_cap, dn);
     }
-    k_scan_block_sums<<<1, 1024, 0, st>>>(m > 0 ? nblk : 0, t, n);
-    if (m > 0) k_octree_base<<<nblk, kMarkThreads, 0, st>>>(n, t);
-    k_octree_emit<<<ceil_div(m > 0 ? m : 1, 256), 256, 0, st>>>(n, t, leaf_cap);
+    k_scan_block_sums<<<1, 1024, 0, st>>>(m > 0 ? nblk : 0, t, n, dn);
+    if (m > 0) k_octree_base<<<nblk, kMarkThreads, 0, st>>>(n, t, dn);
+    k_octree_emit<<<ceil_div(m > 0 ? m : 1, 256), 256, 0, st>>>(n, t, leaf_cap, dn);
     cudaMemsetAsync(t.counter, 0, sizeof(int) * 2 * (size_t)n, st);
     cudaMemsetAsync(t.n_leaves, 0, sizeof(int), st);
     k_multipole_leaves<<<std::min(ceil_div(2 * n, 256), leaves_grid()), 256, 0, st>>>(

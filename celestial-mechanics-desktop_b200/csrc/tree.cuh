@@ -43,9 +43,10 @@ void tree_carve(TreeBufs& t, void* base, int capacity);
 // srad may be null (then max radius is 0).  Batched systems: the keys hold
 // the system index in bits 62..51 (four octree levels) and a 17-bit-per-axis
 // Morton code in that system's own cube below; sys_half16[s] = that cube's
-// half-size x 16 (cube is then unused).
+// half-size x 16 (cube is then unused).  dn: optional device body count
+// replacing n when smaller (the launches stay sized for n).
 void tree_build(cudaStream_t st, const TreeBufs& t, int n, const uint64_t* skeys,
                 const double4* sbody, const float* srad, const double* cube, int leaf_cap,
-                int* err, const double* sys_half16 = nullptr);
+                int* err, const double* sys_half16 = nullptr, const int* dn = nullptr);
 
 }  // namespace nb

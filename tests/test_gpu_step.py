@@ -306,6 +306,44 @@ def test_collisional_steps_conserve_mass_and_momentum(engine):
     assert len(ids) <= 20_001 and np.all(np.diff(ids) > 0)
 
 
+def _collisional_run(d, flags, dt, steps, one_by_one):
+    from nbody_b200 import Engine
+
+    with Engine(1 << 21, device=0) as e:  # room for the pairs of the first steps
+        e.set_state(d, old_acc=False)
+        if one_by_one:
+            for _ in range(steps):
+                e.step(1, dt, 1e-4, flags)
+        else:
+            e.step(steps, dt, 1e-4, flags)
+        st, ids = e.get_state()
+        return st, ids, e.counters()
+
+
+@pytest.mark.parametrize("n, scale, dt, steps, yoshida", [
+    (20_000, 1500.0, 1e-3, 5, False),     # merges in every step, odd step count
+    (262_145, 100.0, 0.0, 3, False),      # 2,093 pairs in the first step: the large pair sort
+    (20_000, 1500.0, 1e-3, 4, True),      # Yoshida4 sub-steps, collisions after the last
+])
+def test_captured_collisional_steps_equal_single_steps(n, scale, dt, steps, yoshida):
+    """Multi-step collisional calls replay two captured steps that keep every
+    count on the device (the merge block sorts the pairs itself; compaction
+    hands the row count to the next step): the state, row ids and the last
+    step's pair and merge counts equal those of one nb_step(1) per step, the
+    path pinned to the oracle above, bit for bit."""
+    d = scenarios.collisional_disk(n - 1, seed=2, radius_scale=scale)
+    flags = MODE_BARNES_HUT | FLAG_SHELL_THEOREM | FLAG_COLLISIONS
+    if yoshida:
+        flags |= FLAG_YOSHIDA4
+    a, ida, ca = _collisional_run(d, flags, dt, steps, one_by_one=False)
+    b, idb, cb = _collisional_run(d, flags, dt, steps, one_by_one=True)
+    assert len(ida) < n  # bodies merged
+    np.testing.assert_array_equal(ida, idb)
+    for k in ("px", "py", "pz", "vx", "vy", "vz", "ax", "ay", "az", "mass", "radius"):
+        np.testing.assert_array_equal(getattr(a, k), getattr(b, k), err_msg=k)
+    assert ca[N.C_PAIRS] == cb[N.C_PAIRS] and ca[N.C_MERGES] == cb[N.C_MERGES]
+
+
 def test_step_before_state_is_an_error():
     from nbody_b200 import Engine
 
