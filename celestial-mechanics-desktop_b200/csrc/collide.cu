@@ -62,10 +62,10 @@ int collide_alloc(CollideBufs& b, int capacity, const std::function<int(void**, 
 
 // Warp-cooperative broad phase: one warp per walk group of up to 32
 // consecutive sorted bodies.  The warp walks the tree once for the group's
-// box, the union of its collidable bodies' spheres (x +- r) widened by the
-// same pad as the cell boxes: a node is accepted when the gap between the
-// group box and its padded cell box is within the node's largest radius
-// (1 + 1e-9).  The ball of every body lies inside the group box, so every
+// box, the union of its collidable bodies' spheres (x +- r) widened by a pad
+// of 1e-9 of the cube's half-size, as the nodes' body boxes are: a node is
+// accepted when the gap between the group box and its padded body box is
+// within the node's largest radius (1 + 1e-9).  The ball of every body lies inside the group box, so every
 // node a body's own query accepts is accepted here; accepted leaves are
 // collected, and each lane runs the exact FP64 test of its body against their
 // bodies (higher rows only), so the pair set is the per-body query's.
@@ -74,8 +74,7 @@ constexpr int kBpStack = 1024;   // nodes pending per warp
 constexpr int kBpLeaves = 64;    // candidate leaves per evaluation
 
 __global__ void __launch_bounds__(kBpWarps * 32)
-k_broad_phase_groups(State s, const uint64_t* __restrict__ skeys,
-                     const uint32_t* __restrict__ sidx, TreeBufs t,
+k_broad_phase_groups(State s, const uint32_t* __restrict__ sidx, TreeBufs t,
                      const double* __restrict__ cube, const int2* __restrict__ groups,
                      const int* __restrict__ n_groups, unsigned* group_ctr,
                      uint64_t* __restrict__ pairs, int cap, int* __restrict__ count, int* err) {
@@ -92,9 +91,7 @@ k_broad_phase_groups(State s, const uint64_t* __restrict__ skeys,
     double* cz = s_cand[warp][2];
     double* crad = s_cand[warp][3];
     uint32_t* cr = s_crow[warp];
-    const double h = cube[3];
-    const double lo[3] = {cube[0] - h, cube[1] - h, cube[2] - h};
-    const double pad = 1e-9 * h;
+    const double pad = 1e-9 * cube[3];
     const int ng = *n_groups;
     const int nnodes = *t.n_nodes;
     for (;;) {
@@ -188,17 +185,18 @@ k_broad_phase_groups(State s, const uint64_t* __restrict__ skeys,
             bool accept = false;
             int4 lk = make_int4(0, 0, 0, 0);
             if (node >= 0) {
+                // the node's body box (FP32, rounded outwards, so it holds
+                // every body of the node) and its largest radius: the words
+                // arrive together, and the box is tighter than the cell's
                 lk = t.link[node];
                 const float reach = t.q1[node].z;
-                const int Lv = t.level[node];
-                const uint64_t key = skeys[lk.z];
-                const double w = ldexp(2.0 * h, -Lv);
-                const uint32_t c[3] = {compact21(key >> 2) >> (21 - Lv),
-                                       compact21(key >> 1) >> (21 - Lv), compact21(key) >> (21 - Lv)};
+                const float4 bl = t.blo[node], bh = t.bhi[node];
+                const double b0[3] = {(double)bl.x - pad, (double)bl.y - pad, (double)bl.z - pad};
+                const double b1[3] = {(double)bh.x + pad, (double)bh.y + pad, (double)bh.z + pad};
                 double d2 = 0.0;
                 for (int a = 0; a < 3; a++) {
-                    const double b0 = lo[a] + c[a] * w - pad, b1 = lo[a] + (c[a] + 1) * w + pad;
-                    const double e = ghi[a] < b0 ? b0 - ghi[a] : (glo[a] > b1 ? glo[a] - b1 : 0.0);
+                    const double e = ghi[a] < b0[a] ? b0[a] - ghi[a]
+                                                    : (glo[a] > b1[a] ? glo[a] - b1[a] : 0.0);
                     d2 += e * e;
                 }
                 const double rr = (double)reach;
@@ -255,7 +253,7 @@ int broad_phase(cudaStream_t st, CollideBufs& b, CollideArgs& a, bool build_tree
         find_groups(st, a.tree, a.sbody, a.n_active, a.groups, a.n_groups, 2.25, 0);
         cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
         k_broad_phase_groups<<<a.sms * 4, kBpWarps * 32, 0, st>>>(
-            a.s, a.keys0, a.vals0, a.tree, a.cube, a.groups, a.n_groups, a.group_ctr,
+            a.s, a.vals0, a.tree, a.cube, a.groups, a.n_groups, a.group_ctr,
             b.pair_keys, b.pair_cap, a.n_pairs, a.err);
     }
     int cnt = 0;
@@ -656,7 +654,7 @@ int collide_step_device(cudaStream_t st, CollideBufs& b, CollideArgs& a, int* dn
         find_groups(st, a.tree, a.sbody, a.n_active, a.groups, a.n_groups, 2.25, 0);
         cudaMemsetAsync(a.group_ctr, 0, sizeof(unsigned), st);
         k_broad_phase_groups<<<a.sms * 4, kBpWarps * 32, 0, st>>>(
-            a.s, a.keys0, a.vals0, a.tree, a.cube, a.groups, a.n_groups, a.group_ctr,
+            a.s, a.vals0, a.tree, a.cube, a.groups, a.n_groups, a.group_ctr,
             b.pair_keys, b.pair_cap, a.n_pairs, a.err);
     }
     cudaMemsetAsync(b.merge_count, 0, sizeof(int) * (size_t)a.n, st);
