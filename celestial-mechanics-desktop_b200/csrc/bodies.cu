@@ -1,6 +1,8 @@
 // bodies.cu - per-body kernels of the step.
 #include "bodies.cuh"
 
+#include <algorithm>
+
 namespace nb {
 
 // Half kick + drift of SoAVerletIntegrator.Step phases 1-2
@@ -16,11 +18,14 @@ __global__ void k_kick_drift_bbox(int n, State s, int kick, double dt,
     __shared__ int sa[8];
     n = dev_rows(n, dn);
     const double half = 0.5 * dt;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double lo[3] = {1.0e308 * 10, 1.0e308 * 10, 1.0e308 * 10};
     double hi[3] = {-lo[0], -lo[0], -lo[0]};
     int act = 0;
-    if (i < n && s.active[i]) {
+    // a grid-stride loop over a few resident waves of blocks: each block adds
+    // its box and count to the 7 global words once (one block per 256 rows
+    // made those same-address atomics, not memory, bound the pass at 8M rows)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!s.active[i]) continue;
         double x = s.px[i], y = s.py[i], z = s.pz[i];
         if (kick) {
             double vx = __dadd_rn(s.vx[i], __dmul_rn(half, s.ax[i]));
@@ -34,10 +39,10 @@ __global__ void k_kick_drift_bbox(int n, State s, int kick, double dt,
         }
         if (!isfinite(x) || !isfinite(y) || !isfinite(z) || !isfinite(s.mass[i]))
             dev_flag(err, kErrNonFinite);
-        lo[0] = hi[0] = x;
-        lo[1] = hi[1] = y;
-        lo[2] = hi[2] = z;
-        act = 1;
+        lo[0] = fmin(lo[0], x); hi[0] = fmax(hi[0], x);
+        lo[1] = fmin(lo[1], y); hi[1] = fmax(hi[1], y);
+        lo[2] = fmin(lo[2], z); hi[2] = fmax(hi[2], z);
+        act++;
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -227,8 +232,8 @@ void launch_kick_drift_bbox(cudaStream_t st, int n, State s, bool kick, double d
     cudaMemsetAsync(bbox_ord + 3, 0, 3 * sizeof(unsigned long long), st);
     cudaMemsetAsync(n_active, 0, sizeof(int), st);
     if (n <= 0) return;
-    k_kick_drift_bbox<<<ceil_div(n, 256), 256, 0, st>>>(n, s, kick ? 1 : 0, dt, bbox_ord,
-                                                        n_active, err, dn);
+    k_kick_drift_bbox<<<std::min(ceil_div(n, 256), kSMs * 8), 256, 0, st>>>(
+        n, s, kick ? 1 : 0, dt, bbox_ord, n_active, err, dn);
 }
 
 void launch_kick(cudaStream_t st, int n, State s, double dt, const int* dn) {

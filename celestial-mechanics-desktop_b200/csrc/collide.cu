@@ -374,7 +374,7 @@ __device__ void block_sort_pairs(uint64_t* keys, uint64_t* alt, int w) {
     __shared__ uint64_t s_b[kBitonicMax];
     __shared__ uint16_t s_wc[kMergeThreads / 32][256];  // per-warp digit counts, then offsets
     __shared__ uint32_t s_base[256], s_tot[256];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int t = threadIdx.x, warp = t >> 5;
     if (w <= 1) return;
     if (w <= kBitonicMax) {
         int n2 = 2;
