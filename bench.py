@@ -207,7 +207,7 @@ def run_reference(args, ws, rank):
     """The reference's own CPU Barnes-Hut (oracle/_ref: BarnesHutSolver with
     its job system on all host threads, theta 0.5, monopole, FP64) on the
     headline input: W untimed and K timed full force evaluations, and its
-    force error on the same 4096 sampled bodies the engine's arms are judged
+    force error on the same 4096 sampled bodies the engine's arms are measured
     on.  Only the scenario generator of the package is imported, so the
     engine library is never loaded in this process."""
     if rank != 0:
@@ -325,7 +325,7 @@ RMS_TARGET = 1e-3
 # that the force error after the timed steps (the state moves) stays within it
 CALIBRATION_TARGET = 0.98 * RMS_TARGET
 # the in-run audit samples 1024 bodies, whose rms scatters by about 10 %
-# around the 4096-sample figure the target is judged on; its fallback bound
+# around the 4096-sample figure the target is stated on; its fallback bound
 # sits 20 % above the target so that only a real failure of the criterion
 # (errors several times the target) switches to the geometric MAC
 AUDIT_SAMPLES, AUDIT_RMS_BOUND = 1024, 1.2 * RMS_TARGET

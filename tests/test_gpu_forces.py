@@ -7,7 +7,7 @@ Tolerances:
   * NB_MODE_BARNES_HUT_REF (FP64, reference MAC): per-body relative error vs
     the reference BarnesHutSolver max < 1e-9.
   * NB_MODE_BARNES_HUT, theta 0.5, monopole + quadrupole: rms relative force
-    error vs the FP64 direct sum < 1e-3 (the north-star budget).
+    error vs the FP64 direct sum < 1e-3 (the engine's force-error target).
 """
 from __future__ import annotations
 
