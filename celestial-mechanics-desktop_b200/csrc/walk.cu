@@ -260,19 +260,13 @@ __global__ void __launch_bounds__(WalkShape<MAC, SHAPE, GS>::warps * 32,
                                   WalkShape<MAC, SHAPE, GS>::min_blocks)
 k_walk_group(WalkArgs a) {
     constexpr int WARPS = WalkShape<MAC, SHAPE, GS>::warps;
-    // two-body lanes evaluate each cell-list block for both bodies in one
-    // pass (one shared-memory read of the block for the two); the learned
-    // walk, at its register limit, evaluates the cell list once per body
-#ifdef NB_WALK_FUSE2_LEARNED
-    constexpr bool FUSE2 = true;
-#else
-    constexpr bool FUSE2 = MAC == kMacGeometric;
-#endif
-    // the particle list is lighter: its one pass for both bodies fits the
-    // learned walk's registers too (8 bytes spilled against 12 with one pass
-    // per body) and measured 2.22 -> 2.16 ms at 2^20; each body's terms are
-    // summed in the same order either way
-    constexpr bool FUSE2_PARTS = FUSE2 || MAC == kMacLearned;
+    // two-body lanes evaluate each list block for both bodies in one pass
+    // (one shared-memory read of the block for the two; each body's terms
+    // are summed in the same order as in a pass per body).  The harvest walk
+    // keeps a pass per body.  The learned walk fits the fused passes only
+    // because no list is flushed inside a round (see the loop below): with
+    // flushes there it spilled 76-92 bytes and ran 2.22 -> 3.07 ms at 2^20
+    constexpr bool FUSE2 = MAC != kMacHarvest;
     extern __shared__ __align__(16) float s_walk[];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -518,7 +512,7 @@ k_walk_group(WalkArgs a) {
                 }
             }
             float tx, ty, tz, tp;
-            if (!SHELL && !POT && FUSE2_PARTS && two) {
+            if (!SHELL && !POT && FUSE2 && two) {
                 float ux, uy, uz;
                 eval_parts2(tx, ty, tz, ux, uy, uz);
                 kahan(sbx, cbx, ux);
@@ -559,8 +553,7 @@ k_walk_group(WalkArgs a) {
             // 1. accepted cells -> cell list
             const unsigned mcell = __ballot_sync(FULL, take_cell);
             if (mcell) {
-                const int k = __popc(mcell);
-                if (nc + k > kCellCap) flush_cells();
+                const int k = __popc(mcell);  // room was made at the round's start
                 if (take_cell) {
                     const int cs = nc + __popc(mcell & lanemask_lt());
                     float* e = cbuf + (cs >> 1) * 20 + (cs & 1);
@@ -668,6 +661,13 @@ k_walk_group(WalkArgs a) {
                 if (lane == 0) dev_flag(a.err, kErrOverflow);
                 break;
             }
+            // room for the cells this round appends: up to 32 from its own
+            // nodes and, in the learned walk, up to 32 more decided by a
+            // mid-round network call.  Flushing here rather than inside the
+            // append keeps the round's node words out of the flush's live
+            // registers (both walks 2.8 % faster at 2^20; it is what lets the
+            // learned walk fuse its two-body passes without spilling)
+            if (nc > kCellCap - (MAC == kMacLearned ? 64 : 32)) flush_cells();
             if (MAC == kMacLearned && sp == 0) {
                 flush_pending();
                 continue;
