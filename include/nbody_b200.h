@@ -241,7 +241,10 @@ NB_API int32_t nb_get_state(nb_engine* h, int32_t* n_out,
  * device-resident state: half kick, drift, forces, half kick.  With
  * NB_FLAG_COLLISIONS each step then runs broad phase, merge
  * (collision_resolver.cpp:20-100 semantics) and order-preserving compaction
- * (compact_kernel.cu:39 mask). */
+ * (compact_kernel.cu:39 mask).  A call of several collisional Barnes-Hut
+ * steps (geometric MAC) keeps every count on the device between its steps:
+ * the result is the same as one call per step, and NB_C_PAIRS / NB_C_MERGES
+ * then hold the last step's counts. */
 NB_API int32_t nb_step(nb_engine* h, int32_t n_steps, double dt, double softening,
                        int32_t flags);
 /* Energy/momentum diagnostics of the device state, FP64
