@@ -80,7 +80,10 @@ struct nb_engine {
     double adapt_dt = 0.0;  // the next adaptive step's dt; 0 = take nb_step's dt
     // learned MAC
     double mac_theta_lo = 0.35, mac_theta_hi = 1.0;
-    double mac_screen_q = 0.9;             // residual quantile that sets the screen margin
+    // residual quantile that sets the screen margin: at N = 2^20 and equal
+    // rms, 0.8 measured 1 % faster than 0.9 and 4 % faster than 0.97 (fewer
+    // rows reach the network)
+    double mac_screen_q = 0.8;
     // sampled FP64 audit of the learned MAC inside nb_step, geometric fallback
     int mac_audit_every = 0, mac_audit_samples = 1024, mac_since_audit = 0;
     double mac_audit_rms_max = 1e-3, mac_audit_last_rms = 0.0, mac_audit_last_max = 0.0;

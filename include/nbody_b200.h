@@ -119,7 +119,7 @@ enum nb_param {
                                       opened; in between the network decides (default 1.0)   */
     NB_PARAM_MAC_SCREEN_QUANTILE = 13, /* f64, learned MAC: quantile of |network - screen| over
                                       the training set that sets the linear screen's margin;
-                                      0 = no screen (default 0.9, used by the next fit)       */
+                                      0 = no screen (default 0.8, used by the next fit)       */
     NB_PARAM_ENS_DIRECT_SHAPE = 14, /* i32, ensembles: direct-sum tile shape 0..8 (threads x
                                       targets/thread: 64x1 64x2 64x4 128x1 128x2 128x4 256x1
                                       256x2 256x4; default 4), normally set by nb_ens_autotune */
