@@ -39,6 +39,9 @@ constexpr int kWalkThreads = kWalkWarps * 32;
 #endif
 constexpr int kCellCap = NB_WALK_CELL_CAP;
 constexpr int kPartCap = NB_WALK_PART_CAP;
+// a round appends up to 64 cells (its own 32 and a mid-round network call's
+// 32, room made at its start) and bodies 32 at a time
+static_assert(kCellCap >= 64 && kPartCap >= 32, "interaction-list capacities");
 // per-warp shared memory, in floats
 constexpr int kWarpFloats = kCellCap * 10 + kPartCap * 4 + kPartCap * 2 + kPartCap;
 constexpr int kWalkSmem = kWalkWarps * kWarpFloats * 4;
